@@ -1,0 +1,266 @@
+"""ctypes front end of the float64 CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU legs of ``bench.py``
+import this module; the product (``brainpy.state_b200``) never does.
+
+What is pinned and what is not
+------------------------------
+* Pinned against the reference's own tests (``tests/test_oracle_golden.py``):
+  the ``iaf_psc_alpha`` NEST trace and equation checks
+  (``_nest_neuron/iaf_psc_alpha_test.py:57-127,200-245``), the ``iaf_psc_exp``
+  first-spike time, the ``aeif_cond_alpha`` one-step current delay and RKF45
+  reference loop, the STDP rule cases
+  (``_nest_plasticity/stdp_synapse_rule_test.py``), the delay timing examples
+  (``_nest_network/delay_test.py``, ``_kernel/delay_scatter.py:144-153``) and
+  the CSR structure example (``_nest_network/connectivity_test.py:290-307``).
+* Pinned against published known-answer vectors: the Threefry-2x32-20 block
+  cipher (Random123).
+* Parity unpinned: the JAX key-derivation layer (``fold_in``/``split``/
+  ``randint`` on top of the cipher) and therefore concrete connectivity for a
+  seed, because JAX cannot be installed or run in this build environment; and
+  the Poisson stream, which is the library's own (JAX's ``poisson`` depends on
+  XLA's float32 ``log``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+MODEL_IDS = {"iaf_psc_alpha": 0, "iaf_psc_exp": 1, "aeif_cond_alpha": 2}
+LEGACY, RING = 0, 1
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "libbspk_oracle.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        i64, i32, u32, dbl, vp = C.c_int64, C.c_int32, C.c_uint32, C.c_double, C.c_void_p
+        L.bo_create.restype = vp
+        L.bo_create.argtypes = [dbl, C.c_int, C.c_int]
+        L.bo_destroy.argtypes = [vp]
+        L.bo_add_pop.argtypes = [vp, C.c_int, vp, C.c_int]
+        L.bo_set_state.argtypes = [vp, C.c_int, C.c_char_p, vp]
+        L.bo_get_state.argtypes = [vp, C.c_int, C.c_char_p, vp]
+        L.bo_add_proj.argtypes = [vp, C.c_int, C.c_int, i64, vp, vp, vp, vp, C.c_int]
+        L.bo_add_drive.argtypes = [vp, C.c_int, dbl, dbl, C.c_int, u32, i64, i64, C.c_int]
+        L.bo_set_stdp.argtypes = [vp, C.c_int] + [dbl] * 7
+        L.bo_get_weights.argtypes = [vp, C.c_int, vp]
+        L.bo_record_v.argtypes = [vp, C.c_int, vp]
+        L.bo_run.restype = i64
+        L.bo_run.argtypes = [vp, i64, vp, vp, i64, vp]
+        L.bo_step_neuron.argtypes = [vp, C.c_int, dbl, dbl, dbl]
+        L.bo_step_count.restype = i64
+        L.bo_step_count.argtypes = [vp]
+        L.bo_n_total.argtypes = [vp]
+        L.bo_rk_substeps.restype = i64
+        L.bo_rk_substeps.argtypes = [vp]
+        L.bo_threefry2x32.argtypes = [u32, u32, u32, u32, vp, vp]
+        L.bo_jax_key.argtypes = [i64, vp]
+        L.bo_jax_fold_in.argtypes = [vp, u32, vp]
+        L.bo_jax_split.argtypes = [vp, C.c_int, vp]
+        L.bo_jax_random_bits.argtypes = [vp, C.c_int, i64, vp]
+        L.bo_jax_randint.argtypes = [vp, i64, i64, i64, C.c_int, vp]
+        L.bo_fixed_indegree.argtypes = [i64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                        C.c_int, vp, vp]
+        L.bo_csr_structure.argtypes = [vp, vp, i64, C.c_int, vp, vp, vp]
+        L.bo_uniform01.restype = dbl
+        L.bo_uniform01.argtypes = [u32, u32, u32, u32]
+        L.bo_poisson.argtypes = [dbl, dbl, dbl]
+        L.bo_alpha_p31_p32.argtypes = [dbl, dbl, dbl, dbl, vp, vp]
+        L.bo_propagator_exp.restype = dbl
+        L.bo_propagator_exp.argtypes = [dbl, dbl, dbl, dbl]
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+# ---------------------------------------------------------------- RNG helpers
+
+def threefry2x32(key, count):
+    y0, y1 = C.c_uint32(), C.c_uint32()
+    lib().bo_threefry2x32(int(key[0]), int(key[1]), int(count[0]), int(count[1]),
+                          C.byref(y0), C.byref(y1))
+    return y0.value, y1.value
+
+
+def jax_key(seed):
+    k = np.zeros(2, np.uint32)
+    lib().bo_jax_key(int(seed), _p(k))
+    return k
+
+
+def jax_fold_in(key, data):
+    k = np.ascontiguousarray(key, np.uint32)
+    out = np.zeros(2, np.uint32)
+    lib().bo_jax_fold_in(_p(k), int(data) & 0xFFFFFFFF, _p(out))
+    return out
+
+
+def jax_split(key, num):
+    k = np.ascontiguousarray(key, np.uint32)
+    out = np.zeros((num, 2), np.uint32)
+    lib().bo_jax_split(_p(k), int(num), _p(out))
+    return out
+
+
+def jax_randint(key, n, minval, maxval, nbits=32):
+    k = np.ascontiguousarray(key, np.uint32)
+    out = np.zeros(n, np.int64)
+    lib().bo_jax_randint(_p(k), int(n), int(minval), int(maxval), int(nbits), _p(out))
+    return out
+
+
+def fixed_indegree(seed, n_pre, n_post, K, pre_is_post=False, allow_autapses=True, nbits=32):
+    pre = np.zeros(n_post * K, np.int32)
+    post = np.zeros(n_post * K, np.int32)
+    rc = lib().bo_fixed_indegree(int(seed), n_pre, n_post, K, int(pre_is_post),
+                                 int(allow_autapses), int(nbits), _p(pre), _p(post))
+    if rc != 0:
+        raise ValueError("fixed_indegree failed")
+    return pre, post
+
+
+def csr_structure(pre, post, n_pre):
+    pre = np.ascontiguousarray(pre, np.int32)
+    post = np.ascontiguousarray(post, np.int32)
+    n = pre.shape[0]
+    order = np.zeros(n, np.int64)
+    indices = np.zeros(n, np.int32)
+    indptr = np.zeros(n_pre + 1, np.int64)
+    rc = lib().bo_csr_structure(_p(pre), _p(post), n, int(n_pre), _p(order), _p(indices),
+                                _p(indptr))
+    if rc != 0:
+        raise ValueError("csr_structure failed")
+    return order, indices, indptr
+
+
+def uniform01(seed, stream, step, idx):
+    return lib().bo_uniform01(seed, stream, step, idx)
+
+
+def poisson(lam, u):
+    return lib().bo_poisson(float(lam), float(np.exp(-lam)), float(u))
+
+
+def alpha_p31_p32(tau_syn, tau_m, c_m, h):
+    a, b = C.c_double(), C.c_double()
+    lib().bo_alpha_p31_p32(tau_syn, tau_m, c_m, h, C.byref(a), C.byref(b))
+    return a.value, b.value
+
+
+def propagator_exp(tau_syn, tau_m, c_m, h):
+    return lib().bo_propagator_exp(tau_syn, tau_m, c_m, h)
+
+
+# ------------------------------------------------------------------ simulator
+
+class OracleSim:
+    """Serial float64 restatement of one network (test checker only)."""
+
+    def __init__(self, dt, model="iaf_psc_alpha", semantics=LEGACY):
+        self._L = lib()
+        self.dt = float(dt)
+        self.model = model
+        self._h = self._L.bo_create(self.dt, int(semantics), MODEL_IDS[model])
+        self._keep = []
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._L.bo_destroy(self._h)
+            self._h = None
+
+    def add_pop(self, n, params):
+        p = np.ascontiguousarray(params, np.float64)
+        r = self._L.bo_add_pop(self._h, int(n), _p(p), int(p.size))
+        if r < 0:
+            raise ValueError("add_pop failed")
+        return r
+
+    def set_state(self, pop, name, values):
+        v = np.ascontiguousarray(values, np.float64)
+        if self._L.bo_set_state(self._h, pop, name.encode(), _p(v)) != 0:
+            raise KeyError(name)
+
+    def get_state(self, pop, name, n):
+        v = np.zeros(n, np.float64)
+        if self._L.bo_get_state(self._h, pop, name.encode(), _p(v)) != 0:
+            raise KeyError(name)
+        return v
+
+    def add_proj(self, pre_pop, post_pop, indptr, post_local, w, delay_steps, receptor=0):
+        indptr = np.ascontiguousarray(indptr, np.int64)
+        post_local = np.ascontiguousarray(post_local, np.int32)
+        w = np.ascontiguousarray(w, np.float64)
+        d = np.ascontiguousarray(delay_steps, np.int32)
+        r = self._L.bo_add_proj(self._h, pre_pop, post_pop, int(post_local.size), _p(indptr),
+                                _p(post_local), _p(w), _p(d), int(receptor))
+        if r < 0:
+            raise ValueError(f"add_proj failed ({r})")
+        return r
+
+    def add_drive(self, post_pop, rate_hz, weight, delay_steps, seed, t_min=0,
+                  t_max=2 ** 62, receptor=0):
+        r = self._L.bo_add_drive(self._h, post_pop, float(rate_hz), float(weight),
+                                 int(delay_steps), int(seed) & 0xFFFFFFFF, int(t_min),
+                                 int(t_max), int(receptor))
+        if r < 0:
+            raise ValueError("add_drive failed")
+        return r
+
+    def set_stdp(self, proj, tau_plus, tau_minus, lambda_, alpha, mu_plus, mu_minus, wmax):
+        if self._L.bo_set_stdp(self._h, proj, tau_plus, tau_minus, lambda_, alpha, mu_plus,
+                               mu_minus, wmax) != 0:
+            raise ValueError("set_stdp failed")
+
+    def weights(self, proj, n_edges):
+        w = np.zeros(n_edges, np.float64)
+        self._L.bo_get_weights(self._h, proj, _p(w))
+        return w
+
+    def record_v(self, gids):
+        self._rec = np.ascontiguousarray(gids, np.int32)
+        self._L.bo_record_v(self._h, int(self._rec.size), _p(self._rec))
+
+    def run(self, n_steps, cap=None):
+        n_rec = int(getattr(self, "_rec", np.zeros(0)).size)
+        if cap is None:
+            cap = max(1024, self._L.bo_n_total(self._h) * n_steps // 20)
+        st = np.zeros(cap, np.int64)
+        gid = np.zeros(cap, np.int32)
+        v = np.zeros((n_steps, n_rec), np.float64)
+        n = self._L.bo_run(self._h, int(n_steps), _p(st), _p(gid), int(cap), _p(v))
+        if n == -2:
+            raise FloatingPointError("Numerical instability in aeif_cond_alpha dynamics.")
+        if n > cap:
+            raise OverflowError("spike buffer too small")
+        return st[:n], gid[:n], v
+
+    def step_neuron(self, gid, w0=0.0, w1=0.0, x_next=0.0):
+        r = self._L.bo_step_neuron(self._h, int(gid), float(w0), float(w1), float(x_next))
+        if r == -2:
+            raise FloatingPointError("Numerical instability in aeif_cond_alpha dynamics.")
+        return r
+
+    @property
+    def step(self):
+        return self._L.bo_step_count(self._h)
+
+    @property
+    def rk_substeps(self):
+        return self._L.bo_rk_substeps(self._h)
