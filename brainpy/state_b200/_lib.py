@@ -1,0 +1,249 @@
+"""ctypes binding of libbspk.so (the C ABI of include/bspk.h).
+
+The library is built in-tree (``brainpy/state_b200/libbspk.so``).  There is no
+fallback: if the shared object is missing or the GPU is absent, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbspk.so")
+
+BSPK_OK = 0
+ERRORS = {
+    -1: ValueError, -2: RuntimeError, -3: RuntimeError, -4: NotImplementedError,
+    -5: TimeoutError, -6: FloatingPointError, -7: OverflowError, -8: RuntimeError,
+}
+MODELS = {"iaf_psc_alpha": 0, "iaf_psc_exp": 1, "aeif_cond_alpha": 2}
+LEGACY, RING = 0, 1
+
+
+class Config(C.Structure):
+    _fields_ = [("dt", C.c_double), ("precision", C.c_int), ("semantics", C.c_int),
+                ("deterministic", C.c_int), ("model", C.c_int), ("device", C.c_int),
+                ("spike_capacity", C.c_int64)]
+
+
+class StdpParams(C.Structure):
+    _fields_ = [("tau_plus", C.c_double), ("tau_minus", C.c_double), ("lambda_", C.c_double),
+                ("alpha", C.c_double), ("mu_plus", C.c_double), ("mu_minus", C.c_double),
+                ("Wmax", C.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libbspk.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"libbspk.so not built ({LIB_PATH}); run "
+                              "python -m brainpy.state_b200.csrc.build")
+        L = C.CDLL(LIB_PATH)
+        vp, i64, i32, dbl, u32 = C.c_void_p, C.c_int64, C.c_int32, C.c_double, C.c_uint32
+        sig = {
+            "bspk_version": (C.c_char_p, []),
+            "bspk_last_error": (C.c_char_p, []),
+            "bspk_plan_create": (C.c_int, [C.POINTER(Config), C.POINTER(vp)]),
+            "bspk_plan_destroy": (C.c_int, [vp]),
+            "bspk_pop_add": (C.c_int, [vp, C.c_int, vp, C.c_int, C.POINTER(C.c_int)]),
+            "bspk_proj_add_csr": (C.c_int, [vp, C.c_int, C.c_int, i64, vp, vp, vp, vp, C.c_int,
+                                            C.POINTER(C.c_int)]),
+            "bspk_proj_add_fixed_indegree": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, i64, C.c_int,
+                                                       C.c_int, dbl, vp, C.c_int, C.c_int,
+                                                       C.POINTER(C.c_int)]),
+            "bspk_drive_add_poisson": (C.c_int, [vp, C.c_int, dbl, dbl, C.c_int, u32, i64, i64,
+                                                 C.c_int, C.POINTER(C.c_int)]),
+            "bspk_stdp_attach": (C.c_int, [vp, C.c_int, C.POINTER(StdpParams)]),
+            "bspk_proj_csr_get": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
+            "bspk_record_v": (C.c_int, [vp, C.c_int, vp]),
+            "bspk_record_spikes_of": (C.c_int, [vp, C.c_int, vp]),
+            "bspk_plan_upload": (C.c_int, [vp, vp]),
+            "bspk_run": (C.c_int, [vp, i64, vp]),
+            "bspk_spikes_get": (C.c_int, [vp, i64, vp, vp, C.POINTER(i64)]),
+            "bspk_v_get": (C.c_int, [vp, vp]),
+            "bspk_weights_get": (C.c_int, [vp, C.c_int, vp]),
+            "bspk_state_get": (C.c_int, [vp, C.c_int, C.c_char_p, vp]),
+            "bspk_state_set": (C.c_int, [vp, C.c_int, C.c_char_p, vp]),
+            "bspk_step_count": (i64, [vp]),
+            "bspk_last_kernel_time": (C.c_int, [vp, C.POINTER(dbl), C.POINTER(i64)]),
+            "bspk_checkpoint_size": (C.c_int, [vp, C.POINTER(i64)]),
+            "bspk_checkpoint_save": (C.c_int, [vp, vp, i64]),
+            "bspk_checkpoint_restore": (C.c_int, [vp, vp, i64]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != BSPK_OK:
+        msg = lib().bspk_last_error().decode()
+        raise ERRORS.get(rc, RuntimeError)(msg or f"libbspk error {rc}")
+    return rc
+
+
+def ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Plan:
+    """Thin owner of one ``bspk_plan`` handle (one neuron model per plan)."""
+
+    def __init__(self, dt, model="iaf_psc_alpha", precision=32, semantics=LEGACY,
+                 deterministic=False, device=0, spike_capacity=1 << 22):
+        self._L = lib()
+        cfg = Config(float(dt), int(precision), int(semantics), int(bool(deterministic)),
+                     MODELS[model], int(device), int(spike_capacity))
+        h = C.c_void_p()
+        check(self._L.bspk_plan_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.model = model
+        self.precision = precision
+        self.dt = float(dt)
+        self.pop_sizes = []
+        self.n_rec_v = 0
+        self._proj_edges = []
+        self._proj_pre_n = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.bspk_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    # -- building
+    def add_pop(self, n, params):
+        p = np.ascontiguousarray(params, np.float64)
+        out = C.c_int()
+        check(self._L.bspk_pop_add(self._h, int(n), ptr(p), int(p.size), C.byref(out)))
+        self.pop_sizes.append(int(n))
+        return out.value
+
+    def add_csr(self, pre, post, indptr, post_local, w, delay_steps, receptor=0):
+        indptr = np.ascontiguousarray(indptr, np.int64)
+        post_local = np.ascontiguousarray(post_local, np.int32)
+        w = np.ascontiguousarray(w, np.float64)
+        d = np.ascontiguousarray(delay_steps, np.int32)
+        out = C.c_int()
+        check(self._L.bspk_proj_add_csr(self._h, pre, post, int(post_local.size), ptr(indptr),
+                                        ptr(post_local), ptr(w), ptr(d), int(receptor),
+                                        C.byref(out)))
+        self._proj_edges.append(int(post_local.size))
+        self._proj_pre_n.append(self.pop_sizes[pre])
+        return out.value
+
+    def add_fixed_indegree(self, pre, post, K, seed, weight, delay_steps=None, delay_const=0,
+                           allow_autapses=True, nbits=32, receptor=0):
+        d = None if delay_steps is None else np.ascontiguousarray(delay_steps, np.int32)
+        out = C.c_int()
+        check(self._L.bspk_proj_add_fixed_indegree(self._h, pre, post, int(K), int(seed),
+                                                   int(bool(allow_autapses)), int(nbits),
+                                                   float(weight), ptr(d), int(delay_const),
+                                                   int(receptor), C.byref(out)))
+        self._proj_edges.append(int(K) * self.pop_sizes[post])
+        self._proj_pre_n.append(self.pop_sizes[pre])
+        return out.value
+
+    def add_poisson(self, post, rate_hz, weight, delay_steps, seed, t_min=0, t_max=2 ** 62,
+                    receptor=0):
+        out = C.c_int()
+        check(self._L.bspk_drive_add_poisson(self._h, post, float(rate_hz), float(weight),
+                                             int(delay_steps), int(seed) & 0xFFFFFFFF,
+                                             int(t_min), int(t_max), int(receptor),
+                                             C.byref(out)))
+        return out.value
+
+    def csr(self, proj):
+        """(indptr, post_local, delay_steps, w) of a projection (host copy)."""
+        E = self._proj_edges[proj]
+        pre_n = self._proj_pre_n[proj]
+        indptr = np.zeros(pre_n + 1, np.int64)
+        post = np.zeros(E, np.int32)
+        d = np.zeros(E, np.int32)
+        w = np.zeros(E, np.float64)
+        check(self._L.bspk_proj_csr_get(self._h, int(proj), ptr(indptr), ptr(post), ptr(d),
+                                        ptr(w)))
+        return indptr, post, d, w
+
+    def attach_stdp(self, proj, tau_plus=20.0, tau_minus=20.0, lambda_=0.01, alpha=1.0,
+                    mu_plus=1.0, mu_minus=1.0, Wmax=100.0):
+        sp = StdpParams(tau_plus, tau_minus, lambda_, alpha, mu_plus, mu_minus, Wmax)
+        check(self._L.bspk_stdp_attach(self._h, proj, C.byref(sp)))
+
+    def record_v(self, gids):
+        g = np.ascontiguousarray(gids, np.int32)
+        check(self._L.bspk_record_v(self._h, int(g.size), ptr(g)))
+        self.n_rec_v = int(g.size)
+
+    def record_spikes_of(self, gids):
+        g = np.ascontiguousarray(gids, np.int32)
+        check(self._L.bspk_record_spikes_of(self._h, int(g.size), ptr(g)))
+
+    def upload(self, stream=None):
+        check(self._L.bspk_plan_upload(self._h, stream))
+
+    # -- running
+    def run(self, n_steps, stream=None):
+        check(self._L.bspk_run(self._h, int(n_steps), stream))
+        self._last_steps = int(n_steps)
+
+    def spikes(self, cap=None):
+        if cap is None:
+            cap = 1 << 24
+        st = np.zeros(cap, np.int64)
+        g = np.zeros(cap, np.int32)
+        n = C.c_int64()
+        check(self._L.bspk_spikes_get(self._h, int(cap), ptr(st), ptr(g), C.byref(n)))
+        m = n.value
+        order = np.lexsort((g[:m], st[:m]))
+        return st[:m][order], g[:m][order]
+
+    def v_trace(self):
+        out = np.zeros((self._last_steps, self.n_rec_v), np.float64)
+        check(self._L.bspk_v_get(self._h, ptr(out)))
+        return out
+
+    def weights(self, proj):
+        out = np.zeros(self._proj_edges[proj], np.float64)
+        check(self._L.bspk_weights_get(self._h, int(proj), ptr(out)))
+        return out
+
+    def get_state(self, pop, name):
+        out = np.zeros(self.pop_sizes[pop], np.float64)
+        check(self._L.bspk_state_get(self._h, int(pop), name.encode(), ptr(out)))
+        return out
+
+    def set_state(self, pop, name, values):
+        v = np.ascontiguousarray(np.broadcast_to(values, (self.pop_sizes[pop],)), np.float64)
+        check(self._L.bspk_state_set(self._h, int(pop), name.encode(), ptr(v)))
+
+    @property
+    def step(self):
+        return self._L.bspk_step_count(self._h)
+
+    def kernel_time(self):
+        ms, n = C.c_double(), C.c_int64()
+        check(self._L.bspk_last_kernel_time(self._h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def checkpoint(self):
+        n = C.c_int64()
+        check(self._L.bspk_checkpoint_size(self._h, C.byref(n)))
+        buf = np.zeros(n.value, np.uint8)
+        check(self._L.bspk_checkpoint_save(self._h, ptr(buf), n.value))
+        return buf
+
+    def restore(self, buf):
+        buf = np.ascontiguousarray(buf, np.uint8)
+        check(self._L.bspk_checkpoint_restore(self._h, ptr(buf), int(buf.size)))

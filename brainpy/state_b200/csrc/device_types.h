@@ -1,0 +1,69 @@
+// device_types.h -- plain structs shared by the host plan and the kernels.
+#pragma once
+#include <cstdint>
+
+#ifndef __CUDACC__
+#define __host__
+#define __device__
+#endif
+
+namespace bspk {
+
+enum {
+    BSPK_DEV_OK = 0,
+    BSPK_DEV_ERR_TIMEOUT = 1,
+    BSPK_DEV_ERR_OVERFLOW = 2,
+    BSPK_DEV_ERR_BOUNDS = 3,
+    BSPK_DEV_ERR_UNSTABLE = 4,
+    BSPK_DEV_ERR_RKCAP = 5,
+};
+
+constexpr int kMaxPops = 64;
+constexpr int kMaxInputs = 64;   // drives + projections per plan
+constexpr int kMaxWindow = 32;   // d_min batching window (steps)
+constexpr int kEdgeDelayShift = 24;
+constexpr uint32_t kEdgePostMask = (1u << kEdgeDelayShift) - 1u;
+
+// Per-population coefficients, computed on the host in float64 and cast to
+// the compute type.  Covers iaf_psc_alpha (P11..P32, epsc/ipsc) and
+// iaf_psc_exp (eP*); the aeif fields hold the NEST parameters directly.
+template <typename Real>
+struct PopCoef {
+    Real E_L, I_e, lower, theta, vreset;
+    Real P11ex, P21ex, P22ex, P11in, P21in, P22in, expm1_tm, P30, P31ex, P32ex, P31in, P32in,
+        epsc, ipsc;
+    Real eP11ex, eP11in, eP22, eP21ex, eP21in, eP20, one_m_eP11ex;
+    // aeif_cond_alpha
+    Real V_peak, V_reset, g_L, C_m, E_ex, E_in, Delta_T, tau_w, a, b, V_th, tau_syn_ex,
+        tau_syn_in, atol, pscon_ex, pscon_in, v_peak_detect;
+    int ref_count;
+    int off, n;  // gid range of the population
+};
+
+// Poisson drive of one population.
+struct DriveDev {
+    int pop;
+    int lag;           // arrival lag in steps (LEGACY: delay + 1)
+    uint32_t seed;
+    int cdf_off, cdf_n;
+    int receptor;
+    double weight;
+    int64_t tmin, tmax;
+};
+
+// One projection (CSR over the pre population's local indices).
+template <typename Real>
+struct ProjDev {
+    int pre_pop, post_pop, post_off, receptor;
+    int homogeneous;     // 1: every edge carries w0
+    Real w0;
+    const int64_t *indptr;   // n_pre + 1
+    const uint32_t *edges;   // post_local | (arrival lag << 24)
+    const Real *w;           // per edge (nullptr when homogeneous)
+    // deterministic pull (CSC over post local indices, sorted by pre)
+    const int64_t *cindptr;  // n_post + 1
+    const uint32_t *cedges;  // pre_local | (arrival lag << 24)
+    const double *cw;        // per in-edge weight (nullptr when homogeneous)
+};
+
+}  // namespace bspk

@@ -1,0 +1,68 @@
+// lif_args.h -- launch arguments of the windowed iaf kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "device_types.h"
+
+namespace bspk {
+
+template <typename Real>
+struct LifArgs {
+    int N, npop, nproj, ndrive;
+    const PopCoef<Real> *coef;
+    Real *s[6];
+    int *r;
+    Real *ring;
+    int L;
+    const ProjDev<Real> *projs;
+    const int *pop_out_ptr, *pop_out_list;      // outgoing projections per pre pop
+    const int *pop_in_ptr, *pop_in_list;        // inputs per post pop, creation order
+                                                // (>= 0 projection, < 0 drive -(id+1))
+    const DriveDev *drives;
+    const int *pop_drive_ptr, *pop_drive_list;  // drives per post pop
+    const double *cdf;
+    int cdf_total;
+    int64_t step0, n_steps, run_step0;
+    int W;
+    int tile;
+    int model;
+    int64_t *spk_step;
+    int32_t *spk_gid;
+    unsigned long long *spk_count;
+    int64_t spk_cap;
+    const uint8_t *spk_flag;
+    const int32_t *rec_slot;
+    Real *v_out;
+    int n_rec;
+    uint64_t *hist;  // exact mode spike history (bit m & 63 of neuron g)
+    unsigned int *barrier;
+    int *err;
+};
+
+// Launchers (cooperative, persistent).  Return the cudaError_t of the launch.
+template <typename Real>
+cudaError_t launch_lif_fast(const LifArgs<Real> &a, int grid, int block, cudaStream_t st);
+cudaError_t launch_lif_exact(const LifArgs<double> &a, int grid, int block, cudaStream_t st);
+
+size_t lif_fast_smem(int tile, int W, int npop, int ndrive, int nproj, int cdf_total, bool dbl);
+
+// Shared-memory layout of the windowed kernels (16-byte aligned sections).
+struct SmemLayout {
+    size_t coef, drive, proj, cdf, spk, total;
+};
+__host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+__host__ __device__ inline SmemLayout smem_layout(size_t coef_sz, size_t proj_sz, int npop,
+                                                  int ndrive, int nproj, int cdf_total,
+                                                  int spk_rows, int spk_cols) {
+    SmemLayout l;
+    l.coef = 0;
+    l.drive = align16(l.coef + coef_sz * npop);
+    l.proj = align16(l.drive + sizeof(DriveDev) * ndrive);
+    l.cdf = align16(l.proj + proj_sz * nproj);
+    l.spk = align16(l.cdf + sizeof(double) * cdf_total);
+    l.total = align16(l.spk + sizeof(uint32_t) * static_cast<size_t>(spk_rows) * spk_cols);
+    return l;
+}
+size_t lif_exact_smem(int block, int npop, int ndrive, int nproj, int cdf_total);
+
+}  // namespace bspk

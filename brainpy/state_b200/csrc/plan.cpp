@@ -1,0 +1,971 @@
+// plan.cpp -- host side of libbspk: the C ABI declared in include/bspk.h.
+//
+// A plan is built on the host (populations, projections, drives), uploaded
+// once, then advanced by bspk_run.  All float64 preprocessing (propagators,
+// Poisson CDF tables, connectivity sampling, CSR/CSC layouts) happens here;
+// the kernels only see packed device structures.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../../include/bspk.h"
+#include "aeif_args.h"
+#include "device_types.h"
+#include "host_rng.h"
+#include "lif_args.h"
+#include "stdp_args.h"
+#include "plan_internal.h"
+
+using namespace bspk;
+
+namespace bspk {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+}  // namespace bspk
+
+namespace {
+
+template <typename T>
+int dalloc(bspk_plan *p, T **ptr, size_t count) {
+    void *raw = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(&raw, sizeof(T) * count);
+    if (e != cudaSuccess)
+        return fail(BSPK_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    p->allocs.push_back(raw);
+    *ptr = static_cast<T *>(raw);
+    return BSPK_OK;
+}
+
+}  // namespace
+
+int bspk::dalloc_bytes(bspk_plan *p, void **ptr, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess)
+        return fail(BSPK_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    p->allocs.push_back(*ptr);
+    return BSPK_OK;
+}
+
+namespace {
+
+template <typename T>
+int upload_vec(bspk_plan *p, T **ptr, const std::vector<T> &v) {
+    int rc = dalloc(p, ptr, v.size());
+    if (rc) return rc;
+    if (!v.empty()) BSPK_CUDA(cudaMemcpy(*ptr, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+    return BSPK_OK;
+}
+
+const char *kStateNames[3][9] = {
+    {"V_m", "I_syn_ex", "dI_syn_ex", "I_syn_in", "dI_syn_in", "y0", "", "", ""},
+    {"V_m", "i_syn_ex", "i_syn_in", "i_0", "i_1", "", "", "", ""},
+    {"V_m", "dg_ex", "g_ex", "dg_in", "g_in", "w", "h", "I_stim", ""},
+};
+
+int state_slot(int model, const char *name) {
+    if (!strcmp(name, "r") || !strcmp(name, "refractory_step_count")) return 100;
+    for (int i = 0; i < 9; ++i)
+        if (kStateNames[model][i][0] && !strcmp(kStateNames[model][i], name)) return i;
+    return -1;
+}
+
+int n_state_slots(int model) { return model == BSPK_AEIF_COND_ALPHA ? 8 : 6; }
+
+// Float64 propagators and thresholds, following the reference formulas
+// (_nest_neuron/iaf_psc_alpha.py:451-556, iaf_psc_exp.py:492-512,
+// _nest_base/utils.py:126-229).
+void alpha_p31_p32(double tau_syn, double tau_m, double c_m, double h, double *p31, double *p32) {
+    const double beta = tau_syn * tau_m / (tau_m - tau_syn);
+    const double gamma = beta / c_m;
+    const double inv_beta = (tau_m - tau_syn) / (tau_syn * tau_m);
+    const double exp_h_tau_syn = std::exp(-h / tau_syn);
+    const double expm1_h_tau = std::expm1(h * inv_beta);
+    const double p32_raw = gamma * exp_h_tau_syn * expm1_h_tau;
+    const double exp_h_tau_m = std::exp(-h / tau_m);
+    const double p32_singular = h / c_m * exp_h_tau_m;
+    const bool reg32 = std::isfinite(p32_raw) && std::fabs(p32_raw) >= 2.2250738585072014e-308 &&
+                       p32_raw > 0.0;
+    *p32 = reg32 ? p32_raw : p32_singular;
+    const double h_min_regular = 1e-7 * tau_m * tau_m / std::fabs(tau_m - tau_syn);
+    const bool reg31 = std::isfinite(h_min_regular) && (h > h_min_regular);
+    const double p31_regular = gamma * exp_h_tau_syn * (beta * expm1_h_tau - h);
+    const double p31_singular = 0.5 * h * h / c_m * exp_h_tau_m;
+    *p31 = reg31 ? p31_regular : p31_singular;
+}
+
+double propagator_exp(double tau_syn, double tau_m, double c_m, double h) {
+    const double beta = tau_syn * tau_m / (tau_m - tau_syn);
+    const double gamma = beta / c_m;
+    const double inv_beta = (tau_m - tau_syn) / (tau_syn * tau_m);
+    const double exp_h_tau_syn = std::exp(-h / tau_syn);
+    const double expm1_h_tau = std::expm1(h * inv_beta);
+    const double p32_raw = gamma * exp_h_tau_syn * expm1_h_tau;
+    const bool reg = std::isfinite(p32_raw) && std::fabs(p32_raw) >= 2.2250738585072014e-308 &&
+                     p32_raw > 0.0;
+    return reg ? p32_raw : h / c_m * std::exp(-h / tau_m);
+}
+
+constexpr double kE = 2.718281828459045;
+
+int make_coef(int model, const std::vector<double> &p, double h, PopCoef<double> *c) {
+    memset(c, 0, sizeof(*c));
+    if (model == BSPK_IAF_PSC_ALPHA || model == BSPK_IAF_PSC_EXP) {
+        const size_t need = model == BSPK_IAF_PSC_ALPHA ? 10 : 9;
+        if (p.size() < need) return fail(BSPK_ERR_ARG, "too few parameters");
+        const double E_L = p[0], C_m = p[1], tau_m = p[2], t_ref = p[3], V_th = p[4],
+                     V_reset = p[5], tex = p[6], tin = p[7], I_e = p[8];
+        // parameter validation (iaf_psc_alpha.py:385-410)
+        if (!(C_m > 0)) return fail(BSPK_ERR_ARG, "Capacitance must be > 0.");
+        if (!(tau_m > 0)) return fail(BSPK_ERR_ARG, "Membrane time constant must be > 0.");
+        if (!(tex > 0) || !(tin > 0))
+            return fail(BSPK_ERR_ARG, "All synaptic time constants must be > 0.");
+        if (t_ref < 0) return fail(BSPK_ERR_ARG, "The refractory time t_ref can't be negative.");
+        if (!(V_reset < V_th)) return fail(BSPK_ERR_ARG, "Reset potential must be smaller than threshold.");
+        c->E_L = E_L;
+        c->I_e = I_e;
+        c->theta = V_th - E_L;
+        c->vreset = V_reset - E_L;
+        c->lower = model == BSPK_IAF_PSC_ALPHA ? p[9] - E_L : -INFINITY;
+        c->ref_count = static_cast<int>(std::ceil(t_ref / h));
+        c->P11ex = std::exp(-h / tex);
+        c->P22ex = c->P11ex;
+        c->P21ex = h * c->P11ex;
+        c->P11in = std::exp(-h / tin);
+        c->P22in = c->P11in;
+        c->P21in = h * c->P11in;
+        c->expm1_tm = std::expm1(-h / tau_m);
+        c->P30 = -tau_m / C_m * c->expm1_tm;
+        alpha_p31_p32(tex, tau_m, C_m, h, &c->P31ex, &c->P32ex);
+        alpha_p31_p32(tin, tau_m, C_m, h, &c->P31in, &c->P32in);
+        c->epsc = kE / tex;
+        c->ipsc = kE / tin;
+        c->eP11ex = std::exp(-h / tex);
+        c->eP11in = std::exp(-h / tin);
+        c->eP22 = std::exp(-h / tau_m);
+        c->eP21ex = propagator_exp(tex, tau_m, C_m, h);
+        c->eP21in = propagator_exp(tin, tau_m, C_m, h);
+        c->eP20 = tau_m / C_m * (1.0 - std::exp(-h / tau_m));
+        c->one_m_eP11ex = 1.0 - c->eP11ex;
+        return BSPK_OK;
+    }
+    if (model == BSPK_AEIF_COND_ALPHA) {
+        if (p.size() < 17) return fail(BSPK_ERR_ARG, "too few parameters");
+        c->V_peak = p[0];
+        c->V_reset = p[1];
+        const double t_ref = p[2];
+        c->g_L = p[3];
+        c->C_m = p[4];
+        c->E_ex = p[5];
+        c->E_in = p[6];
+        c->E_L = p[7];
+        c->Delta_T = p[8];
+        c->tau_w = p[9];
+        c->a = p[10];
+        c->b = p[11];
+        c->V_th = p[12];
+        c->tau_syn_ex = p[13];
+        c->tau_syn_in = p[14];
+        c->I_e = p[15];
+        c->atol = p[16];
+        // validation (aeif_cond_alpha.py:_validate_parameters, utils.py:85-119)
+        if (!(c->V_peak >= c->V_th)) return fail(BSPK_ERR_ARG, "V_peak >= V_th required.");
+        if (c->Delta_T < 0) return fail(BSPK_ERR_ARG, "Delta_T must be positive.");
+        if (!(c->C_m > 0)) return fail(BSPK_ERR_ARG, "Capacitance must be strictly positive.");
+        if (t_ref < 0) return fail(BSPK_ERR_ARG, "Refractory time cannot be negative.");
+        if (!(c->tau_syn_ex > 0) || !(c->tau_syn_in > 0) || !(c->tau_w > 0))
+            return fail(BSPK_ERR_ARG, "All time constants must be strictly positive.");
+        if (!(c->atol > 0)) return fail(BSPK_ERR_ARG, "The gsl_error_tol must be strictly positive.");
+        if (c->Delta_T > 0) {
+            const double max_exp_arg = std::log(1.7976931348623157e308 / 1e20);
+            if ((c->V_peak - c->V_th) / c->Delta_T >= max_exp_arg)
+                return fail(BSPK_ERR_ARG, "The current combination of V_peak, V_th and Delta_T will "
+                                          "lead to numerical overflow at spike time.");
+        }
+        c->ref_count = static_cast<int>(std::ceil(t_ref / h));
+        c->pscon_ex = kE / c->tau_syn_ex;
+        c->pscon_in = kE / c->tau_syn_in;
+        c->v_peak_detect = c->Delta_T > 0.0 ? c->V_peak : c->V_th;
+        return BSPK_OK;
+    }
+    return fail(BSPK_ERR_ARG, "unknown model");
+}
+
+template <typename Real>
+PopCoef<Real> cast_coef(const PopCoef<double> &d) {
+    PopCoef<Real> c;
+#define C_(f) c.f = static_cast<Real>(d.f);
+    C_(E_L) C_(I_e) C_(lower) C_(theta) C_(vreset) C_(P11ex) C_(P21ex) C_(P22ex) C_(P11in)
+    C_(P21in) C_(P22in) C_(expm1_tm) C_(P30) C_(P31ex) C_(P32ex) C_(P31in) C_(P32in) C_(epsc)
+    C_(ipsc) C_(eP11ex) C_(eP11in) C_(eP22) C_(eP21ex) C_(eP21in) C_(eP20) C_(one_m_eP11ex)
+    C_(V_peak) C_(V_reset) C_(g_L) C_(C_m) C_(E_ex) C_(E_in) C_(Delta_T) C_(tau_w) C_(a) C_(b)
+    C_(V_th) C_(tau_syn_ex) C_(tau_syn_in) C_(atol) C_(pscon_ex) C_(pscon_in) C_(v_peak_detect)
+#undef C_
+    c.ref_count = d.ref_count;
+    c.off = d.off;
+    c.n = d.n;
+    return c;
+}
+
+// CDF table of Poisson(lam): F[0] = exp(-lam), p_k = p_{k-1} * lam / k,
+// F[k] = F[k-1] + p_k, until F stops growing.  The count for a uniform u is
+// the smallest k with u <= F[k] (table length if none).
+std::vector<double> poisson_cdf(double lam) {
+    std::vector<double> F;
+    double p = std::exp(-lam), Fk = p;
+    F.push_back(Fk);
+    for (int k = 1; k < 4096; ++k) {
+        p = p * lam;
+        p = p / static_cast<double>(k);
+        const double Fn = Fk + p;
+        if (!(Fn > Fk)) break;
+        Fk = Fn;
+        F.push_back(Fk);
+    }
+    return F;
+}
+
+int lag_of(const bspk_plan *p, int delay_steps) {
+    return p->cfg.semantics == BSPK_LEGACY ? delay_steps + 1 : delay_steps;
+}
+
+}  // namespace
+
+// =================================================================== C ABI
+
+extern "C" {
+
+const char *bspk_version(void) { return "bspk 0.1 (sm_100a)"; }
+const char *bspk_last_error(void) { return g_err.c_str(); }
+
+int bspk_plan_create(const bspk_config *cfg, bspk_plan **out) {
+    if (!cfg || !out) return fail(BSPK_ERR_ARG, "null argument");
+    if (!(cfg->dt > 0)) return fail(BSPK_ERR_ARG, "dt must be > 0");
+    if (cfg->precision != 32 && cfg->precision != 64)
+        return fail(BSPK_ERR_ARG, "precision must be 32 or 64");
+    if (cfg->model < 0 || cfg->model > 2) return fail(BSPK_ERR_ARG, "unknown model");
+    if (cfg->semantics != BSPK_LEGACY && cfg->semantics != BSPK_RING)
+        return fail(BSPK_ERR_ARG, "unknown delivery semantics");
+    if (cfg->deterministic && (cfg->precision != 64 || cfg->semantics != BSPK_LEGACY ||
+                               cfg->model == BSPK_AEIF_COND_ALPHA))
+        return fail(BSPK_ERR_UNSUPPORTED,
+                    "deterministic mode needs precision 64, LEGACY semantics and an iaf model");
+    bspk_plan *p = new bspk_plan();
+    p->cfg = *cfg;
+    if (p->cfg.spike_capacity <= 0) p->cfg.spike_capacity = 1 << 22;
+    p->elt = cfg->precision == 64 ? 8 : 4;
+    *out = p;
+    return BSPK_OK;
+}
+
+int bspk_plan_destroy(bspk_plan *p) {
+    if (!p) return BSPK_OK;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (p->uploaded) cudaSetDevice(p->cfg.device);
+    for (void *a : p->allocs) cudaFree(a);
+    if (p->ev0) cudaEventDestroy(p->ev0);
+    if (p->ev1) cudaEventDestroy(p->ev1);
+    cudaSetDevice(dev);
+    delete p;
+    return BSPK_OK;
+}
+
+int bspk_pop_add(bspk_plan *p, int n, const double *params, int n_params, int *pop_id) {
+    if (!p || n < 0 || !params) return fail(BSPK_ERR_ARG, "bad population");
+    if (p->uploaded) return fail(BSPK_ERR_STATE, "plan already uploaded");
+    if (static_cast<int>(p->pops.size()) >= kMaxPops) return fail(BSPK_ERR_ARG, "too many populations");
+    Pop P;
+    P.n = n;
+    P.off = p->N;
+    P.p.assign(params, params + n_params);
+    int rc = make_coef(p->cfg.model, P.p, p->cfg.dt, &P.c);
+    if (rc) return rc;
+    P.c.off = P.off;
+    P.c.n = n;
+    p->pops.push_back(P);
+    p->N += n;
+    if (pop_id) *pop_id = static_cast<int>(p->pops.size()) - 1;
+    return BSPK_OK;
+}
+
+int bspk_proj_add_csr(bspk_plan *p, int pre_pop, int post_pop, int64_t n_edges,
+                      const int64_t *indptr, const int32_t *post_local, const double *w,
+                      const int32_t *delay_steps, int receptor, int *proj_id) {
+    if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    if (p->uploaded) return fail(BSPK_ERR_STATE, "plan already uploaded");
+    const int npop = static_cast<int>(p->pops.size());
+    if (pre_pop < 0 || pre_pop >= npop || post_pop < 0 || post_pop >= npop)
+        return fail(BSPK_ERR_ARG, "population index out of range");
+    if (n_edges < 0 || (n_edges > 0 && (!post_local || !w || !delay_steps)) || !indptr)
+        return fail(BSPK_ERR_ARG, "bad edge arrays");
+    if (receptor < 0 || receptor > 1) return fail(BSPK_ERR_ARG, "receptor must be 0 or 1");
+    if (static_cast<int>(p->input_kind.size()) >= kMaxInputs) return fail(BSPK_ERR_ARG, "too many inputs");
+    const int npre = p->pops[pre_pop].n, npost = p->pops[post_pop].n;
+    if (npost >= (1 << kEdgeDelayShift) || npre >= (1 << kEdgeDelayShift))
+        return fail(BSPK_ERR_UNSUPPORTED, "population larger than 2^24 neurons");
+    Proj J;
+    J.pre = pre_pop;
+    J.post = post_pop;
+    J.receptor = receptor;
+    J.indptr.assign(indptr, indptr + npre + 1);
+    if (J.indptr[0] != 0 || J.indptr[npre] != n_edges) return fail(BSPK_ERR_ARG, "indptr does not span the edges");
+    for (int i = 0; i < npre; ++i)
+        if (J.indptr[i + 1] < J.indptr[i]) return fail(BSPK_ERR_ARG, "indptr not monotone");
+    J.post_local.assign(post_local, post_local + n_edges);
+    J.delay.assign(delay_steps, delay_steps + n_edges);
+    J.w.assign(w, w + n_edges);
+    for (int64_t e = 0; e < n_edges; ++e) {
+        if (J.post_local[e] < 0 || J.post_local[e] >= npost) return fail(BSPK_ERR_ARG, "post index out of range");
+        const int lag = lag_of(p, J.delay[e]);
+        if (lag < 1 || lag > 250) return fail(BSPK_ERR_ARG, "delay out of range (1..250 steps of arrival lag)");
+        if (!std::isfinite(J.w[e])) return fail(BSPK_ERR_ARG, "non-finite weight");
+    }
+    J.homogeneous = n_edges > 0;
+    for (int64_t e = 1; e < n_edges; ++e)
+        if (J.w[e] != J.w[0]) { J.homogeneous = false; break; }
+    J.w0 = n_edges > 0 ? J.w[0] : 0.0;
+    J.input_order = static_cast<int>(p->input_kind.size());
+    p->projs.push_back(std::move(J));
+    const int id = static_cast<int>(p->projs.size()) - 1;
+    p->input_kind.push_back(id);
+    if (proj_id) *proj_id = id;
+    return BSPK_OK;
+}
+
+int bspk_proj_add_fixed_indegree(bspk_plan *p, int pre_pop, int post_pop, int K, int64_t seed,
+                                 int allow_autapses, int nbits, double weight,
+                                 const int32_t *delay_steps, int delay_const, int receptor,
+                                 int *proj_id) {
+    if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    const int npop = static_cast<int>(p->pops.size());
+    if (pre_pop < 0 || pre_pop >= npop || post_pop < 0 || post_pop >= npop)
+        return fail(BSPK_ERR_ARG, "population index out of range");
+    if (K < 0) return fail(BSPK_ERR_ARG, "K must be >= 0");
+    if (nbits != 32 && nbits != 64) return fail(BSPK_ERR_ARG, "nbits must be 32 or 64");
+    const int npre = p->pops[pre_pop].n, npost = p->pops[post_pop].n;
+    const bool pre_is_post = pre_pop == post_pop;
+    std::vector<int32_t> pre(static_cast<size_t>(npost) * K), post(pre.size());
+    int rc = host_fixed_indegree(seed, npre, npost, K, pre_is_post, allow_autapses != 0, nbits,
+                                 pre.data(), post.data());
+    if (rc) return fail(BSPK_ERR_ARG, "fixed_indegree: a target has no available source");
+    const int64_t E = static_cast<int64_t>(pre.size());
+    std::vector<int64_t> order(E), indptr(npre + 1);
+    std::vector<int32_t> indices(E);
+    host_csr_structure(pre.data(), post.data(), E, npre, order.data(), indices.data(), indptr.data());
+    std::vector<int32_t> dl(E);
+    for (int64_t e = 0; e < E; ++e) dl[e] = delay_steps ? delay_steps[order[e]] : delay_const;
+    std::vector<double> w(E, weight);
+    return bspk_proj_add_csr(p, pre_pop, post_pop, E, indptr.data(), indices.data(), w.data(),
+                             dl.data(), receptor, proj_id);
+}
+
+int bspk_drive_add_poisson(bspk_plan *p, int post_pop, double rate_hz, double weight,
+                           int delay_steps, uint32_t seed, int64_t t_min_step,
+                           int64_t t_max_step, int receptor, int *drive_id) {
+    if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    if (p->uploaded) return fail(BSPK_ERR_STATE, "plan already uploaded");
+    if (post_pop < 0 || post_pop >= static_cast<int>(p->pops.size()))
+        return fail(BSPK_ERR_ARG, "population index out of range");
+    if (static_cast<int>(p->input_kind.size()) >= kMaxInputs) return fail(BSPK_ERR_ARG, "too many inputs");
+    if (receptor < 0 || receptor > 1) return fail(BSPK_ERR_ARG, "receptor must be 0 or 1");
+    const double lam = rate_hz * p->cfg.dt / 1000.0;
+    if (!(lam >= 0) || lam > 700.0) return fail(BSPK_ERR_ARG, "rate*dt/1000 must be in [0, 700]");
+    const int lag = lag_of(p, delay_steps);
+    if (lag < 0 || delay_steps < 0) return fail(BSPK_ERR_ARG, "negative delay");
+    Drive D;
+    D.post = post_pop;
+    D.lag = lag;
+    D.delay = delay_steps;
+    D.receptor = receptor;
+    D.rate = rate_hz;
+    D.weight = weight;
+    D.seed = seed;
+    D.tmin = t_min_step;
+    D.tmax = rate_hz > 0 ? t_max_step : t_min_step;  // rate <= 0: never active
+    D.cdf = poisson_cdf(lam);
+    D.input_order = static_cast<int>(p->input_kind.size());
+    p->drives.push_back(std::move(D));
+    const int id = static_cast<int>(p->drives.size()) - 1;
+    p->input_kind.push_back(-(id + 1));
+    if (drive_id) *drive_id = id;
+    return BSPK_OK;
+}
+
+int bspk_proj_csr_get(bspk_plan *p, int proj_id, int64_t *indptr, int32_t *post_local,
+                      int32_t *delay_steps, double *w) {
+    if (!p || proj_id < 0 || proj_id >= static_cast<int>(p->projs.size()))
+        return fail(BSPK_ERR_ARG, "bad projection");
+    const Proj &J = p->projs[proj_id];
+    if (indptr) std::copy(J.indptr.begin(), J.indptr.end(), indptr);
+    if (post_local) std::copy(J.post_local.begin(), J.post_local.end(), post_local);
+    if (delay_steps) std::copy(J.delay.begin(), J.delay.end(), delay_steps);
+    if (w) std::copy(J.w.begin(), J.w.end(), w);
+    return BSPK_OK;
+}
+
+int bspk_stdp_attach(bspk_plan *p, int proj_id, const bspk_stdp_params *sp) {
+    if (!p || !sp) return fail(BSPK_ERR_ARG, "null argument");
+    if (p->uploaded) return fail(BSPK_ERR_STATE, "plan already uploaded");
+    if (proj_id < 0 || proj_id >= static_cast<int>(p->projs.size())) return fail(BSPK_ERR_ARG, "bad projection");
+    if (!(sp->tau_plus > 0)) return fail(BSPK_ERR_ARG, "'tau_plus' must be > 0.");
+    if (!(sp->tau_minus > 0)) return fail(BSPK_ERR_ARG, "'tau_minus' must be > 0.");
+    if (p->cfg.deterministic) return fail(BSPK_ERR_UNSUPPORTED, "STDP is not available in deterministic mode");
+    Proj &J = p->projs[proj_id];
+    for (size_t e = 1; e < J.delay.size(); ++e)
+        if (J.delay[e] != J.delay[0])
+            return fail(BSPK_ERR_UNSUPPORTED, "a plastic projection needs one homogeneous delay");
+    for (double w : J.w)
+        if ((w > 0) != (sp->Wmax > 0) && w != 0.0)
+            return fail(BSPK_ERR_ARG, "Weight and Wmax must have same sign.");
+    J.plastic = true;
+    J.homogeneous = false;
+    J.stdp = *sp;
+    return BSPK_OK;
+}
+
+int bspk_record_v(bspk_plan *p, int n, const int32_t *gids) {
+    if (!p || n < 0 || (n > 0 && !gids)) return fail(BSPK_ERR_ARG, "bad record list");
+    for (int i = 0; i < n; ++i)
+        if (gids[i] < 0 || gids[i] >= p->N) return fail(BSPK_ERR_ARG, "record gid out of range");
+    p->rec_v.assign(gids, gids + n);
+    if (p->uploaded) {
+        std::vector<int32_t> slot(p->N, -1);
+        for (int i = 0; i < n; ++i) slot[gids[i]] = i;
+        BSPK_CUDA(cudaSetDevice(p->cfg.device));
+        BSPK_CUDA(cudaMemcpy(p->d_rec_slot, slot.data(), sizeof(int32_t) * p->N, cudaMemcpyHostToDevice));
+    }
+    return BSPK_OK;
+}
+
+int bspk_record_spikes_of(bspk_plan *p, int n, const int32_t *gids) {
+    if (!p || n < 0 || (n > 0 && !gids)) return fail(BSPK_ERR_ARG, "bad record list");
+    p->spk_flag.assign(p->N, 0);
+    for (int i = 0; i < n; ++i) {
+        if (gids[i] < 0 || gids[i] >= p->N) return fail(BSPK_ERR_ARG, "record gid out of range");
+        p->spk_flag[gids[i]] = 1;
+    }
+    p->has_spk_flag = true;
+    if (p->uploaded) {
+        BSPK_CUDA(cudaSetDevice(p->cfg.device));
+        if (!p->d_spk_flag) {
+            int rc = dalloc(p, &p->d_spk_flag, p->N);
+            if (rc) return rc;
+        }
+        BSPK_CUDA(cudaMemcpy(p->d_spk_flag, p->spk_flag.data(), p->N, cudaMemcpyHostToDevice));
+    }
+    return BSPK_OK;
+}
+
+}  // extern "C"
+
+// --------------------------------------------------------------- upload
+
+namespace {
+
+template <typename Real>
+int upload_projs(bspk_plan *p) {
+    const bool exact = p->cfg.deterministic != 0;
+    std::vector<ProjDev<Real>> pd;
+    for (Proj &J : p->projs) {
+        const int npre = p->pops[J.pre].n, npost = p->pops[J.post].n;
+        const int64_t E = static_cast<int64_t>(J.post_local.size());
+        std::vector<uint32_t> edges(E);
+        for (int64_t e = 0; e < E; ++e)
+            edges[e] = static_cast<uint32_t>(J.post_local[e]) |
+                       (static_cast<uint32_t>(lag_of(p, J.delay[e])) << kEdgeDelayShift);
+        int rc = upload_vec(p, &J.d_indptr, J.indptr);
+        if (!rc) rc = upload_vec(p, &J.d_edges, edges);
+        if (rc) return rc;
+        if (!J.homogeneous) {
+            std::vector<Real> w(E);
+            for (int64_t e = 0; e < E; ++e) w[e] = static_cast<Real>(J.w[e]);
+            Real *dw = nullptr;
+            rc = upload_vec(p, &dw, w);
+            if (rc) return rc;
+            J.d_w = dw;
+        }
+        if (J.plastic) {
+            rc = upload_vec(p, &J.d_wplastic, J.w);
+            if (rc) return rc;
+        }
+        if (exact || J.plastic) {
+            // CSC by post, stable in CSR order (so ascending pre for each post)
+            std::vector<int64_t> cptr(npost + 1, 0);
+            for (int64_t e = 0; e < E; ++e) cptr[J.post_local[e] + 1]++;
+            for (int i = 0; i < npost; ++i) cptr[i + 1] += cptr[i];
+            std::vector<int64_t> fill(cptr.begin(), cptr.end() - 1), perm(E);
+            std::vector<uint32_t> ced(E);
+            std::vector<double> cw(E);
+            for (int i = 0; i < npre; ++i)
+                for (int64_t e = J.indptr[i]; e < J.indptr[i + 1]; ++e) {
+                    const int64_t q = fill[J.post_local[e]]++;
+                    ced[q] = static_cast<uint32_t>(i) |
+                             (static_cast<uint32_t>(lag_of(p, J.delay[e])) << kEdgeDelayShift);
+                    cw[q] = J.w[e];
+                    perm[q] = e;
+                }
+            rc = upload_vec(p, &J.d_cindptr, cptr);
+            if (!rc) rc = upload_vec(p, &J.d_cedges, ced);
+            if (!rc && !J.homogeneous) rc = upload_vec(p, &J.d_cw, cw);
+            if (!rc && J.plastic) rc = upload_vec(p, &J.d_cperm, perm);
+            if (rc) return rc;
+        }
+        if (J.plastic) {
+            void *t1 = nullptr, *t2 = nullptr;
+            int rc2 = dalloc_bytes(p, &t1, sizeof(double) * npre);
+            if (!rc2) rc2 = dalloc_bytes(p, &t2, sizeof(double) * npost);
+            if (rc2) return rc2;
+            BSPK_CUDA(cudaMemset(t1, 0, sizeof(double) * npre));
+            BSPK_CUDA(cudaMemset(t2, 0, sizeof(double) * npost));
+            J.d_pre_trace = t1;
+            J.d_post_trace = t2;
+        }
+        ProjDev<Real> d{};
+        d.pre_pop = J.pre;
+        d.post_pop = J.post;
+        d.post_off = p->pops[J.post].off;
+        d.receptor = J.receptor;
+        d.homogeneous = J.homogeneous ? 1 : 0;
+        d.w0 = static_cast<Real>(J.w0);
+        d.indptr = J.d_indptr;
+        d.edges = J.d_edges;
+        d.w = static_cast<const Real *>(J.d_w);
+        d.cindptr = J.d_cindptr;
+        d.cedges = J.d_cedges;
+        d.cw = J.d_cw;
+        pd.push_back(d);
+    }
+    ProjDev<Real> *dp = nullptr;
+    int rc = upload_vec(p, &dp, pd);
+    p->d_projs = dp;
+    return rc;
+}
+
+template <typename Real>
+int upload_coef(bspk_plan *p) {
+    std::vector<PopCoef<Real>> c;
+    for (auto &P : p->pops) c.push_back(cast_coef<Real>(P.c));
+    PopCoef<Real> *dc = nullptr;
+    int rc = upload_vec(p, &dc, c);
+    p->d_coef = dc;
+    return rc;
+}
+
+}  // namespace
+
+extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
+    (void)stream;
+    if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    if (p->uploaded) return fail(BSPK_ERR_STATE, "plan already uploaded");
+    if (p->N == 0) return fail(BSPK_ERR_ARG, "plan has no neurons");
+    BSPK_CUDA(cudaSetDevice(p->cfg.device));
+    cudaDeviceProp prop;
+    BSPK_CUDA(cudaGetDeviceProperties(&prop, p->cfg.device));
+    p->sm_count = prop.multiProcessorCount;
+    const bool dbl = p->cfg.precision == 64;
+    const bool exact = p->cfg.deterministic != 0;
+    const bool aeif = p->cfg.model == BSPK_AEIF_COND_ALPHA;
+    bool plastic = false;
+    for (auto &J : p->projs) plastic |= J.plastic;
+
+    // window and ring length
+    int min_lag = 1 << 30, max_lag = 0;
+    for (auto &J : p->projs)
+        for (int32_t d : J.delay) {
+            const int lag = lag_of(p, d);
+            min_lag = std::min(min_lag, lag);
+            max_lag = std::max(max_lag, lag);
+        }
+    if (p->projs.empty() || max_lag == 0) min_lag = kMaxWindow;
+    p->max_lag = max_lag;
+    p->W = std::max(1, std::min(min_lag, kMaxWindow));
+    if (exact) {
+        if (max_lag + 1 > 63) return fail(BSPK_ERR_UNSUPPORTED, "deterministic mode needs lags <= 62 steps");
+        p->W = std::max(1, std::min(p->W, 64 - max_lag));
+    }
+    if (aeif || plastic) p->W = 1;
+    p->L = p->W + max_lag + 1;
+
+    // state
+    const int ns = n_state_slots(p->cfg.model);
+    for (int i = 0; i < 9; ++i) p->d_s[i] = nullptr;
+    std::vector<double> init(p->N, 0.0);
+    for (int i = 0; i < ns; ++i) {
+        int rc = dalloc_bytes(p, &p->d_s[i], static_cast<size_t>(p->elt) * p->N);
+        if (rc) return rc;
+    }
+    int rc = dalloc(p, &p->d_r, p->N);
+    if (rc) return rc;
+    BSPK_CUDA(cudaMemset(p->d_r, 0, sizeof(int) * p->N));
+    for (int i = 0; i < ns; ++i) {
+        for (auto &P : p->pops)
+            for (int k = 0; k < P.n; ++k) {
+                double v = 0.0;
+                if (i == 0) v = aeif ? P.c.E_L : P.c.E_L;
+                if (aeif && i == 6) v = p->cfg.dt;  // integration_step = dt
+                init[P.off + k] = v;
+            }
+        if (dbl) {
+            BSPK_CUDA(cudaMemcpy(p->d_s[i], init.data(), 8 * p->N, cudaMemcpyHostToDevice));
+        } else {
+            std::vector<float> f(init.begin(), init.end());
+            BSPK_CUDA(cudaMemcpy(p->d_s[i], f.data(), 4 * p->N, cudaMemcpyHostToDevice));
+        }
+    }
+    // ring: [L][R][N], R = 2 for conductance models
+    const int R = aeif ? 2 : 1;
+    const size_t ring_bytes = static_cast<size_t>(p->elt) * p->L * R * p->N;
+    rc = dalloc_bytes(p, &p->d_ring, ring_bytes);
+    if (rc) return rc;
+    BSPK_CUDA(cudaMemset(p->d_ring, 0, ring_bytes));
+    rc = dalloc(p, &p->d_hist, p->N);
+    if (rc) return rc;
+    BSPK_CUDA(cudaMemset(p->d_hist, 0, sizeof(uint64_t) * p->N));
+
+    rc = dbl ? upload_coef<double>(p) : upload_coef<float>(p);
+    if (!rc) rc = dbl ? upload_projs<double>(p) : upload_projs<float>(p);
+    if (rc) return rc;
+
+    // drives and CDF tables
+    std::vector<DriveDev> dd;
+    std::vector<double> cdf;
+    for (auto &D : p->drives) {
+        DriveDev d{};
+        d.pop = D.post;
+        d.lag = D.lag;
+        d.seed = D.seed;
+        d.cdf_off = static_cast<int>(cdf.size());
+        d.cdf_n = static_cast<int>(D.cdf.size());
+        d.receptor = D.receptor;
+        d.weight = D.weight;
+        d.tmin = D.tmin;
+        d.tmax = D.tmax;
+        cdf.insert(cdf.end(), D.cdf.begin(), D.cdf.end());
+        dd.push_back(d);
+    }
+    p->cdf_total = static_cast<int>(cdf.size());
+    rc = upload_vec(p, &p->d_drives, dd);
+    if (!rc) rc = upload_vec(p, &p->d_cdf, cdf);
+    if (rc) return rc;
+    // adjacency lists per population
+    const int npop = static_cast<int>(p->pops.size());
+    std::vector<int> out_ptr(npop + 1, 0), out_list, in_ptr(npop + 1, 0), in_list,
+        dr_ptr(npop + 1, 0), dr_list;
+    for (int q = 0; q < npop; ++q) {
+        for (size_t j = 0; j < p->projs.size(); ++j)
+            if (p->projs[j].pre == q && !p->projs[j].plastic) out_list.push_back(static_cast<int>(j));
+        out_ptr[q + 1] = static_cast<int>(out_list.size());
+        for (int id : p->input_kind) {
+            const int post = id >= 0 ? p->projs[id].post : p->drives[-id - 1].post;
+            if (post == q) in_list.push_back(id);
+        }
+        in_ptr[q + 1] = static_cast<int>(in_list.size());
+        for (size_t j = 0; j < p->drives.size(); ++j)
+            if (p->drives[j].post == q) dr_list.push_back(static_cast<int>(j));
+        dr_ptr[q + 1] = static_cast<int>(dr_list.size());
+    }
+    rc = upload_vec(p, &p->d_pop_out_ptr, out_ptr);
+    if (!rc) rc = upload_vec(p, &p->d_pop_out_list, out_list);
+    if (!rc) rc = upload_vec(p, &p->d_pop_in_ptr, in_ptr);
+    if (!rc) rc = upload_vec(p, &p->d_pop_in_list, in_list);
+    if (!rc) rc = upload_vec(p, &p->d_pop_drive_ptr, dr_ptr);
+    if (!rc) rc = upload_vec(p, &p->d_pop_drive_list, dr_list);
+    if (rc) return rc;
+
+    // recording
+    rc = dalloc(p, &p->d_spk_step, p->cfg.spike_capacity);
+    if (!rc) rc = dalloc(p, &p->d_spk_gid, p->cfg.spike_capacity);
+    if (!rc) rc = dalloc(p, &p->d_spk_count, 1);
+    if (!rc) rc = dalloc(p, &p->d_rec_slot, p->N);
+    if (!rc) rc = dalloc(p, &p->d_barrier, 1);
+    if (!rc) rc = dalloc(p, &p->d_err, 1);
+    if (!rc) rc = dalloc(p, &p->d_step_spk, p->N);
+    if (!rc) rc = dalloc(p, &p->d_step_nspk, 1);
+    if (!rc) rc = dalloc(p, &p->d_rk_iters, 1);
+    if (rc) return rc;
+    BSPK_CUDA(cudaMemset(p->d_spk_count, 0, sizeof(unsigned long long)));
+    BSPK_CUDA(cudaMemset(p->d_err, 0, sizeof(int)));
+    BSPK_CUDA(cudaMemset(p->d_rk_iters, 0, sizeof(unsigned long long)));
+    {
+        std::vector<int32_t> slot(p->N, -1);
+        for (size_t i = 0; i < p->rec_v.size(); ++i) slot[p->rec_v[i]] = static_cast<int32_t>(i);
+        BSPK_CUDA(cudaMemcpy(p->d_rec_slot, slot.data(), sizeof(int32_t) * p->N, cudaMemcpyHostToDevice));
+    }
+    if (p->has_spk_flag) {
+        rc = dalloc(p, &p->d_spk_flag, p->N);
+        if (rc) return rc;
+        BSPK_CUDA(cudaMemcpy(p->d_spk_flag, p->spk_flag.data(), p->N, cudaMemcpyHostToDevice));
+    }
+    BSPK_CUDA(cudaEventCreate(&p->ev0));
+    BSPK_CUDA(cudaEventCreate(&p->ev1));
+
+    // launch geometry of the persistent kernels: one CTA per SM when the
+    // network is small, so every SM takes part in delivery.
+    int block = ((p->N + p->sm_count - 1) / p->sm_count + 31) / 32 * 32;
+    block = std::max(64, std::min(block, exact ? 256 : 512));
+    int grid = (p->N + block - 1) / block;
+    p->block = block;
+    p->grid = grid;
+    p->tile = block;
+    p->uploaded = true;
+    p->step = 0;
+    return BSPK_OK;
+}
+
+// ------------------------------------------------------------------ run
+
+namespace {
+
+template <typename Real>
+LifArgs<Real> lif_args(bspk_plan *p, int64_t n_steps) {
+    LifArgs<Real> a{};
+    a.N = p->N;
+    a.npop = static_cast<int>(p->pops.size());
+    a.nproj = static_cast<int>(p->projs.size());
+    a.ndrive = static_cast<int>(p->drives.size());
+    a.coef = static_cast<const PopCoef<Real> *>(p->d_coef);
+    for (int i = 0; i < 6; ++i) a.s[i] = static_cast<Real *>(p->d_s[i]);
+    a.r = p->d_r;
+    a.ring = static_cast<Real *>(p->d_ring);
+    a.L = p->L;
+    a.projs = static_cast<const ProjDev<Real> *>(p->d_projs);
+    a.pop_out_ptr = p->d_pop_out_ptr;
+    a.pop_out_list = p->d_pop_out_list;
+    a.pop_in_ptr = p->d_pop_in_ptr;
+    a.pop_in_list = p->d_pop_in_list;
+    a.drives = p->d_drives;
+    a.pop_drive_ptr = p->d_pop_drive_ptr;
+    a.pop_drive_list = p->d_pop_drive_list;
+    a.cdf = p->d_cdf;
+    a.cdf_total = p->cdf_total;
+    a.step0 = p->step;
+    a.n_steps = n_steps;
+    a.run_step0 = p->step;
+    a.W = p->W;
+    a.tile = p->tile;
+    a.model = p->cfg.model;
+    a.spk_step = p->d_spk_step;
+    a.spk_gid = p->d_spk_gid;
+    a.spk_count = p->d_spk_count;
+    a.spk_cap = p->cfg.spike_capacity;
+    a.spk_flag = p->has_spk_flag ? p->d_spk_flag : nullptr;
+    a.rec_slot = p->rec_v.empty() ? nullptr : p->d_rec_slot;
+    a.v_out = static_cast<Real *>(p->d_v);
+    a.n_rec = static_cast<int>(p->rec_v.size());
+    a.hist = p->d_hist;
+    a.barrier = p->d_barrier;
+    a.err = p->d_err;
+    return a;
+}
+
+
+}  // namespace
+
+extern "C" int bspk_run(bspk_plan *p, int64_t n_steps, void *stream) {
+    if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    if (!p->uploaded) return fail(BSPK_ERR_STATE, "plan not uploaded");
+    if (n_steps < 0) return fail(BSPK_ERR_ARG, "n_steps must be >= 0");
+    if (p->step + n_steps >= (int64_t(1) << 32))
+        return fail(BSPK_ERR_UNSUPPORTED, "step counter beyond 2^32 (RNG counter width)");
+    BSPK_CUDA(cudaSetDevice(p->cfg.device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // V recording buffer for this run
+    const size_t vbytes = static_cast<size_t>(p->elt) * n_steps * p->rec_v.size();
+    if (!p->rec_v.empty() && n_steps > p->v_steps_cap) {
+        if (p->d_v) {
+            cudaFree(p->d_v);
+            p->allocs.erase(std::remove(p->allocs.begin(), p->allocs.end(), p->d_v), p->allocs.end());
+            p->d_v = nullptr;
+        }
+        int rc = dalloc_bytes(p, &p->d_v, vbytes);
+        if (rc) return rc;
+        p->v_steps_cap = n_steps;
+    }
+    BSPK_CUDA(cudaMemsetAsync(p->d_spk_count, 0, sizeof(unsigned long long), st));
+    BSPK_CUDA(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
+    p->last_run_steps = n_steps;
+    if (n_steps == 0) return BSPK_OK;
+    const bool dbl = p->cfg.precision == 64;
+    BSPK_CUDA(cudaMemsetAsync(p->d_barrier, 0, sizeof(unsigned int), st));
+    BSPK_CUDA(cudaEventRecord(p->ev0, st));
+    cudaError_t e = cudaSuccess;
+    bool per_step = p->cfg.model == BSPK_AEIF_COND_ALPHA;
+    for (auto &J : p->projs) per_step |= J.plastic;
+    if (per_step) {
+        int rc = run_per_step(p, n_steps, st);
+        if (rc) return rc;
+    } else if (p->cfg.deterministic) {
+        LifArgs<double> a = lif_args<double>(p, n_steps);
+        e = launch_lif_exact(a, p->grid, p->block, st);
+        p->last_launches = 1;
+    } else if (dbl) {
+        LifArgs<double> a = lif_args<double>(p, n_steps);
+        e = launch_lif_fast<double>(a, p->grid, p->block, st);
+        p->last_launches = 1;
+    } else {
+        LifArgs<float> a = lif_args<float>(p, n_steps);
+        e = launch_lif_fast<float>(a, p->grid, p->block, st);
+        p->last_launches = 1;
+    }
+    if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    BSPK_CUDA(cudaEventRecord(p->ev1, st));
+    p->step += n_steps;
+    return BSPK_OK;
+}
+
+int bspk::sync_and_check(bspk_plan *p) {
+    BSPK_CUDA(cudaSetDevice(p->cfg.device));
+    BSPK_CUDA(cudaDeviceSynchronize());
+    int err = 0;
+    BSPK_CUDA(cudaMemcpy(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err == BSPK_DEV_ERR_TIMEOUT) return fail(BSPK_ERR_TIMEOUT, "device barrier timed out");
+    if (err == BSPK_DEV_ERR_UNSTABLE) return fail(BSPK_ERR_UNSTABLE, "Numerical instability in aeif_cond_alpha dynamics.");
+    if (err == BSPK_DEV_ERR_RKCAP) return fail(BSPK_ERR_RKCAP, "RKF45 iteration cap reached");
+    if (err == BSPK_DEV_ERR_BOUNDS) return fail(BSPK_ERR_ARG, "device bounds check failed");
+    if (err) return fail(BSPK_ERR_CUDA, "device error flag " + std::to_string(err));
+    return BSPK_OK;
+}
+
+
+extern "C" {
+
+int bspk_spikes_get(bspk_plan *p, int64_t cap, int64_t *steps, int32_t *gids, int64_t *n_out) {
+    if (!p || !p->uploaded || !n_out) return fail(BSPK_ERR_ARG, "bad arguments");
+    int rc = sync_and_check(p);
+    if (rc) return rc;
+    unsigned long long cnt = 0;
+    BSPK_CUDA(cudaMemcpy(&cnt, p->d_spk_count, sizeof(cnt), cudaMemcpyDeviceToHost));
+    if (static_cast<int64_t>(cnt) > p->cfg.spike_capacity) {
+        *n_out = static_cast<int64_t>(cnt);
+        return fail(BSPK_ERR_OVERFLOW, "spike record overflowed its device capacity");
+    }
+    const int64_t n = std::min<int64_t>(static_cast<int64_t>(cnt), cap);
+    if (n > 0) {
+        std::vector<int64_t> s(n);
+        std::vector<int32_t> g(n);
+        BSPK_CUDA(cudaMemcpy(s.data(), p->d_spk_step, 8 * n, cudaMemcpyDeviceToHost));
+        BSPK_CUDA(cudaMemcpy(g.data(), p->d_spk_gid, 4 * n, cudaMemcpyDeviceToHost));
+        int64_t m = 0;
+        for (int64_t i = 0; i < n; ++i) {
+            if (g[i] < 0) continue;  // unrecorded neuron
+            steps[m] = s[i];
+            gids[m] = g[i];
+            ++m;
+        }
+        *n_out = m;
+    } else {
+        *n_out = static_cast<int64_t>(cnt);
+    }
+    return BSPK_OK;
+}
+
+int bspk_v_get(bspk_plan *p, double *out) {
+    if (!p || !p->uploaded || !out) return fail(BSPK_ERR_ARG, "bad arguments");
+    int rc = sync_and_check(p);
+    if (rc) return rc;
+    const size_t n = static_cast<size_t>(p->last_run_steps) * p->rec_v.size();
+    if (n == 0) return BSPK_OK;
+    if (p->elt == 8) {
+        BSPK_CUDA(cudaMemcpy(out, p->d_v, 8 * n, cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> f(n);
+        BSPK_CUDA(cudaMemcpy(f.data(), p->d_v, 4 * n, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < n; ++i) out[i] = f[i];
+    }
+    return BSPK_OK;
+}
+
+int bspk_weights_get(bspk_plan *p, int proj_id, double *w) {
+    if (!p || proj_id < 0 || proj_id >= static_cast<int>(p->projs.size()) || !w)
+        return fail(BSPK_ERR_ARG, "bad arguments");
+    Proj &J = p->projs[proj_id];
+    const size_t E = J.post_local.size();
+    if (!p->uploaded || !J.plastic) {
+        std::copy(J.w.begin(), J.w.end(), w);
+        return BSPK_OK;
+    }
+    int rc = sync_and_check(p);
+    if (rc) return rc;
+    if (E) BSPK_CUDA(cudaMemcpy(w, J.d_wplastic, 8 * E, cudaMemcpyDeviceToHost));
+    return BSPK_OK;
+}
+
+int bspk_state_get(bspk_plan *p, int pop, const char *name, double *values) {
+    if (!p || !name || !values || pop < 0 || pop >= static_cast<int>(p->pops.size()))
+        return fail(BSPK_ERR_ARG, "bad arguments");
+    const int slot = state_slot(p->cfg.model, name);
+    if (slot < 0) return fail(BSPK_ERR_ARG, std::string("unknown state ") + name);
+    if (!p->uploaded) return fail(BSPK_ERR_STATE, "plan not uploaded");
+    int rc = sync_and_check(p);
+    if (rc) return rc;
+    const Pop &P = p->pops[pop];
+    if (slot == 100) {
+        std::vector<int> r(P.n);
+        BSPK_CUDA(cudaMemcpy(r.data(), p->d_r + P.off, 4 * P.n, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < P.n; ++i) values[i] = r[i];
+        return BSPK_OK;
+    }
+    const char *base = static_cast<const char *>(p->d_s[slot]) + static_cast<size_t>(p->elt) * P.off;
+    if (p->elt == 8) {
+        BSPK_CUDA(cudaMemcpy(values, base, 8 * P.n, cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> f(P.n);
+        BSPK_CUDA(cudaMemcpy(f.data(), base, 4 * P.n, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < P.n; ++i) values[i] = f[i];
+    }
+    return BSPK_OK;
+}
+
+int bspk_state_set(bspk_plan *p, int pop, const char *name, const double *values) {
+    if (!p || !name || !values || pop < 0 || pop >= static_cast<int>(p->pops.size()))
+        return fail(BSPK_ERR_ARG, "bad arguments");
+    const int slot = state_slot(p->cfg.model, name);
+    if (slot < 0) return fail(BSPK_ERR_ARG, std::string("unknown state ") + name);
+    if (!p->uploaded) return fail(BSPK_ERR_STATE, "plan not uploaded");
+    BSPK_CUDA(cudaSetDevice(p->cfg.device));
+    BSPK_CUDA(cudaDeviceSynchronize());
+    const Pop &P = p->pops[pop];
+    if (slot == 100) {
+        std::vector<int> r(P.n);
+        for (int i = 0; i < P.n; ++i) r[i] = static_cast<int>(values[i]);
+        BSPK_CUDA(cudaMemcpy(p->d_r + P.off, r.data(), 4 * P.n, cudaMemcpyHostToDevice));
+        return BSPK_OK;
+    }
+    char *base = static_cast<char *>(p->d_s[slot]) + static_cast<size_t>(p->elt) * P.off;
+    if (p->elt == 8) {
+        BSPK_CUDA(cudaMemcpy(base, values, 8 * P.n, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> f(values, values + P.n);
+        BSPK_CUDA(cudaMemcpy(base, f.data(), 4 * P.n, cudaMemcpyHostToDevice));
+    }
+    return BSPK_OK;
+}
+
+int64_t bspk_step_count(bspk_plan *p) { return p ? p->step : -1; }
+
+int bspk_last_kernel_time(bspk_plan *p, double *ms, int64_t *launches) {
+    if (!p || !p->uploaded) return fail(BSPK_ERR_ARG, "bad arguments");
+    BSPK_CUDA(cudaEventSynchronize(p->ev1));
+    float f = 0.f;
+    BSPK_CUDA(cudaEventElapsedTime(&f, p->ev0, p->ev1));
+    if (ms) *ms = f;
+    if (launches) *launches = p->last_launches;
+    return BSPK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,116 @@
+// plan_internal.h -- the plan object behind the C ABI (host only).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../../include/bspk.h"
+#include "device_types.h"
+
+namespace bspk {
+
+int fail(int code, const std::string &msg);
+
+#define BSPK_CUDA(call)                                                                 \
+    do {                                                                                \
+        cudaError_t e__ = (call);                                                       \
+        if (e__ != cudaSuccess)                                                         \
+            return ::bspk::fail(BSPK_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e__)); \
+    } while (0)
+
+struct Pop {
+    int n = 0, off = 0;
+    std::vector<double> p;
+    PopCoef<double> c{};
+};
+
+struct Proj {
+    int pre = 0, post = 0, receptor = 0;
+    std::vector<int64_t> indptr;
+    std::vector<int32_t> post_local, delay;
+    std::vector<double> w;
+    bool homogeneous = false;
+    double w0 = 0.0;
+    bool plastic = false;
+    bspk_stdp_params stdp{};
+    int input_order = 0;
+    // device
+    int64_t *d_indptr = nullptr;
+    uint32_t *d_edges = nullptr;
+    void *d_w = nullptr;
+    int64_t *d_cindptr = nullptr;
+    uint32_t *d_cedges = nullptr;
+    double *d_cw = nullptr;
+    double *d_wplastic = nullptr;   // FP64 plastic weights (CSR order)
+    int64_t *d_cperm = nullptr;     // CSC position -> CSR edge id
+    void *d_pre_trace = nullptr, *d_post_trace = nullptr;
+};
+
+struct Drive {
+    int post = 0, lag = 0, receptor = 0, delay = 0;
+    double rate = 0, weight = 0;
+    uint32_t seed = 0;
+    int64_t tmin = 0, tmax = 0;
+    std::vector<double> cdf;
+    int input_order = 0;
+};
+
+}  // namespace bspk
+
+struct bspk_plan {
+    bspk_config cfg{};
+    std::vector<bspk::Pop> pops;
+    std::vector<bspk::Proj> projs;
+    std::vector<bspk::Drive> drives;
+    std::vector<int> input_kind;  // creation order: >= 0 proj id, < 0 drive -(id+1)
+    std::vector<int32_t> rec_v;
+    std::vector<uint8_t> spk_flag;
+    bool has_spk_flag = false;
+    int N = 0;
+    bool uploaded = false;
+    int64_t step = 0;
+    // derived
+    int W = 1, L = 1, max_lag = 0;
+    int elt = 4;  // bytes per Real
+    // device buffers
+    std::vector<void *> allocs;
+    void *d_s[9] = {};
+    int *d_r = nullptr;
+    void *d_ring = nullptr;
+    uint64_t *d_hist = nullptr;
+    void *d_coef = nullptr;
+    void *d_projs = nullptr;
+    bspk::DriveDev *d_drives = nullptr;
+    double *d_cdf = nullptr;
+    int cdf_total = 0;
+    int *d_pop_out_ptr = nullptr, *d_pop_out_list = nullptr;
+    int *d_pop_in_ptr = nullptr, *d_pop_in_list = nullptr;
+    int *d_pop_drive_ptr = nullptr, *d_pop_drive_list = nullptr;
+    int64_t *d_spk_step = nullptr;
+    int32_t *d_spk_gid = nullptr;
+    unsigned long long *d_spk_count = nullptr;
+    uint8_t *d_spk_flag = nullptr;
+    int32_t *d_rec_slot = nullptr;
+    void *d_v = nullptr;
+    int64_t v_steps_cap = 0;
+    int64_t last_run_steps = 0;
+    unsigned int *d_barrier = nullptr;
+    int *d_err = nullptr;
+    // per-step engine (aeif / plastic)
+    uint32_t *d_step_spk = nullptr;  // spikes of the current step (gids)
+    int *d_step_nspk = nullptr;
+    unsigned long long *d_rk_iters = nullptr;
+    // timing
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0.0;
+    int64_t last_launches = 0;
+    int grid = 0, block = 0, tile = 0;
+    int sm_count = 0;
+};
+
+namespace bspk {
+int dalloc_bytes(bspk_plan *p, void **ptr, size_t bytes);
+int sync_and_check(bspk_plan *p);
+}  // namespace bspk

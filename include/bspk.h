@@ -1,0 +1,161 @@
+/*
+ * bspk.h -- C ABI of libbspk.so, the B200 (sm_100a) network-step library.
+ *
+ * The reference (brainspike, formerly chaobrain/brainpy.state) has no native
+ * ABI: its hot path is Python/JAX with brainevent operators.  Each entry
+ * point below replaces one reference interface, cited as
+ * <file>:<line> relative to the brainspike project root.
+ *
+ * Conventions
+ *  - Every function returns an int status (BSPK_OK = 0, negative = error);
+ *    bspk_last_error() returns a thread-local message for the last failure.
+ *  - Host pointers passed in are borrowed for the duration of the call.
+ *  - The plan owns all device buffers.  `stream` is a cudaStream_t passed as
+ *    void* (NULL = the legacy default stream).  One plan is driven from one
+ *    stream at a time; calls on one plan are not re-entrant.
+ *  - Units are NEST's: ms, mV, pA, pF, nS, Hz.
+ */
+#ifndef BSPK_H
+#define BSPK_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    BSPK_OK = 0,
+    BSPK_ERR_ARG = -1,       /* bad argument (ValueError in the reference) */
+    BSPK_ERR_STATE = -2,     /* call out of order (e.g. add after upload) */
+    BSPK_ERR_CUDA = -3,      /* CUDA runtime failure */
+    BSPK_ERR_UNSUPPORTED = -4,
+    BSPK_ERR_TIMEOUT = -5,   /* a bounded device wait ran out */
+    BSPK_ERR_UNSTABLE = -6,  /* aeif_cond_alpha instability guard */
+    BSPK_ERR_OVERFLOW = -7,  /* a device buffer (spike record) overflowed */
+    BSPK_ERR_RKCAP = -8      /* RKF45 iteration cap reached */
+};
+
+/* neuron models: iaf_psc_alpha (_nest_neuron/iaf_psc_alpha.py:558),
+ * iaf_psc_exp (_nest_neuron/iaf_psc_exp.py:552), aeif_cond_alpha
+ * (_nest_neuron/aeif_cond_alpha.py:627) */
+enum { BSPK_IAF_PSC_ALPHA = 0, BSPK_IAF_PSC_EXP = 1, BSPK_AEIF_COND_ALPHA = 2 };
+
+/* delivery semantics:
+ *  LEGACY: Simulator timing, a spike of step m reaches step m + D + 1
+ *          (_nest_network/simulator.py:1719-1788, delay.py:114-128);
+ *  RING:   kernel/NEST timing, an event of step n over delay d arrives at
+ *          step n + d (_kernel/delay_scatter.py:1-25, _kernel/delays.py:260). */
+enum { BSPK_LEGACY = 0, BSPK_RING = 1 };
+
+typedef struct bspk_plan bspk_plan;
+
+typedef struct {
+    double dt;              /* ms */
+    int precision;          /* 32 or 64: state, ring and weight arithmetic */
+    int semantics;          /* BSPK_LEGACY or BSPK_RING */
+    int deterministic;      /* 1: FP64 pull delivery, bit-reproducible order */
+    int model;              /* one neuron model per plan */
+    int device;             /* CUDA device ordinal */
+    int64_t spike_capacity; /* recorded spike events kept on the device */
+} bspk_config;
+
+typedef struct {
+    double tau_plus, tau_minus, lambda_, alpha, mu_plus, mu_minus, Wmax;
+} bspk_stdp_params;
+
+/* Library version string and build arch. */
+const char *bspk_version(void);
+const char *bspk_last_error(void);
+
+/* Plan lifecycle.  Replaces Simulator(dt) + brainstate.environ precision
+ * (_nest_network/simulator.py:417-456). */
+int bspk_plan_create(const bspk_config *cfg, bspk_plan **out);
+int bspk_plan_destroy(bspk_plan *plan);
+
+/* Population of `n` neurons with per-population NEST parameters in the
+ * model's fixed order (see DESIGN: iaf_psc_alpha E_L C_m tau_m t_ref V_th
+ * V_reset tau_syn_ex tau_syn_in I_e V_min; iaf_psc_exp the same without V_min;
+ * aeif_cond_alpha V_peak V_reset t_ref g_L C_m E_ex E_in E_L Delta_T tau_w a b
+ * V_th tau_syn_ex tau_syn_in I_e gsl_error_tol).  Propagators are computed
+ * here in float64.  Replaces Simulator.create (simulator.py:458) and the
+ * models' _precompute_propagators (iaf_psc_alpha.py:451-479,
+ * iaf_psc_exp.py:492-512). */
+int bspk_pop_add(bspk_plan *plan, int n, const double *params, int n_params, int *pop_id);
+
+/* Static CSR projection (rows = pre neurons of pre_pop, local indices):
+ * indptr[n_pre+1], post_local[E], w[E] (pA or nS), delay_steps[E] (the
+ * reference's delay in steps; LEGACY adds the holder lag), receptor 0/1
+ * (conductance models: 0 = g_ex, 1 = g_in).  Replaces the brainevent
+ * CSR + BinaryArray event matmul (_nest_network/projections.py:36-59,
+ * event_proj.py:293-325) and DelayScatter (_kernel/delay_scatter.py:109). */
+int bspk_proj_add_csr(bspk_plan *plan, int pre_pop, int post_pop, int64_t n_edges,
+                      const int64_t *indptr, const int32_t *post_local, const double *w,
+                      const int32_t *delay_steps, int receptor, int *proj_id);
+
+/* fixed_indegree projection sampled inside the library with the reference's
+ * key derivation (jax.random.key(seed) -> split(3)[0] -> fold_in(post) ->
+ * randint with nbits-wide bits), then CSR by stable pre sort.  Replaces
+ * sample_fixed_indegree + csr_structure (_nest_network/connectivity.py:39-53,
+ * :101-135).  `delay_steps` may be NULL (then `delay_const` for all edges). */
+int bspk_proj_add_fixed_indegree(bspk_plan *plan, int pre_pop, int post_pop, int K,
+                                 int64_t seed, int allow_autapses, int nbits, double weight,
+                                 const int32_t *delay_steps, int delay_const, int receptor,
+                                 int *proj_id);
+
+/* Poisson drive, one independent train per target neuron of post_pop (the
+ * Simulator realises a generator per target, simulator.py:1437-1463):
+ * count ~ Poisson(rate*dt/1000) per step, active iff t_min < step <= t_max
+ * (poisson_generator.py:501-579), delivered with weight after delay_steps. */
+int bspk_drive_add_poisson(bspk_plan *plan, int post_pop, double rate_hz, double weight,
+                           int delay_steps, uint32_t seed, int64_t t_min_step,
+                           int64_t t_max_step, int receptor, int *drive_id);
+
+/* Copy a projection's CSR (host copy: indptr[n_pre+1], post_local[E],
+ * delay_steps[E], w[E] as given or as sampled).  Replaces the structure
+ * arrays read back from a brainevent CSR (_nest_network/projections.py:51-54). */
+int bspk_proj_csr_get(bspk_plan *plan, int proj_id, int64_t *indptr, int32_t *post_local,
+                      int32_t *delay_steps, double *w);
+
+/* Make a CSR projection plastic with the pair STDP rule of
+ * _nest_plasticity/stdp_synapse.py:163-179 driven by the eager substrate of
+ * _nest_network/event_plastic.py:390-518 (weights kept in FP64). */
+int bspk_stdp_attach(bspk_plan *plan, int proj_id, const bspk_stdp_params *p);
+
+/* Recording taps (simulator.py:645-662, :1858-1870): V_m of the listed
+ * neurons every step; spikes of all neurons (or of the flagged ones). */
+int bspk_record_v(bspk_plan *plan, int n, const int32_t *gids);
+int bspk_record_spikes_of(bspk_plan *plan, int n, const int32_t *gids);
+
+/* Upload structure and state to the device (after all adds). */
+int bspk_plan_upload(bspk_plan *plan, void *stream);
+
+/* Advance n_steps (Simulator.simulate/cont, simulator.py:1790-1883; kernel
+ * Program.rollout, _kernel/runner.py:689-779).  Asynchronous on `stream`. */
+int bspk_run(bspk_plan *plan, int64_t n_steps, void *stream);
+
+/* Synchronise and copy out what the last bspk_run recorded.
+ * spikes: (step, gid) pairs in no particular order, *n_out = count. */
+int bspk_spikes_get(bspk_plan *plan, int64_t cap, int64_t *steps, int32_t *gids,
+                    int64_t *n_out);
+/* V_m trace of the last run: [n_steps][n_rec] as double. */
+int bspk_v_get(bspk_plan *plan, double *out);
+int bspk_weights_get(bspk_plan *plan, int proj_id, double *w_csr_order);
+int bspk_state_get(bspk_plan *plan, int pop, const char *name, double *values);
+int bspk_state_set(bspk_plan *plan, int pop, const char *name, const double *values);
+int64_t bspk_step_count(bspk_plan *plan);
+
+/* Timing of the dominant kernel of the last bspk_run (CUDA events on the
+ * launching stream): total ms and number of launches. */
+int bspk_last_kernel_time(bspk_plan *plan, double *ms, int64_t *launches);
+
+/* Checkpoint of every device buffer that evolves (state, rings, spike
+ * history, plastic weights and traces, step counter); restore is bit-exact
+ * (simulator.py:1822-1839 continues without re-init). */
+int bspk_checkpoint_size(bspk_plan *plan, int64_t *bytes);
+int bspk_checkpoint_save(bspk_plan *plan, void *host_buf, int64_t bytes);
+int bspk_checkpoint_restore(bspk_plan *plan, const void *host_buf, int64_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

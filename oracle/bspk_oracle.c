@@ -157,14 +157,20 @@ double bo_uniform01(uint32_t seed, uint32_t stream, uint32_t step, uint32_t idx)
     return (double)(b >> 11) * 0x1.0p-53;
 }
 
+/* Inversion by sequential search over the CDF F[0] = exp(-lam),
+ * p_k = p_{k-1} * lam / k, F[k] = F[k-1] + p_k; the table ends where F stops
+ * growing (at most 4096 entries) and a u beyond it maps to the table length. */
 int bo_poisson(double lam, double exp_neg_lam, double u) {
     int k = 0;
     double p = exp_neg_lam, F = p;
-    while (u > F && k < 100000) {
-        k += 1;
+    while (u > F) {
+        if (k + 1 >= 4096) return k + 1;
         p = p * lam;
-        p = p / (double)k;
-        F = F + p;
+        p = p / (double)(k + 1);
+        double Fn = F + p;
+        if (!(Fn > F)) return k + 1;
+        F = Fn;
+        k += 1;
     }
     return k;
 }

@@ -1,0 +1,120 @@
+"""GPU parity of the iaf network step against the float64 oracle (C-ABI path).
+
+Tolerances:
+  * deterministic FP64 mode: bit-exact spikes and V_m (same operation order);
+  * fast FP64 (atomic delivery): identical spikes and |dV| <= 1e-9 mV over a
+    horizon shorter than the network's divergence time;
+  * FP32: |dV| <= 2e-3 mV over the first 30 steps, population rate within 5 %
+    over a long run (the network is chaotic, so trajectories separate).
+"""
+import numpy as np
+import pytest
+
+from tests.netbuild import Net
+
+pytestmark = pytest.mark.gpu
+
+
+def _raster(steps, gids):
+    return set(zip(steps.tolist(), gids.tolist()))
+
+
+@pytest.mark.parametrize("model", ["iaf_psc_alpha", "iaf_psc_exp"])
+def test_exact_fp64_matches_oracle_bitwise(oracle, model):
+    net = Net(model=model)
+    rec = np.arange(0, 250, 7)
+    pl = net.to_plan(precision=64, deterministic=True, rec=rec)
+    sim = net.to_oracle(oracle, rec=rec)
+    for chunk in (300, 137, 63):      # several runs: cont() semantics
+        pl.run(chunk)
+        st, g = pl.spikes()
+        ost, og, ov = sim.run(chunk)
+        assert len(st) > 0
+        assert _raster(st, g) == _raster(ost, og)
+        np.testing.assert_array_equal(pl.v_trace(), ov)
+    for pop, n in ((0, 200), (1, 50)):
+        np.testing.assert_array_equal(pl.get_state(pop, "V_m"), sim.get_state(pop, "V_m", n))
+
+
+def test_fast_fp64_matches_oracle_short_horizon(oracle):
+    net = Net()
+    rec = np.arange(250)
+    pl = net.to_plan(precision=64, rec=rec)
+    sim = net.to_oracle(oracle, rec=rec)
+    pl.run(120)
+    st, g = pl.spikes()
+    ost, og, ov = sim.run(120)
+    assert _raster(st, g) == _raster(ost, og)
+    np.testing.assert_allclose(pl.v_trace(), ov, rtol=0, atol=1e-9)
+
+
+def test_ring_semantics_per_edge_delays(oracle):
+    net = Net(per_edge_delay=(10, 30), delay=10)
+    rec = np.arange(250)
+    pl = net.to_plan(precision=64, semantics=1, rec=rec)
+    sim = net.to_oracle(oracle, semantics=1, rec=rec)
+    pl.run(150)
+    st, g = pl.spikes()
+    ost, og, ov = sim.run(150)
+    assert len(st) > 0
+    assert _raster(st, g) == _raster(ost, og)
+    np.testing.assert_allclose(pl.v_trace(), ov, rtol=0, atol=1e-9)
+
+
+def test_fp32_trace_and_rate(oracle):
+    net = Net(NE=400, NI=100, CE=40, CI=10)
+    rec = np.arange(500)
+    pl = net.to_plan(precision=32, rec=rec)
+    sim = net.to_oracle(oracle, rec=rec)
+    pl.run(30)
+    _, _, ov = sim.run(30)
+    np.testing.assert_allclose(pl.v_trace(), ov, rtol=0, atol=2e-3)
+    pl.run(3000)
+    st, _ = pl.spikes()
+    ost, _, _ = sim.run(3000)
+    rate_gpu, rate_cpu = len(st), len(ost)
+    assert rate_cpu > 100
+    assert abs(rate_gpu - rate_cpu) / rate_cpu < 0.05
+
+
+def test_checkpoint_restore_is_bit_exact():
+    net = Net(per_edge_delay=(10, 30), delay=10)
+    pl = net.to_plan(precision=32, semantics=1, rec=np.arange(250))
+    pl.run(100)
+    ck = pl.checkpoint()
+    pl.run(200)
+    v1 = pl.v_trace().copy()
+    s1 = pl.spikes()
+    pl.restore(ck)
+    assert pl.step == 100
+    pl.run(200)
+    # atomics make FP32 delivery order-dependent, so compare the deterministic
+    # part: the first window after restore depends only on restored state
+    np.testing.assert_array_equal(pl.v_trace()[:10], v1[:10])
+    assert len(pl.spikes()[0]) > 0 and len(s1[0]) > 0
+
+
+def test_empty_and_edge_cases(oracle):
+    # a projection with zero edges, a population of one neuron, lag-1 edges
+    from brainpy.state_b200 import _lib
+    params = [0.0, 250.0, 20.0, 2.0, 20.0, 10.0, 0.5, 0.5, 400.0, -np.inf]
+    pl = _lib.Plan(0.1, precision=64, deterministic=True)
+    sim = oracle.OracleSim(0.1)
+    for s in (pl, sim):
+        a = s.add_pop(5, params)
+        b = s.add_pop(1, params)
+    pl.add_csr(0, 1, np.zeros(6, np.int64), np.zeros(0, np.int32), np.zeros(0), np.zeros(0, np.int32))
+    sim.add_proj(0, 1, np.zeros(6, np.int64), np.zeros(0, np.int32), np.zeros(0), np.zeros(0, np.int32))
+    ind = np.array([0, 1, 2, 3, 4, 5], np.int64)
+    for s in (pl, sim):
+        (s.add_csr if s is pl else s.add_proj)(0, 1, ind, np.zeros(5, np.int32), np.full(5, 30.0),
+                                               np.zeros(5, np.int32))
+    pl.record_v([5])
+    sim.record_v([5])
+    pl.upload()
+    pl.run(400)
+    st, g = pl.spikes()
+    ost, og, ov = sim.run(400)
+    assert len(st) > 0
+    assert _raster(st, g) == _raster(ost, og)
+    np.testing.assert_array_equal(pl.v_trace(), ov)
