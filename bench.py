@@ -1,0 +1,355 @@
+"""Benchmark: Brunel-12.5k real-time factor & synaptic events/s on one B200.
+
+Workload (the reference's full-scale Brunel, per-edge delays): NE=10000,
+NI=2500 iaf_psc_alpha, CE=1000, CI=250, g=5, eta=2, J=0.1 mV PSP, recurrent
+delays uniform on the 0.1 ms grid in [1.0, 3.0] ms (NEST/kernel ring timing),
+Poisson drive per neuron (delay 1.5 ms), dt=0.1 ms.  One bench step = one
+simulated second (10 000 time steps) of the resident network.  Synthetic,
+seeded inputs; no dataset is involved.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  ``value`` is the whole-job real-time factor
+(simulated seconds per wall second, summed over ranks; each rank runs an
+independent replica); ``e2e`` is the same metric through the public
+``Simulator.simulate`` call with host buffers.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+STEPS_PER_SIM_S = 10_000  # dt = 0.1 ms
+STEPS_PER_BENCH_STEP = STEPS_PER_SIM_S  # --sim-ms changes the simulated time per bench step
+METRIC = "Brunel-12.5k real-time factor & synaptic events/s, FP32 vs FP64 path, 1 B200"
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9 and parts[1].isdigit():
+                    rows.append(parts)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [int(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v == "Active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": int(rows[0][2]),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def out_degree(pl, p):
+    N = p["NE"] + p["NI"]
+    deg = np.zeros(N, np.int64)
+    offs = [0, p["NE"]]
+    for j in range(4):
+        indptr, _, _, _ = pl.csr(j)
+        pre = 0 if j < 2 else 1
+        deg[offs[pre]:offs[pre] + indptr.size - 1] += np.diff(indptr)
+    return deg
+
+
+def time_runs(pl, n_runs, stream, flush):
+    import torch
+    times, spikes, events = [], 0, 0
+    for _ in range(n_runs):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        pl.run(STEPS_PER_BENCH_STEP, stream=stream.cuda_stream)
+        e1.record(stream)
+        flush.zero_()  # write 256 MiB > L2 between timed iterations
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        st, g = pl.spikes()
+        spikes += st.size
+        events += int(pl._deg[g].sum())
+    return times, spikes, events
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from brainpy.state_b200 import brunel
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    pl, p = brunel.build_plan(order=2500, precision=32, seed=1234 + rank)
+    pl._deg = out_degree(pl, p)
+    N = p["NE"] + p["NI"]
+    time_runs(pl, args.warmup, stream, flush)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        times, nspk, nev = time_runs(pl, args.steps, stream, flush)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    ms_step = sum(times) / len(times)
+    if world > 1:
+        t = torch.tensor([ms_step], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    sim_ms = STEPS_PER_BENCH_STEP * 0.1
+    rtf = world * sim_ms / ms_step
+    syn_ev_s = world * (nev / args.steps) / (ms_step / 1000.0)
+    rate_hz = nspk / args.steps / N
+    drive_ev_s = world * N * p["rate"] / (ms_step / 1000.0)
+    kms, launches = pl.kernel_time()
+
+    # roofline of the persistent kernel: algorithmic bytes per launch
+    # (64 B/neuron/time step: 7 FP32 state words read+written and the ring
+    # slot read+clear; 16 B per synaptic event: packed edge + weight read and
+    # the 4 B red.add read-modify-write; 8 B per spiking row: indptr pair)
+    ev_launch = nev / args.steps
+    spk_launch = nspk / args.steps
+    alg_bytes = 64.0 * N * STEPS_PER_BENCH_STEP + 16.0 * ev_launch + 8.0 * spk_launch
+    peak, peak_kind = _peaks()
+    achieved = alg_bytes / (ms_step / 1000.0) / 1e9
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traffic_k_lif_fast.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            traffic = json.load(f).get("bytes_per_launch")
+
+    result = {
+        "metric": METRIC, "value": round(rtf, 3), "unit": "x real time (simulated s / wall s)",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Brunel network)",
+        "config": {"workload": "brunel_order2500_per_edge_delay_1.0-3.0ms", "N": N,
+                   "CE": p["CE"], "CI": p["CI"], "edges": int(pl._deg.sum()),
+                   "delays_steps": [10, 30], "dt_ms": 0.1,
+                   "step": f"{sim_ms:.0f} ms simulated ({STEPS_PER_BENCH_STEP} time steps)",
+                   "l2": "flushed between timed iterations (256 MiB write)",
+                   "parallelism": f"replicas{world}"},
+        "syn_events_per_s": round(syn_ev_s, 1), "drive_events_per_s": round(drive_ev_s, 1),
+        "rate_hz": round(rate_hz / (sim_ms / 1000.0), 3),
+        "ms_per_time_step": round(ms_step / STEPS_PER_BENCH_STEP, 6),
+        "wall_s_timed": round(wall, 4),
+        "gpu_launches": int(args.steps) * 1,
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
+                     "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "peak_kind": peak_kind, "kernel": "k_lif_fast<float>"},
+        "clocks": clk.summary(),
+    }
+    del pl
+    if rank == 0 and not args.quick:
+        result["fp64"] = fp64_numbers(args, stream, flush)
+        result["e2e"] = e2e_numbers(args)
+        result["cpu_baseline"] = cpu_baseline(args)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+def fp64_numbers(args, stream, flush):
+    from brainpy.state_b200 import brunel
+    pl, p = brunel.build_plan(order=2500, precision=64, seed=1234)
+    pl._deg = out_degree(pl, p)
+    time_runs(pl, 1, stream, flush)
+    k = max(2, args.steps // 3)
+    times, nspk, nev = time_runs(pl, k, stream, flush)
+    ms = sum(times) / len(times)
+    sim_ms = STEPS_PER_BENCH_STEP * 0.1
+    return {"path": "FP64 state/ring/weights, atomic delivery", "rtf": round(sim_ms / ms, 3),
+            "ms_per_step": round(ms, 4), "syn_events_per_s": round(nev / k / (ms / 1000.0), 1),
+            "rate_hz": round(nspk / k / (p["NE"] + p["NI"]) / (sim_ms / 1000.0), 3)}
+
+
+def e2e_numbers(args):
+    """Same metric through the public Simulator API, host buffers in the loop:
+    every step is ``sim.simulate(1000 ms)`` = re-initialise state from the host
+    (h2d), run, read back 50+50 recorded spike trains and 100 V_m traces (d2h)."""
+    import torch
+    from brainpy.state_b200 import (Simulator, Uniform, fixed_indegree, all_to_all,
+                                    iaf_psc_alpha, poisson_generator, spike_recorder,
+                                    voltmeter)
+    from brainpy.state_b200 import brunel
+    from brainpy.state_b200.units import Hz, ms, mV, pA, pF
+    p = brunel.brunel_params(2500)
+    sim = Simulator(dt=0.1 * ms, precision=32, delivery="nest")
+    npar = dict(C_m=250.0 * pF, tau_m=20.0 * ms, tau_syn_ex=0.5 * ms, tau_syn_in=0.5 * ms,
+                t_ref=2.0 * ms, E_L=0.0 * mV, V_reset=10.0 * mV, V_th=20.0 * mV,
+                V_initializer=Uniform(0.0 * mV, 20.0 * mV))
+    ne = sim.create(iaf_psc_alpha, p["NE"], params=npar)
+    ni = sim.create(iaf_psc_alpha, p["NI"], params=npar)
+    noise = sim.create(poisson_generator, rate=p["rate"] * Hz)
+    esr, isr = sim.create(spike_recorder), sim.create(spike_recorder)
+    vm = sim.create(voltmeter)
+    sim.connect(noise, ne, weight=p["J_ex"] * pA, delay=1.5 * ms, rule=all_to_all)
+    sim.connect(noise, ni, weight=p["J_ex"] * pA, delay=1.5 * ms, rule=all_to_all)
+    d = Uniform(0.95 * ms, 3.05 * ms)
+    sim.connect(ne, ne + ni, weight=p["J_ex"] * pA, delay=d, rule=fixed_indegree(p["CE"]), seed=1)
+    sim.connect(ni, ne + ni, weight=p["J_in"] * pA, delay=d, rule=fixed_indegree(p["CI"]), seed=2)
+    sim.connect(ne[:50], esr)
+    sim.connect(ni[:50], isr)
+    sim.connect(vm, ne[:100])
+    sim.simulate(1000.0 * ms)  # build + warm-up
+    k = max(2, args.steps // 2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for _ in range(k):
+        res = sim.simulate(1000.0 * ms)
+        h2d += sim._ck0.nbytes
+        d2h += res.spikes(esr).nbytes + res.spikes(isr).nbytes + res.trace(vm).nbytes
+    wall = (time.perf_counter() - t0) / k
+    return {"value": round(1.0 / wall, 3), "unit": "x real time (simulated s / wall s)",
+            "h2d_bytes_per_step": int(h2d // k), "d2h_bytes_per_step": int(d2h // k),
+            "api": "Simulator.simulate(1000 ms)", "rate_hz_E": round(res.rate(esr), 3)}
+
+
+def _oracle_network(pl_builder_seed=1234, precision=32):
+    """The bench network rebuilt in the float64 oracle (same CSR, drives)."""
+    from oracle import oracle as O
+    from brainpy.state_b200 import brunel
+    pl, p = brunel.build_plan(order=2500, precision=precision, seed=pl_builder_seed, rec_v=0)
+    sim = O.OracleSim(0.1, "iaf_psc_alpha", semantics=O.RING)
+    e = sim.add_pop(p["NE"], p["neuron"])
+    i = sim.add_pop(p["NI"], p["neuron"])
+    sim.add_drive(e, p["rate"], p["J_ex"], 15, brunel.derive_seed(pl_builder_seed, 0))
+    sim.add_drive(i, p["rate"], p["J_ex"], 15, brunel.derive_seed(pl_builder_seed, 1))
+    for j, (pre, post) in enumerate(((0, 0), (0, 1), (1, 0), (1, 1))):
+        indptr, post_l, d, w = pl.csr(j)
+        sim.add_proj(pre, post, indptr, post_l, w, d)
+    sim.set_state(e, "V_m", pl.get_state(0, "V_m"))
+    sim.set_state(i, "V_m", pl.get_state(1, "V_m"))
+    del pl
+    return sim, p
+
+
+def cpu_baseline(args, sample_ms=200.0):
+    """float64 oracle (single thread) on a bounded sample of the workload."""
+    sim, p = _oracle_network()
+    n = int(sample_ms / 0.1)
+    t0 = time.perf_counter()
+    sim.run(n, cap=5_000_000)
+    wall = time.perf_counter() - t0
+    return {"value": round((sample_ms / 1000.0) / wall, 5), "unit": "x real time",
+            "cores": 1, "kind": "port",
+            "sample": f"{sample_ms:.0f} ms simulated ({n} steps) of the same network, float64 "
+                      "oracle, one thread"}
+
+
+def run_reference(args):
+    """CPU reference arm: the float64 restatement of the reference's step
+    (oracle port), timed on the host; rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sim, p = _oracle_network()
+    sample_ms = 50.0
+    n = int(sample_ms / 0.1)
+    for _ in range(args.warmup):
+        sim.run(n, cap=5_000_000)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        sim.run(n, cap=5_000_000)
+        times.append(time.perf_counter() - t0)
+    wall = sum(times) / len(times)
+    rtf = (sample_ms / 1000.0) / wall
+    res = {"impl": "reference", "metric": METRIC, "value": round(rtf, 5),
+           "unit": "x real time (simulated s / wall s)", "n_gpus": int(args.gpus),
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(wall * 1000, 3),
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded Brunel network)",
+           "config": {"workload": "brunel_order2500_per_edge_delay_1.0-3.0ms",
+                      "step": f"{sample_ms:.0f} ms simulated (bounded sample)"},
+           "cpu_baseline": {"value": round(rtf, 5), "unit": "x real time", "cores": 1,
+                            "kind": "port",
+                            "sample": f"{sample_ms:.0f} ms simulated per step, float64 "
+                                      "oracle restatement, one thread (the reference is "
+                                      "JAX, not installable here)"},
+           "e2e": {"value": round(rtf, 5), "unit": "x real time (simulated s / wall s)",
+                   "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(res), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--quick", action="store_true", help="FP32 headline only")
+    ap.add_argument("--sim-ms", type=float, default=1000.0,
+                    help="simulated time per bench step (default one second)")
+    args = ap.parse_args()
+    global STEPS_PER_BENCH_STEP
+    STEPS_PER_BENCH_STEP = int(round(args.sim_ms / 0.1))
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

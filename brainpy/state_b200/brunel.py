@@ -1,0 +1,81 @@
+"""Brunel (2000) balanced-network builders used by the benchmark and examples.
+
+Parameters follow the reference's Brunel script (``examples/nest_like/
+brunel_alpha.py:32-69`` and ``benchmarks/brunel_simulator_baseline.py:63-131``):
+tau_syn 0.5 ms, tau_m 20 ms, C_m 250 pF, theta 20 mV, t_ref 2 ms, g = 5,
+eta = 2, epsilon = 0.1, J = 0.1 mV PSP amplitude.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import _lib
+
+
+def psp_norm(tau_mem, c_mem, tau_syn):
+    """Peak PSP of a 1 pA alpha current (brunel_alpha.py:32-38)."""
+    from scipy.special import lambertw
+    a = tau_mem / tau_syn
+    b = 1.0 / tau_syn - 1.0 / tau_mem
+    x = -math.exp(-1.0 / a) / a
+    lw = lambertw(x, k=-1 if x < 0 else 0).real
+    t_max = 1.0 / b * (-lw - 1.0 / a)
+    return (math.exp(1.0) / (tau_syn * c_mem * b)
+            * ((math.exp(-t_max / tau_mem) - math.exp(-t_max / tau_syn)) / b
+               - t_max * math.exp(-t_max / tau_syn)))
+
+
+def brunel_params(order, g=5.0, eta=2.0, epsilon=0.1, J=0.1, V_reset=10.0):
+    tau_syn, tau_mem, c_mem, theta, t_ref = 0.5, 20.0, 250.0, 20.0, 2.0
+    NE, NI = 4 * order, order
+    CE, CI = int(epsilon * NE), int(epsilon * NI)
+    j_ex = J / psp_norm(tau_mem, c_mem, tau_syn)
+    nu_th = (theta * c_mem) / (j_ex * CE * math.e * tau_mem * tau_syn)
+    rate = 1000.0 * (eta * nu_th) * CE
+    neuron = [0.0, c_mem, tau_mem, t_ref, theta, V_reset, tau_syn, tau_syn, 0.0, -math.inf]
+    return dict(NE=NE, NI=NI, CE=CE, CI=CI, J_ex=j_ex, J_in=-g * j_ex, rate=rate,
+                neuron=neuron, g=g, eta=eta)
+
+
+def derive_seed(base, ordinal):
+    return ((0 if base is None else int(base)) * 1_000_003 + ordinal + 1) & 0x7FFFFFFF
+
+
+def build_plan(order=2500, precision=32, delay_steps=(10, 30), noise_delay=15, seed=1234,
+               semantics=_lib.RING, deterministic=False, rec_v=100, spike_capacity=1 << 23,
+               v_init=(0.0, 20.0), g=5.0, eta=2.0):
+    """Brunel network in one plan.  ``delay_steps``: an int (homogeneous) or a
+    (lo, hi) pair of per-edge delays drawn uniformly on the step grid."""
+    p = brunel_params(order, g=g, eta=eta)
+    pl = _lib.Plan(0.1, "iaf_psc_alpha", precision=precision, semantics=semantics,
+                   deterministic=deterministic, spike_capacity=spike_capacity)
+    e = pl.add_pop(p["NE"], p["neuron"])
+    i = pl.add_pop(p["NI"], p["neuron"])
+    # creation order as in the reference script: noise -> E, noise -> I,
+    # E -> E+I (seed 1), I -> E+I (seed 2)
+    pl.add_poisson(e, p["rate"], p["J_ex"], noise_delay, derive_seed(seed, 0))
+    pl.add_poisson(i, p["rate"], p["J_ex"], noise_delay, derive_seed(seed, 1))
+    rng = np.random.default_rng(seed)
+    nbits = 64 if precision == 64 else 32
+    ordinal = 2
+    for pre, K, w, s in ((e, p["CE"], p["J_ex"], 1), (i, p["CI"], p["J_in"], 2)):
+        for post in (e, i):
+            n_post = p["NE"] if post == e else p["NI"]
+            if isinstance(delay_steps, tuple):
+                d = rng.integers(delay_steps[0], delay_steps[1] + 1, size=K * n_post)
+                pl.add_fixed_indegree(pre, post, K, derive_seed(s, ordinal), w,
+                                      delay_steps=d.astype(np.int32), nbits=nbits)
+            else:
+                pl.add_fixed_indegree(pre, post, K, derive_seed(s, ordinal), w,
+                                      delay_const=int(delay_steps), nbits=nbits)
+            ordinal += 1
+    N = p["NE"] + p["NI"]
+    if rec_v:
+        pl.record_v(np.linspace(0, N - 1, rec_v).astype(np.int32))
+    pl.upload()
+    vr = np.random.default_rng(seed + 7)
+    pl.set_state(e, "V_m", vr.uniform(v_init[0], v_init[1], p["NE"]))
+    pl.set_state(i, "V_m", vr.uniform(v_init[0], v_init[1], p["NI"]))
+    return pl, p

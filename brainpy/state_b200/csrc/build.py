@@ -25,6 +25,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3",
 SOURCES = {
     "plan.cpp": [],
     "lif_fast.cu": [],
+    "lif_tiled.cu": [],
     "lif_exact.cu": ["-fmad=false"],
     "per_step.cu": [],
     "batch.cu": [],

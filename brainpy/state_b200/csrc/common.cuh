@@ -43,12 +43,60 @@ __device__ __forceinline__ double uniform01(uint32_t seed, uint32_t stream, uint
     return static_cast<double>(b >> 11) * 0x1.0p-53;
 }
 
-// Smallest k with u <= F[k]; the table ends where the CDF stops growing.
-__device__ __forceinline__ int poisson_from_table(const double *F, int n, double u) {
+// The same draw as an integer: b53 = top 53 bits, u = b53 * 2^-53.
+__device__ __forceinline__ uint64_t bits53(uint32_t seed, uint32_t stream, uint32_t step,
+                                           uint32_t idx) {
+    uint32_t y0, y1;
+    threefry2x32(seed, stream, step, idx, y0, y1);
+    return ((static_cast<uint64_t>(y0) << 32) | y1) >> 11;
+}
+
+// Smallest k with u <= F[k] (table length if none).  The table holds the CDF
+// as integer thresholds T[k] = floor(F[k] * 2^53), so u <= F[k] is exactly
+// b53 <= T[k]: no floating point in the search.
+__device__ __forceinline__ int poisson_from_table(const uint64_t *T, int n, uint64_t b53) {
     int k = 0;
-    while (k < n - 1 && u > F[k]) ++k;
-    if (u > F[k]) ++k;  // beyond the table (probability < 1e-16)
+    while (k < n && b53 > T[k]) ++k;
     return k;
+}
+
+// Split-phase grid barrier over a monotonically increasing arrival counter
+// that the host zeroes before each launch (`epoch` is 1-based): arrive, do
+// independent work, then wait.  The wait gives up after 2 s of globaltimer,
+// raises the error flag and returns false instead of hanging.
+__device__ __forceinline__ void grid_arrive(unsigned int *counter) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(counter, 1u);
+    }
+}
+
+__device__ __forceinline__ bool grid_wait(unsigned int *counter, unsigned int epoch, int *err) {
+    __shared__ int timed_out_w;
+    if (threadIdx.x == 0) {
+        timed_out_w = 0;
+        const unsigned int target = epoch * gridDim.x;
+        uint64_t t0;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+        unsigned int seen;
+        while (true) {
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(seen) : "l"(counter) : "memory");
+            if (seen >= target) break;
+            if (*(volatile int *)err) { timed_out_w = 1; break; }
+            uint64_t t1;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
+            if (t1 - t0 > 2000000000ull) {  // 2 s
+                atomicExch(err, BSPK_DEV_ERR_TIMEOUT);
+                timed_out_w = 1;
+                break;
+            }
+            __nanosleep(20);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return timed_out_w == 0;
 }
 
 // Bounded grid barrier over a monotonically increasing arrival counter that

@@ -20,7 +20,7 @@ struct LifArgs {
                                                 // (>= 0 projection, < 0 drive -(id+1))
     const DriveDev *drives;
     const int *pop_drive_ptr, *pop_drive_list;  // drives per post pop
-    const double *cdf;
+    const uint64_t *cdf;  // Poisson CDF thresholds floor(F * 2^53)
     int cdf_total;
     int64_t step0, n_steps, run_step0;
     int W;
@@ -38,6 +38,55 @@ struct LifArgs {
     unsigned int *barrier;
     int *err;
 };
+
+// Target-partitioned delivery structures of the tiled kernel: for every CTA
+// c a CSR over all pre neurons of the edges that target c's tile,
+// ptr[c * (N + 1) + pre] .. ptr[c * (N + 1) + pre + 1] into `edges` (edge
+// word = post_in_tile | lag << 16 | projection << 24); per-window spike
+// records list[2][G][kRecWords] (tagged count word + kRecInline tagged
+// entries) with an overflow area ovf[2][G][list_cap]; per-CTA spike-record
+// counts rec_count[G].
+constexpr int kRecWords = 16;
+constexpr int kRecInline = kRecWords - 1;
+
+template <typename Real>
+struct TiledArgs {
+    const int *ptr;
+    const uint32_t *edges;
+    const Real *w;  // per-edge weights, or nullptr when every projection is homogeneous
+    uint32_t *list;
+    uint32_t *ovf;
+    long long *rec_count;
+    int list_cap;
+    int smem_ptr;   // 1: the tile's CSR bounds are staged in shared memory
+};
+
+struct TiledLayout {
+    size_t coef, drive, proj, cdf, ring, drv, spk, ptr, total;
+};
+__host__ __device__ inline TiledLayout tiled_layout(size_t coef_sz, size_t proj_sz, size_t real_sz,
+                                                    int npop, int ndrive, int nproj, int cdf_total,
+                                                    int tile, int L, int G, int n_ptr) {
+    auto al = [](size_t x) { return (x + 15) & ~size_t(15); };
+    (void)G;
+    TiledLayout l;
+    l.coef = 0;
+    l.drive = al(l.coef + coef_sz * npop);
+    l.proj = al(l.drive + sizeof(DriveDev) * ndrive);
+    l.cdf = al(l.proj + proj_sz * nproj);
+    l.ring = al(l.cdf + sizeof(uint64_t) * cdf_total);
+    l.drv = al(l.ring + real_sz * static_cast<size_t>(L) * tile);
+    l.spk = al(l.drv + real_sz * static_cast<size_t>(kMaxWindow) * tile);
+    l.ptr = al(l.spk + sizeof(uint32_t) * static_cast<size_t>(tile) * kMaxWindow);
+    l.total = al(l.ptr + sizeof(int) * static_cast<size_t>(n_ptr));
+    return l;
+}
+
+template <typename Real>
+cudaError_t launch_lif_tiled(const LifArgs<Real> &a, const TiledArgs<Real> &t2, int grid,
+                             cudaStream_t st);
+size_t lif_tiled_smem(int tile, int L, int G, int N, int npop, int ndrive, int nproj,
+                      int cdf_total, bool dbl, bool smem_ptr);
 
 // Launchers (cooperative, persistent).  Return the cudaError_t of the launch.
 template <typename Real>

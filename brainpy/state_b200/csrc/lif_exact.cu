@@ -27,7 +27,7 @@ __global__ void __launch_bounds__(256) k_lif_exact(const LifArgs<double> a) {
     PopCoef<double> *s_coef = reinterpret_cast<PopCoef<double> *>(smem_raw + lay.coef);
     DriveDev *s_drive = reinterpret_cast<DriveDev *>(smem_raw + lay.drive);
     ProjDev<double> *s_proj = reinterpret_cast<ProjDev<double> *>(smem_raw + lay.proj);
-    double *s_cdf = reinterpret_cast<double *>(smem_raw + lay.cdf);
+    uint64_t *s_cdf = reinterpret_cast<uint64_t *>(smem_raw + lay.cdf);
     double *ybuf = reinterpret_cast<double *>(smem_raw + lay.total);  // [kMaxWindow][block]
 
     const int tid = threadIdx.x, B = blockDim.x;
@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(256) k_lif_exact(const LifArgs<double> a) {
                             const int64_t se = n0 + k - d.lag;
                             double y = 0.0;
                             if (d.tmin < se && se <= d.tmax) {
-                                const double u = uniform01(d.seed, 0u, static_cast<uint32_t>(se),
+                                const uint64_t u = bits53(d.seed, 0u, static_cast<uint32_t>(se),
                                                            static_cast<uint32_t>(gl));
                                 const int cnt = poisson_from_table(s_cdf + d.cdf_off, d.cdf_n, u);
                                 y = static_cast<double>(cnt) * d.weight;

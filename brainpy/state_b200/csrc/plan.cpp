@@ -566,6 +566,72 @@ int upload_coef(bspk_plan *p) {
     return rc;
 }
 
+// Per-CTA CSR of the edges that target each tile, for the tiled kernel:
+// ptr[c * (N + 1) + pre] .. ptr[c * (N + 1) + pre + 1] into `edges`, edge
+// word post_in_tile | lag << 16 | projection << 24, weights in the same
+// order when any projection is heterogeneous.  Rows of a CTA are all pre
+// neurons, so the bounds of a spike's segment are one shared-memory read.
+int build_tiled(bspk_plan *p) {
+    const int G = p->grid, tile = p->tile, N = p->N;
+    const size_t rows = static_cast<size_t>(G) * (N + 1);
+    std::vector<int> ptr(rows + 1, 0);
+    bool hetero = false;
+    int64_t total = 0;
+    for (auto &J : p->projs) {
+        hetero |= !J.homogeneous;
+        const int pre_off = p->pops[J.pre].off, post_off = p->pops[J.post].off;
+        for (int i = 0; i < p->pops[J.pre].n; ++i)
+            for (int64_t e = J.indptr[i]; e < J.indptr[i + 1]; ++e) {
+                const int c = (post_off + J.post_local[e]) / tile;
+                ptr[static_cast<size_t>(c) * (N + 1) + pre_off + i + 1]++;
+            }
+        total += static_cast<int64_t>(J.post_local.size());
+    }
+    if (total >= (int64_t(1) << 31)) return fail(BSPK_ERR_UNSUPPORTED, "more than 2^31 edges");
+    for (size_t i = 0; i < rows; ++i) ptr[i + 1] += ptr[i];
+    std::vector<int> fill(ptr.begin(), ptr.end() - 1);
+    std::vector<uint32_t> edges(total);
+    std::vector<double> w(hetero ? total : 0);
+    for (size_t j = 0; j < p->projs.size(); ++j) {
+        const Proj &J = p->projs[j];
+        const int pre_off = p->pops[J.pre].off, post_off = p->pops[J.post].off;
+        for (int i = 0; i < p->pops[J.pre].n; ++i)
+            for (int64_t e = J.indptr[i]; e < J.indptr[i + 1]; ++e) {
+                const int post = post_off + J.post_local[e];
+                const int c = post / tile;
+                const int q = fill[static_cast<size_t>(c) * (N + 1) + pre_off + i]++;
+                edges[q] = static_cast<uint32_t>(post - c * tile) |
+                           (static_cast<uint32_t>(lag_of(p, J.delay[e])) << 16) |
+                           (static_cast<uint32_t>(j) << 24);
+                if (hetero) w[q] = J.w[e];
+            }
+    }
+    ptr.pop_back();
+    int rc = upload_vec(p, &p->d_tptr, ptr);
+    if (!rc) rc = upload_vec(p, &p->d_tedges, edges);
+    if (rc) return rc;
+    if (hetero) {
+        if (p->elt == 8) {
+            double *dw = nullptr;
+            rc = upload_vec(p, &dw, w);
+            p->d_tw = dw;
+        } else {
+            std::vector<float> f(w.begin(), w.end());
+            float *dw = nullptr;
+            rc = upload_vec(p, &dw, f);
+            p->d_tw = dw;
+        }
+        if (rc) return rc;
+    }
+    p->list_cap = tile * kMaxWindow;
+    rc = dalloc(p, &p->d_tlist, static_cast<size_t>(2) * G * kRecWords);
+    if (!rc) rc = dalloc(p, &p->d_tovf, static_cast<size_t>(2) * G * p->list_cap);
+    if (!rc) rc = dalloc(p, &p->d_trec, static_cast<size_t>(G));
+    if (rc) return rc;
+    BSPK_CUDA(cudaMemset(p->d_trec, 0, sizeof(long long) * G));
+    return BSPK_OK;
+}
+
 }  // namespace
 
 extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
@@ -643,7 +709,9 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
 
     // drives and CDF tables
     std::vector<DriveDev> dd;
-    std::vector<double> cdf;
+    // CDF tables as integer thresholds floor(F * 2^53): for a 53-bit uniform
+    // b * 2^-53, u <= F[k] holds exactly when b <= floor(F[k] * 2^53).
+    std::vector<uint64_t> cdf;
     for (auto &D : p->drives) {
         DriveDev d{};
         d.pop = D.post;
@@ -655,7 +723,7 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
         d.weight = D.weight;
         d.tmin = D.tmin;
         d.tmax = D.tmax;
-        cdf.insert(cdf.end(), D.cdf.begin(), D.cdf.end());
+        for (double F : D.cdf) cdf.push_back(static_cast<uint64_t>(std::floor(std::ldexp(F, 53))));
         dd.push_back(d);
     }
     p->cdf_total = static_cast<int>(cdf.size());
@@ -716,12 +784,36 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
 
     // launch geometry of the persistent kernels: one CTA per SM when the
     // network is small, so every SM takes part in delivery.
-    int block = ((p->N + p->sm_count - 1) / p->sm_count + 31) / 32 * 32;
-    block = std::max(64, std::min(block, exact ? 256 : 512));
-    int grid = (p->N + block - 1) / block;
-    p->block = block;
-    p->grid = grid;
-    p->tile = block;
+    if (exact) {
+        int block = ((p->N + p->sm_count - 1) / p->sm_count + 31) / 32 * 32;
+        block = std::max(64, std::min(block, 256));
+        p->block = block;
+        p->grid = (p->N + block - 1) / block;
+        p->tile = block;
+    } else {
+        // fast path: one 256-thread CTA per SM, a contiguous tile of neurons each
+        p->block = 256;
+        p->grid = std::max(1, std::min(p->sm_count, (p->N + 31) / 32));
+        p->tile = (p->N + p->grid - 1) / p->grid;
+        if (static_cast<size_t>(p->tile) * p->W * 4 > 160 * 1024)
+            return fail(BSPK_ERR_UNSUPPORTED, "network too large for the persistent kernel tile");
+    }
+    for (auto &J : p->projs)
+        if (J.post_local.size() >= (size_t(1) << 31))
+            return fail(BSPK_ERR_UNSUPPORTED, "projection with >= 2^31 edges");
+    // tiled (target-partitioned) path: state in registers, ring in shared memory
+    p->tiled = false;
+    if (!exact && !aeif && !plastic && p->tile <= 256 && p->grid <= 160 &&
+        lif_tiled_smem(p->tile, p->L, p->grid, p->N, npop, static_cast<int>(p->drives.size()),
+                       static_cast<int>(p->projs.size()), p->cdf_total, dbl, false) <= 200 * 1024) {
+        rc = build_tiled(p);
+        if (rc) return rc;
+        p->tiled = true;
+        p->smem_ptr = lif_tiled_smem(p->tile, p->L, p->grid, p->N, npop,
+                                     static_cast<int>(p->drives.size()),
+                                     static_cast<int>(p->projs.size()), p->cdf_total, dbl,
+                                     true) <= 200 * 1024;
+    }
     p->uploaded = true;
     p->step = 0;
     return BSPK_OK;
@@ -806,12 +898,30 @@ extern "C" int bspk_run(bspk_plan *p, int64_t n_steps, void *stream) {
     cudaError_t e = cudaSuccess;
     bool per_step = p->cfg.model == BSPK_AEIF_COND_ALPHA;
     for (auto &J : p->projs) per_step |= J.plastic;
+    if (p->tiled) {
+        // records of an earlier run must never carry a tag of this one
+        BSPK_CUDA(cudaMemsetAsync(p->d_tlist, 0, sizeof(uint32_t) * 2 * p->grid * kRecWords, st));
+        BSPK_CUDA(cudaMemsetAsync(p->d_tovf, 0,
+                                  sizeof(uint32_t) * 2 * static_cast<size_t>(p->grid) * p->list_cap, st));
+    }
     if (per_step) {
         int rc = run_per_step(p, n_steps, st);
         if (rc) return rc;
     } else if (p->cfg.deterministic) {
         LifArgs<double> a = lif_args<double>(p, n_steps);
         e = launch_lif_exact(a, p->grid, p->block, st);
+        p->last_launches = 1;
+    } else if (p->tiled && dbl) {
+        LifArgs<double> a = lif_args<double>(p, n_steps);
+        TiledArgs<double> t2{p->d_tptr, p->d_tedges, static_cast<const double *>(p->d_tw),
+                             p->d_tlist, p->d_tovf, p->d_trec, p->list_cap, p->smem_ptr ? 1 : 0};
+        e = launch_lif_tiled<double>(a, t2, p->grid, st);
+        p->last_launches = 1;
+    } else if (p->tiled) {
+        LifArgs<float> a = lif_args<float>(p, n_steps);
+        TiledArgs<float> t2{p->d_tptr, p->d_tedges, static_cast<const float *>(p->d_tw),
+                            p->d_tlist, p->d_tovf, p->d_trec, p->list_cap, p->smem_ptr ? 1 : 0};
+        e = launch_lif_tiled<float>(a, t2, p->grid, st);
         p->last_launches = 1;
     } else if (dbl) {
         LifArgs<double> a = lif_args<double>(p, n_steps);
@@ -848,6 +958,39 @@ int bspk_spikes_get(bspk_plan *p, int64_t cap, int64_t *steps, int32_t *gids, in
     if (!p || !p->uploaded || !n_out) return fail(BSPK_ERR_ARG, "bad arguments");
     int rc = sync_and_check(p);
     if (rc) return rc;
+    if (p->tiled) {
+        // per-CTA regions of spike_capacity / G entries each
+        const int G = p->grid;
+        const int64_t region = p->cfg.spike_capacity / G;
+        std::vector<long long> counts(G);
+        BSPK_CUDA(cudaMemcpy(counts.data(), p->d_trec, sizeof(long long) * G, cudaMemcpyDeviceToHost));
+        int64_t m = 0, total = 0;
+        for (int c = 0; c < G; ++c) {
+            total += counts[c];
+            if (counts[c] > region) {
+                *n_out = total;
+                return fail(BSPK_ERR_OVERFLOW, "spike record overflowed its device capacity");
+            }
+        }
+        std::vector<int64_t> s;
+        std::vector<int32_t> g;
+        for (int c = 0; c < G && m < cap; ++c) {
+            const int64_t k = counts[c];
+            if (k == 0) continue;
+            s.resize(k);
+            g.resize(k);
+            BSPK_CUDA(cudaMemcpy(s.data(), p->d_spk_step + c * region, 8 * k, cudaMemcpyDeviceToHost));
+            BSPK_CUDA(cudaMemcpy(g.data(), p->d_spk_gid + c * region, 4 * k, cudaMemcpyDeviceToHost));
+            for (int64_t i = 0; i < k && m < cap; ++i) {
+                if (g[i] < 0) continue;  // unrecorded neuron
+                steps[m] = s[i];
+                gids[m] = g[i];
+                ++m;
+            }
+        }
+        *n_out = m;
+        return BSPK_OK;
+    }
     unsigned long long cnt = 0;
     BSPK_CUDA(cudaMemcpy(&cnt, p->d_spk_count, sizeof(cnt), cudaMemcpyDeviceToHost));
     if (static_cast<int64_t>(cnt) > p->cfg.spike_capacity) {

@@ -83,7 +83,7 @@ struct bspk_plan {
     void *d_coef = nullptr;
     void *d_projs = nullptr;
     bspk::DriveDev *d_drives = nullptr;
-    double *d_cdf = nullptr;
+    uint64_t *d_cdf = nullptr;
     int cdf_total = 0;
     int *d_pop_out_ptr = nullptr, *d_pop_out_list = nullptr;
     int *d_pop_in_ptr = nullptr, *d_pop_in_list = nullptr;
@@ -108,6 +108,16 @@ struct bspk_plan {
     int64_t last_launches = 0;
     int grid = 0, block = 0, tile = 0;
     int sm_count = 0;
+    // tiled (target-partitioned) fast path
+    bool tiled = false;
+    int *d_tptr = nullptr;
+    uint32_t *d_tedges = nullptr;
+    void *d_tw = nullptr;
+    uint32_t *d_tlist = nullptr;   // spike records [2][G][kRecWords]
+    uint32_t *d_tovf = nullptr;    // record overflow [2][G][list_cap]
+    long long *d_trec = nullptr;   // per-CTA spike-record counts
+    int list_cap = 0;
+    bool smem_ptr = false;
 };
 
 namespace bspk {
