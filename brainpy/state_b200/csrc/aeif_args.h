@@ -1,12 +1,63 @@
-// aeif_args.h -- per-step engine (aeif_cond_alpha RKF45 and plastic
-// projections): launched step by step from the host loop.
+// aeif_args.h -- per-step engine: aeif_cond_alpha (adaptive RKF45) and
+// networks with plastic (stdp_synapse) projections.  One step is a short
+// sequence of kernels, replayed through a CUDA graph; the step index lives
+// in device memory (advanced by the last kernel of the step), so the same
+// graph serves every chunk of steps.
 #pragma once
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
+#include "device_types.h"
+
 struct bspk_plan;
 
 namespace bspk {
+
+template <typename Real>
+struct StepArgs {
+    int N, npop, nproj, ndrive, model, R, L;
+    const PopCoef<Real> *coef;
+    Real *s[8];
+    int *r;
+    Real *ring;  // [L][R][N]
+    const ProjDev<Real> *projs;
+    const int *proj_plastic;  // 1 for plastic projections (delivered by the STDP kernels)
+    const DriveDev *drives;
+    const int *pop_drive_ptr, *pop_drive_list;
+    const uint64_t *cdf;
+    uint64_t *hist;       // spike history word per neuron (bit m & 63)
+    uint32_t *step_spk;   // spikes of the current step (gids)
+    int *step_nspk;
+    int64_t *spk_step;
+    int32_t *spk_gid;
+    unsigned long long *spk_count;
+    int64_t spk_cap;
+    const uint8_t *spk_flag;
+    const int32_t *rec_slot;
+    Real *v_out;
+    int n_rec;
+    int64_t *step_ptr;    // device step counter
+    int64_t run_step0;
+    unsigned long long *rk_iters;
+    int *err;
+};
+
+// One plastic projection (pair STDP, eager substrate).
+struct StdpDev {
+    int pre_off, post_off, n_pre, n_post, lag;  // lag: arrival lag of the pre spike
+    int receptor;
+    double tau_plus, tau_minus, lambda_, alpha, mu_plus, mu_minus, Wmax, dec_pre, dec_post;
+    const int64_t *indptr;   // CSR over pre
+    const uint32_t *edges;   // post_local | lag << 24
+    double *w;               // FP64 weights, CSR order
+    const int64_t *cindptr;  // CSC over post
+    const int64_t *cperm;    // CSC position -> CSR edge id
+    const uint32_t *cedges;  // pre_local | lag << 24
+    double *pre_trace, *post_trace;
+    int *pre_list, *post_list, *counts;  // counts[0] pres, counts[1] posts of this step
+};
+
 int run_per_step(bspk_plan *p, int64_t n_steps, cudaStream_t st);
+
 }  // namespace bspk

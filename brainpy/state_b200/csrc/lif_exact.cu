@@ -9,8 +9,12 @@
 // to the input in creation order (sum_delta_inputs, _base.py:312-382).  The
 // pre spike trains come from a 64-step history word per neuron, so a window of
 // W steps reads each in-edge once.  Requires max_lag + W <= 64.
+#include <mutex>
+#include <vector>
+
 #include "common.cuh"
 #include "lif_args.h"
+#include "plan_internal.h"
 
 namespace bspk {
 

@@ -1,7 +1,514 @@
-// per_step.cu -- per-step engine for aeif_cond_alpha and plastic networks.
-#include "../../../include/bspk.h"
+// per_step.cu -- per-step engine: aeif_cond_alpha with adaptive RKF45, and
+// networks with plastic stdp_synapse projections (any neuron model).
+//
+// One step n is this kernel sequence (the reference Simulator's phase order,
+// _nest_network/simulator.py:1719-1788):
+//   memset of the step's counters;
+//   per plastic projection: traces (decay-then-add), facilitation on the
+//   in-edges of neurons that fired at n-1, depression + delivery on the
+//   out-edges of pres whose delayed spike arrives at n (the order of
+//   _nest_plasticity/stdp_synapse.py:171-179), adding into ring slot n;
+//   neuron update (one neuron per thread; RKF45 per neuron with FP64 error
+//   norm and step control, FP64 exponential term);
+//   static delivery of step n's spikes into ring slots n + lag (warp per row);
+//   step counter += 1.
+// The step index lives in device memory, so a CUDA graph captured over K
+// steps is replayed for every chunk of K steps.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <string>
+#include <vector>
+
 #include "aeif_args.h"
+#include "common.cuh"
+#include "plan_internal.h"
 
 namespace bspk {
-int run_per_step(bspk_plan *, int64_t, cudaStream_t) { return BSPK_ERR_UNSUPPORTED; }
+
+namespace {
+
+template <typename Real>
+__device__ __forceinline__ int find_pop_t(const PopCoef<Real> *c, int npop, int g) {
+    int p = 0;
+    while (p + 1 < npop && c[p + 1].off <= g) ++p;
+    return p;
+}
+
+__device__ __forceinline__ bool fired(const uint64_t *hist, int gid, int64_t m) {
+    if (m < 0) return false;
+    return (hist[gid] >> (m & 63)) & 1ull;
+}
+
+// ------------------------------------------------ aeif_cond_alpha + RKF45
+
+// RKF45 tableau (_nest_base/utils.py:266-279); b_err = b - b_hat.
+__constant__ double kA[6][5] = {
+    {0, 0, 0, 0, 0},
+    {1.0 / 4, 0, 0, 0, 0},
+    {3.0 / 32, 9.0 / 32, 0, 0, 0},
+    {1932.0 / 2197, -7200.0 / 2197, 7296.0 / 2197, 0, 0},
+    {439.0 / 216, -8.0, 3680.0 / 513, -845.0 / 4104, 0},
+    {-8.0 / 27, 2.0, -3544.0 / 2565, 1859.0 / 4104, -11.0 / 40},
+};
+__constant__ double kB[6] = {16.0 / 135, 0.0, 6656.0 / 12825, 28561.0 / 56430, -9.0 / 50, 2.0 / 55};
+__constant__ double kBhat[6] = {25.0 / 216, 0.0, 1408.0 / 2565, 2197.0 / 4104, -1.0 / 5, 0.0};
+
+// Vector field (_nest_neuron/aeif_cond_alpha.py:554-592); the exponential
+// spike current is evaluated in FP64 whatever the state precision.
+template <typename Real>
+__device__ __forceinline__ void aeif_vf(const PopCoef<Real> &c, int r, Real i_stim, const Real *y,
+                                        Real *dy) {
+    const bool refr = r > 0;
+    const Real v = y[0];
+    const Real v_eff = refr ? c.V_reset : (v < c.V_peak ? v : (v != v ? v : c.V_peak));
+    const Real i_ex = y[2] * (v_eff - c.E_ex);
+    const Real i_in = y[4] * (v_eff - c.E_in);
+    const double dts = c.Delta_T == Real(0) ? 1.0 : static_cast<double>(c.Delta_T);
+    double arg = static_cast<double>(v_eff - c.V_th) / dts;
+    arg = arg < -500.0 ? -500.0 : (arg > 500.0 ? 500.0 : arg);
+    const Real i_spike =
+        static_cast<Real>(static_cast<double>(c.g_L) * static_cast<double>(c.Delta_T) * exp(arg));
+    const Real dV = (-c.g_L * (v_eff - c.E_L) + i_spike - i_ex - i_in - y[5] + c.I_e + i_stim) / c.C_m;
+    dy[0] = refr ? Real(0) : dV;
+    dy[1] = -y[1] / c.tau_syn_ex;
+    dy[2] = y[1] - y[2] / c.tau_syn_ex;
+    dy[3] = -y[3] / c.tau_syn_in;
+    dy[4] = y[3] - y[4] / c.tau_syn_in;
+    dy[5] = (c.a * (v_eff - c.E_L) - y[5]) / c.tau_w;
+}
+
+// One dt of the adaptive RKF45 loop (_nest_base/utils.py:583-718) with the
+// in-loop spike/reset event (aeif_cond_alpha.py:594-625) and the synaptic
+// jumps after integration (aeif_cond_alpha.py:709-728).  s: V, dg_ex, g_ex,
+// dg_in, g_in, w, h, I_stim.  Returns the spike flag.
+template <typename Real>
+__device__ bool aeif_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Real w_in,
+                          double dt, int *err, unsigned long long *rk_iters) {
+    constexpr double min_h = 1e-8;
+    Real y[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) y[i] = s[i];
+    double h = static_cast<double>(s[6]);
+    const Real i_stim = s[7];
+    const double atol = static_cast<double>(c.atol);
+    bool spiked = false, unstable = false;
+    double t_loc = 0.0;
+    if (h < min_h) h = min_h;
+    int iters = 0;
+    Real k[6][6];
+    while (t_loc < dt && iters < 100000) {
+        const double hh = h < dt - t_loc ? h : dt - t_loc;
+        h = hh > min_h ? hh : min_h;
+        const Real hR = static_cast<Real>(h);
+        for (int st = 0; st < 6; ++st) {
+            Real yi[6];
+            if (st == 0) {
+#pragma unroll
+                for (int i = 0; i < 6; ++i) yi[i] = y[i];
+            } else {
+#pragma unroll
+                for (int i = 0; i < 6; ++i) {
+                    Real acc = Real(0);
+                    bool first = true;
+                    for (int j = 0; j < st; ++j) {
+                        const double aij = kA[st][j];
+                        if (aij == 0.0) continue;
+                        const Real term = static_cast<Real>(aij) * k[j][i];
+                        acc = first ? term : acc + term;
+                        first = false;
+                    }
+                    yi[i] = y[i] + hR * acc;
+                }
+            }
+            aeif_vf<Real>(c, r, i_stim, yi, k[st]);
+        }
+        Real yh[6];
+        double err = 0.0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            Real acc = Real(0), eacc = Real(0);
+            bool first = true, efirst = true;
+#pragma unroll
+            for (int j = 0; j < 6; ++j) {
+                if (kB[j] != 0.0) {
+                    const Real term = static_cast<Real>(kB[j]) * k[j][i];
+                    acc = first ? term : acc + term;
+                    first = false;
+                }
+                const double be = kB[j] - kBhat[j];
+                if (be != 0.0) {
+                    const Real term = static_cast<Real>(be) * k[j][i];
+                    eacc = efirst ? term : eacc + term;
+                    efirst = false;
+                }
+            }
+            yh[i] = y[i] + hR * acc;
+            const Real ye = hR * eacc;
+            const double ay = fabs(static_cast<double>(y[i])) > fabs(static_cast<double>(yh[i]))
+                                  ? fabs(static_cast<double>(y[i]))
+                                  : fabs(static_cast<double>(yh[i]));
+            const double e = fabs(static_cast<double>(ye)) / (atol + 0.0 * ay);
+            err = i == 0 ? e : ((err != err || e != e) ? NAN : (err > e ? err : e));
+        }
+        if (err != err) err = INFINITY;
+        const bool accept = (err <= 1.0) || (h <= min_h);
+        if (accept) {
+#pragma unroll
+            for (int i = 0; i < 6; ++i) y[i] = yh[i];
+            t_loc = t_loc + h;
+            if (y[0] < Real(-1e3) || y[5] < Real(-1e6) || y[5] > Real(1e6)) unstable = true;
+            if (r > 0) y[0] = c.V_reset;
+            if (r <= 0 && y[0] >= c.v_peak_detect) {
+                spiked = true;
+                y[0] = c.V_reset;
+                y[5] = y[5] + c.b;
+                if (c.ref_count > 0) r = c.ref_count + 1;
+            }
+        }
+        const double err_sg = err > 1e-30 ? err : 1e-30;
+        const double inv_err = 1.0 / err_sg;
+        double fac;
+        if (accept) {
+            fac = err_sg <= 1e-30 ? 5.0 : 0.9 * pow(inv_err, 1.0 / 5.0);
+            if (!(err_sg <= 1e-30)) fac = fac < 0.2 ? 0.2 : (fac > 5.0 ? 5.0 : fac);
+        } else {
+            fac = 0.9 * pow(inv_err, 1.0 / 4.0);
+            fac = fac < 0.2 ? 0.2 : (fac > 1.0 ? 1.0 : fac);
+        }
+        const double hn = h * fac;
+        h = hn > min_h ? hn : min_h;
+        ++iters;
+    }
+    if (iters >= 100000 && t_loc < dt) atomicExch(err, BSPK_DEV_ERR_RKCAP);
+    if (unstable) atomicExch(err, BSPK_DEV_ERR_UNSTABLE);
+    atomicAdd(rk_iters, static_cast<unsigned long long>(iters));
+    if (r > 0) r = r - 1;
+    y[1] = y[1] + c.pscon_ex * w_ex;
+    y[3] = y[3] + c.pscon_in * w_in;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) s[i] = y[i];
+    s[6] = static_cast<Real>(h);
+    s[7] = Real(0);  // no current input on this path: I_stim <- 0
+    return spiked;
+}
+
+// ------------------------------------------------------------- kernels
+
+template <typename Real, int MODEL>
+__global__ void __launch_bounds__(128) k_neuron_step(const StepArgs<Real> a, double dt) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= a.N) return;
+    const int64_t n = *a.step_ptr;
+    const int p = find_pop_t(a.coef, a.npop, g);
+    const PopCoef<Real> c = a.coef[p];
+    const int slot = static_cast<int>(n % a.L);
+    Real in[2] = {Real(0), Real(0)};
+    for (int ch = 0; ch < a.R; ++ch) {
+        Real *cell = a.ring + (static_cast<size_t>(slot) * a.R + ch) * a.N + g;
+        in[ch] = *cell;
+        *cell = Real(0);
+    }
+    for (int q = a.pop_drive_ptr[p]; q < a.pop_drive_ptr[p + 1]; ++q) {
+        const DriveDev d = a.drives[a.pop_drive_list[q]];
+        const int64_t se = n - d.lag;
+        if (d.tmin < se && se <= d.tmax) {
+            const uint64_t u = bits53(d.seed, 0u, static_cast<uint32_t>(se),
+                                      static_cast<uint32_t>(g - c.off));
+            const int cnt = poisson_from_table(a.cdf + d.cdf_off, d.cdf_n, u);
+            in[d.receptor < a.R ? d.receptor : 0] += static_cast<Real>(cnt) * static_cast<Real>(d.weight);
+        }
+    }
+    Real st[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) st[i] = (MODEL == 2 || i < 6) ? a.s[i][g] : Real(0);
+    int r = a.r[g];
+    bool sp;
+    if (MODEL == 0) {
+        Real s6[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) s6[i] = st[i];
+        sp = iaf_alpha_step<Real>(c, s6, r, in[0]);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) st[i] = s6[i];
+    } else if (MODEL == 1) {
+        Real s6[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) s6[i] = st[i];
+        sp = iaf_exp_step<Real>(c, s6, r, in[0]);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) st[i] = s6[i];
+    } else {
+        sp = aeif_step<Real>(c, st, r, in[0], in[1], dt, a.err, a.rk_iters);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        if (MODEL == 2 || i < 6) a.s[i][g] = st[i];
+    a.r[g] = r;
+    const int bit = static_cast<int>(n & 63);
+    a.hist[g] = (a.hist[g] & ~(1ull << bit)) | (static_cast<uint64_t>(sp) << bit);
+    if (sp) {
+        const int pos = atomicAdd(a.step_nspk, 1);
+        a.step_spk[pos] = static_cast<uint32_t>(g);
+        if (a.spk_flag == nullptr || a.spk_flag[g]) {
+            const unsigned long long at = atomicAdd(a.spk_count, 1ull);
+            if (at < static_cast<unsigned long long>(a.spk_cap)) {
+                a.spk_step[at] = n;
+                a.spk_gid[at] = g;
+            }
+        }
+    }
+    if (a.rec_slot) {
+        const int rs = a.rec_slot[g];
+        if (rs >= 0) a.v_out[static_cast<size_t>(n - a.run_step0) * a.n_rec + rs] = st[0];
+    }
+}
+
+// Static delivery of this step's spikes: one warp per (spike, projection).
+template <typename Real>
+__global__ void __launch_bounds__(256) k_deliver_static(const StepArgs<Real> a) {
+    const int64_t n = *a.step_ptr;
+    const int nspk = *a.step_nspk;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int slot_n = static_cast<int>(n % a.L);
+    for (int item = warp; item < nspk * a.nproj; item += nwarps) {
+        const int i = item / a.nproj, q = item % a.nproj;
+        if (a.proj_plastic[q]) continue;
+        const ProjDev<Real> P = a.projs[q];
+        const int g = static_cast<int>(a.step_spk[i]);
+        const int pre_off = a.coef[P.pre_pop].off;
+        if (g < pre_off || g >= pre_off + a.coef[P.pre_pop].n) continue;
+        const int gl = g - pre_off;
+        const int64_t beg = P.indptr[gl], end = P.indptr[gl + 1];
+        for (int64_t e = beg + lane; e < end; e += 32) {
+            const uint32_t ed = __ldg(P.edges + e);
+            int slot = slot_n + static_cast<int>(ed >> kEdgeDelayShift);
+            slot %= a.L;
+            const Real w = P.homogeneous ? P.w0 : __ldg(P.w + e);
+            atomicAdd(a.ring + (static_cast<size_t>(slot) * a.R + P.receptor) * a.N + P.post_off +
+                          (ed & kEdgePostMask),
+                      w);
+        }
+    }
+}
+
+__global__ void k_step_end(int64_t *step_ptr) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *step_ptr += 1;
+}
+
+// STDP 1: traces decay-then-add (event_plastic.py:390-420); lists of pres
+// whose delayed spike arrives now and of posts that fired at n - 1.
+__global__ void k_stdp_traces(StdpDev s, const uint64_t *hist, const int64_t *step_ptr) {
+    const int64_t n = *step_ptr;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < s.n_pre) {
+        const bool x = fired(hist, s.pre_off + i, n - s.lag);
+        s.pre_trace[i] = s.pre_trace[i] * s.dec_pre + (x ? 1.0 : 0.0);
+        if (x) s.pre_list[atomicAdd(&s.counts[0], 1)] = i;
+    }
+    if (i < s.n_post) {
+        const bool y = fired(hist, s.post_off + i, n - 1);
+        s.post_trace[i] = s.post_trace[i] * s.dec_post + (y ? 1.0 : 0.0);
+        if (y) s.post_list[atomicAdd(&s.counts[1], 1)] = i;
+    }
+}
+
+__device__ __forceinline__ double stdp_facilitate(const StdpDev &s, double w, double kplus) {
+    const double nw = w / s.Wmax + s.lambda_ * pow(1.0 - w / s.Wmax, s.mu_plus) * kplus;
+    return nw < 1.0 ? nw * s.Wmax : s.Wmax;
+}
+__device__ __forceinline__ double stdp_depress(const StdpDev &s, double w, double kminus) {
+    const double nw = w / s.Wmax - s.alpha * s.lambda_ * pow(w / s.Wmax, s.mu_minus) * kminus;
+    return nw > 0.0 ? nw * s.Wmax : 0.0;
+}
+
+// STDP 2: facilitation on the in-edges of posts that fired at n - 1
+// (_nest_plasticity/stdp_synapse.py:163-165), warp per post.
+__global__ void k_stdp_facilitate(StdpDev s, const uint64_t *hist, const int64_t *step_ptr) {
+    const int64_t n = *step_ptr;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int npost = s.counts[1];
+    for (int it = warp; it < npost; it += nwarps) {
+        const int j = s.post_list[it];
+        for (int64_t e = s.cindptr[j] + lane; e < s.cindptr[j + 1]; e += 32) {
+            const int pre = static_cast<int>(s.cedges[e] & kEdgePostMask);
+            const double x = fired(hist, s.pre_off + pre, n - s.lag) ? 1.0 : 0.0;
+            const double kplus = s.pre_trace[pre] - x;
+            const int64_t eid = s.cperm[e];
+            s.w[eid] = stdp_facilitate(s, s.w[eid], kplus);
+        }
+    }
+}
+
+// STDP 3: depression on the out-edges of pres whose delayed spike arrives
+// now (stdp_synapse.py:167-169), then delivery of the updated weight into
+// this step's ring slot (event_plastic.py:497-518), warp per pre.
+template <typename Real>
+__global__ void k_stdp_depress(StdpDev s, const StepArgs<Real> a) {
+    const int64_t n = *a.step_ptr;
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int npre = s.counts[0];
+    const int slot_n = static_cast<int>(n % a.L);
+    for (int it = warp; it < npre; it += nwarps) {
+        const int i = s.pre_list[it];
+        for (int64_t e = s.indptr[i] + lane; e < s.indptr[i + 1]; e += 32) {
+            const int j = static_cast<int>(s.edges[e] & kEdgePostMask);
+            const double y = fired(a.hist, s.post_off + j, n - 1) ? 1.0 : 0.0;
+            const double kminus = s.post_trace[j] - y;
+            const double w = stdp_depress(s, s.w[e], kminus);
+            s.w[e] = w;
+            atomicAdd(a.ring + (static_cast<size_t>(slot_n) * a.R + s.receptor) * a.N + s.post_off + j,
+                      static_cast<Real>(w));
+        }
+    }
+}
+
+template <typename Real>
+StepArgs<Real> step_args(bspk_plan *p, int64_t *step_ptr) {
+    StepArgs<Real> a{};
+    a.N = p->N;
+    a.npop = static_cast<int>(p->pops.size());
+    a.nproj = static_cast<int>(p->projs.size());
+    a.ndrive = static_cast<int>(p->drives.size());
+    a.model = p->cfg.model;
+    a.R = p->cfg.model == BSPK_AEIF_COND_ALPHA ? 2 : 1;
+    a.L = p->L;
+    a.coef = static_cast<const PopCoef<Real> *>(p->d_coef);
+    for (int i = 0; i < 8; ++i) a.s[i] = static_cast<Real *>(p->d_s[i]);
+    a.r = p->d_r;
+    a.ring = static_cast<Real *>(p->d_ring);
+    a.projs = static_cast<const ProjDev<Real> *>(p->d_projs);
+    a.proj_plastic = p->d_proj_plastic;
+    a.drives = p->d_drives;
+    a.pop_drive_ptr = p->d_pop_drive_ptr;
+    a.pop_drive_list = p->d_pop_drive_list;
+    a.cdf = p->d_cdf;
+    a.hist = p->d_hist;
+    a.step_spk = p->d_step_spk;
+    a.step_nspk = p->d_step_counters;
+    a.spk_step = p->d_spk_step;
+    a.spk_gid = p->d_spk_gid;
+    a.spk_count = p->d_spk_count;
+    a.spk_cap = p->cfg.spike_capacity;
+    a.spk_flag = p->has_spk_flag ? p->d_spk_flag : nullptr;
+    a.rec_slot = p->rec_v.empty() ? nullptr : p->d_rec_slot;
+    a.v_out = static_cast<Real *>(p->d_v);
+    a.n_rec = static_cast<int>(p->rec_v.size());
+    a.step_ptr = step_ptr;
+    a.run_step0 = p->step;
+    a.rk_iters = p->d_rk_iters;
+    a.err = p->d_err;
+    return a;
+}
+
+std::vector<StdpDev> stdp_descs(bspk_plan *p) {
+    std::vector<StdpDev> v;
+    int k = 0;
+    for (auto &J : p->projs) {
+        if (!J.plastic) continue;
+        StdpDev s{};
+        s.pre_off = p->pops[J.pre].off;
+        s.post_off = p->pops[J.post].off;
+        s.n_pre = p->pops[J.pre].n;
+        s.n_post = p->pops[J.post].n;
+        s.lag = (p->cfg.semantics == BSPK_LEGACY ? 1 : 0) + (J.delay.empty() ? 0 : J.delay[0]);
+        s.receptor = J.receptor;
+        s.tau_plus = J.stdp.tau_plus;
+        s.tau_minus = J.stdp.tau_minus;
+        s.lambda_ = J.stdp.lambda_;
+        s.alpha = J.stdp.alpha;
+        s.mu_plus = J.stdp.mu_plus;
+        s.mu_minus = J.stdp.mu_minus;
+        s.Wmax = J.stdp.Wmax;
+        s.dec_pre = std::exp(-p->cfg.dt / J.stdp.tau_plus);
+        s.dec_post = std::exp(-p->cfg.dt / J.stdp.tau_minus);
+        s.indptr = J.d_indptr;
+        s.edges = J.d_edges;
+        s.w = J.d_wplastic;
+        s.cindptr = J.d_cindptr;
+        s.cperm = J.d_cperm;
+        s.cedges = J.d_cedges;
+        s.pre_trace = static_cast<double *>(J.d_pre_trace);
+        s.post_trace = static_cast<double *>(J.d_post_trace);
+        s.pre_list = J.d_pre_list;
+        s.post_list = J.d_post_list;
+        s.counts = p->d_step_counters + 2 + 2 * k;
+        v.push_back(s);
+        ++k;
+    }
+    return v;
+}
+
+template <typename Real>
+cudaError_t enqueue_step(bspk_plan *p, const StepArgs<Real> &a, const std::vector<StdpDev> &sd,
+                         cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(p->d_step_counters, 0, sizeof(int) * p->n_step_counters, st);
+    if (e != cudaSuccess) return e;
+    for (const StdpDev &s : sd) {
+        const int nmax = s.n_pre > s.n_post ? s.n_pre : s.n_post;
+        k_stdp_traces<<<(nmax + 255) / 256, 256, 0, st>>>(s, a.hist, a.step_ptr);
+        k_stdp_facilitate<<<p->sm_count * 4, 256, 0, st>>>(s, a.hist, a.step_ptr);
+        k_stdp_depress<Real><<<p->sm_count * 4, 256, 0, st>>>(s, a);
+    }
+    const int nb = (a.N + 127) / 128;
+    const double dt = p->cfg.dt;
+    if (a.model == 0) k_neuron_step<Real, 0><<<nb, 128, 0, st>>>(a, dt);
+    else if (a.model == 1) k_neuron_step<Real, 1><<<nb, 128, 0, st>>>(a, dt);
+    else k_neuron_step<Real, 2><<<nb, 128, 0, st>>>(a, dt);
+    k_deliver_static<Real><<<p->sm_count * 4, 256, 0, st>>>(a);
+    k_step_end<<<1, 32, 0, st>>>(a.step_ptr);
+    return cudaGetLastError();
+}
+
+template <typename Real>
+int run_typed(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
+    BSPK_CUDA(cudaMemcpyAsync(p->d_step_ptr, &p->step, sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    const StepArgs<Real> a = step_args<Real>(p, p->d_step_ptr);
+    const std::vector<StdpDev> sd = stdp_descs(p);
+    constexpr int64_t kChunk = 32;
+    const int kernels_per_step = 3 + 3 * static_cast<int>(sd.size());
+    int64_t done = 0;
+    if (n_steps >= kChunk) {
+        // capture kChunk steps once per run (the arguments embed this run's
+        // V-recording base), replay for every full chunk
+        cudaGraph_t graph;
+        cudaGraphExec_t exec;
+        cudaStream_t cs;
+        BSPK_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        BSPK_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int64_t k = 0; k < kChunk && e == cudaSuccess; ++k) e = enqueue_step<Real>(p, a, sd, cs);
+        cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            cudaStreamDestroy(cs);
+            return fail(BSPK_ERR_CUDA, std::string("graph capture: ") +
+                                           cudaGetErrorString(e != cudaSuccess ? e : e2));
+        }
+        BSPK_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        for (; done + kChunk <= n_steps; done += kChunk) BSPK_CUDA(cudaGraphLaunch(exec, st));
+        BSPK_CUDA(cudaGraphExecDestroy(exec));
+        BSPK_CUDA(cudaGraphDestroy(graph));
+        BSPK_CUDA(cudaStreamDestroy(cs));
+    }
+    for (; done < n_steps; ++done) {
+        cudaError_t e = enqueue_step<Real>(p, a, sd, st);
+        if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("step launch: ") + cudaGetErrorString(e));
+    }
+    p->last_launches = n_steps * kernels_per_step;
+    return BSPK_OK;
+}
+
+}  // namespace
+
+int run_per_step(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
+    return p->cfg.precision == 64 ? run_typed<double>(p, n_steps, st)
+                                  : run_typed<float>(p, n_steps, st);
+}
+
 }  // namespace bspk

@@ -245,6 +245,18 @@ int lag_of(const bspk_plan *p, int delay_steps) {
 
 }  // namespace
 
+// Host helpers shared with other translation units.
+int bspk::host_make_coef(int model, const std::vector<double> &params, double h,
+                         PopCoef<double> *c) {
+    return make_coef(model, params, h, c);
+}
+
+std::vector<uint64_t> bspk::host_poisson_thresholds(double lam) {
+    std::vector<uint64_t> t;
+    for (double F : poisson_cdf(lam)) t.push_back(static_cast<uint64_t>(std::floor(std::ldexp(F, 53))));
+    return t;
+}
+
 // =================================================================== C ABI
 
 extern "C" {
@@ -314,6 +326,8 @@ int bspk_proj_add_csr(bspk_plan *p, int pre_pop, int post_pop, int64_t n_edges,
     if (n_edges < 0 || (n_edges > 0 && (!post_local || !w || !delay_steps)) || !indptr)
         return fail(BSPK_ERR_ARG, "bad edge arrays");
     if (receptor < 0 || receptor > 1) return fail(BSPK_ERR_ARG, "receptor must be 0 or 1");
+    if (receptor != 0 && p->cfg.model != BSPK_AEIF_COND_ALPHA)
+        return fail(BSPK_ERR_ARG, "receptor ports are for conductance models; current models sum all inputs");
     if (static_cast<int>(p->input_kind.size()) >= kMaxInputs) return fail(BSPK_ERR_ARG, "too many inputs");
     const int npre = p->pops[pre_pop].n, npost = p->pops[post_pop].n;
     if (npost >= (1 << kEdgeDelayShift) || npre >= (1 << kEdgeDelayShift))
@@ -383,6 +397,8 @@ int bspk_drive_add_poisson(bspk_plan *p, int post_pop, double rate_hz, double we
         return fail(BSPK_ERR_ARG, "population index out of range");
     if (static_cast<int>(p->input_kind.size()) >= kMaxInputs) return fail(BSPK_ERR_ARG, "too many inputs");
     if (receptor < 0 || receptor > 1) return fail(BSPK_ERR_ARG, "receptor must be 0 or 1");
+    if (receptor != 0 && p->cfg.model != BSPK_AEIF_COND_ALPHA)
+        return fail(BSPK_ERR_ARG, "receptor ports are for conductance models; current models sum all inputs");
     const double lam = rate_hz * p->cfg.dt / 1000.0;
     if (!(lam >= 0) || lam > 700.0) return fail(BSPK_ERR_ARG, "rate*dt/1000 must be in [0, 700]");
     const int lag = lag_of(p, delay_steps);
@@ -529,6 +545,8 @@ int upload_projs(bspk_plan *p) {
             void *t1 = nullptr, *t2 = nullptr;
             int rc2 = dalloc_bytes(p, &t1, sizeof(double) * npre);
             if (!rc2) rc2 = dalloc_bytes(p, &t2, sizeof(double) * npost);
+            if (!rc2) rc2 = dalloc(p, &J.d_pre_list, npre);
+            if (!rc2) rc2 = dalloc(p, &J.d_post_list, npost);
             if (rc2) return rc2;
             BSPK_CUDA(cudaMemset(t1, 0, sizeof(double) * npre));
             BSPK_CUDA(cudaMemset(t2, 0, sizeof(double) * npost));
@@ -553,6 +571,17 @@ int upload_projs(bspk_plan *p) {
     ProjDev<Real> *dp = nullptr;
     int rc = upload_vec(p, &dp, pd);
     p->d_projs = dp;
+    if (rc) return rc;
+    std::vector<int> plastic;
+    int n_plastic = 0;
+    for (auto &J : p->projs) {
+        plastic.push_back(J.plastic ? 1 : 0);
+        n_plastic += J.plastic ? 1 : 0;
+    }
+    rc = upload_vec(p, &p->d_proj_plastic, plastic);
+    p->n_step_counters = 2 + 2 * n_plastic;
+    if (!rc) rc = dalloc(p, &p->d_step_counters, p->n_step_counters);
+    if (!rc) rc = dalloc(p, &p->d_step_ptr, 1);
     return rc;
 }
 

@@ -46,6 +46,7 @@ struct Proj {
     double *d_wplastic = nullptr;   // FP64 plastic weights (CSR order)
     int64_t *d_cperm = nullptr;     // CSC position -> CSR edge id
     void *d_pre_trace = nullptr, *d_post_trace = nullptr;
+    int *d_pre_list = nullptr, *d_post_list = nullptr;  // per-step STDP work lists
 };
 
 struct Drive {
@@ -102,6 +103,10 @@ struct bspk_plan {
     uint32_t *d_step_spk = nullptr;  // spikes of the current step (gids)
     int *d_step_nspk = nullptr;
     unsigned long long *d_rk_iters = nullptr;
+    int *d_proj_plastic = nullptr;    // 1 per plastic projection
+    int *d_step_counters = nullptr;   // [0] spikes of the step, then 2 per plastic projection
+    int n_step_counters = 0;
+    int64_t *d_step_ptr = nullptr;    // device step counter of the per-step engine
     // timing
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
@@ -122,5 +127,9 @@ struct bspk_plan {
 
 namespace bspk {
 int dalloc_bytes(bspk_plan *p, void **ptr, size_t bytes);
+// float64 coefficients of a population (propagators, thresholds) and the
+// Poisson CDF of rate*dt as 53-bit integer thresholds
+int host_make_coef(int model, const std::vector<double> &params, double h, PopCoef<double> *c);
+std::vector<uint64_t> host_poisson_thresholds(double lam);
 int sync_and_check(bspk_plan *p);
 }  // namespace bspk
