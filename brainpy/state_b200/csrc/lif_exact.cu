@@ -162,3 +162,179 @@ cudaError_t launch_lif_exact(const LifArgs<double> &a, int grid, int block, cuda
 }
 
 }  // namespace bspk
+
+// ===================================================== no-allocation entry
+//
+// bspk_iaf_exact_run_noalloc: the deterministic FP64 kernel above, launched
+// for one iaf_psc_alpha population (one Poisson drive, then one recurrent
+// projection) without a plan and without any device allocation.  It is for
+// callers that cannot call cudaMalloc: code running inside another
+// framework's memory pool or allocator hooks (an XLA custom call, a CUDA
+// graph being captured, a plugin whose host forbids allocations).  The
+// caller passes every input and output buffer; everything else the kernel
+// needs lives in one file-scope device array of fixed size (parameter
+// tables, Poisson CDF, 64-step spike-history words, barrier counter, error
+// flag, spike counter), so at most kNoAllocMaxNeurons neurons and a CDF of
+// kNoAllocMaxCdf entries.
+namespace {
+
+constexpr int kNoAllocMaxNeurons = 1 << 16;
+constexpr int kNoAllocMaxCdf = 4096;
+
+struct NoAllocScratch {
+    uint64_t hist[kNoAllocMaxNeurons];
+    uint64_t cdf[kNoAllocMaxCdf];
+    bspk::PopCoef<double> coef;
+    bspk::DriveDev drive;
+    bspk::ProjDev<double> proj;
+    int in_ptr[2], in_list[2], drv_ptr[2], drv_list[1], out_ptr[2], out_list[1];
+    unsigned int barrier;
+    int err;
+    unsigned long long spk_count;
+};
+
+// Shared by every call on a device and kept until the process exits; a call
+// clears the parts that must start at zero.  Calls that overlap on the GPU
+// (two streams at once) race on it.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[256] = {};
+
+}  // namespace
+
+extern "C" int bspk_iaf_exact_run_noalloc(double dt, const double *params, int n_params, int n,
+                                          const int64_t *in_indptr, const uint32_t *in_edges,
+                                          const double *in_w, double w_const,
+                                          int min_delay_steps, int max_delay_steps,
+                                          double drive_rate_hz, double drive_weight,
+                                          int drive_delay_steps, uint32_t drive_seed,
+                                          double *state, int32_t *refr, int64_t n_steps,
+                                          int64_t *spike_step, int32_t *spike_gid,
+                                          int64_t spike_cap, int64_t *spike_count, int *status,
+                                          void *stream) {
+    using namespace bspk;
+    if (!params || !in_indptr || !state || !refr || !spike_step || !spike_gid || !spike_count ||
+        !status || n <= 0 || n_steps < 0 || spike_cap < 0 || !(dt > 0))
+        return fail(BSPK_ERR_ARG, "bad argument");
+    if (n > kNoAllocMaxNeurons)
+        return fail(BSPK_ERR_ARG, "no-allocation entry point: more than 65536 neurons");
+    if (min_delay_steps < 0 || max_delay_steps < min_delay_steps || max_delay_steps + 1 > 62)
+        return fail(BSPK_ERR_ARG, "no-allocation entry point: delays must be 0..61 steps");
+    const double lam = drive_rate_hz * dt / 1000.0;
+    if (!(lam >= 0) || lam > 700.0) return fail(BSPK_ERR_ARG, "rate*dt/1000 must be in [0, 700]");
+    const std::vector<uint64_t> cdf = host_poisson_thresholds(lam);
+    if (static_cast<int>(cdf.size()) > kNoAllocMaxCdf) return fail(BSPK_ERR_ARG, "drive CDF too long");
+    PopCoef<double> coef;
+    int rc = host_make_coef(BSPK_IAF_PSC_ALPHA, std::vector<double>(params, params + n_params), dt,
+                            &coef);
+    if (rc) return rc;
+    coef.off = 0;
+    coef.n = n;
+
+    int dev = 0;
+    BSPK_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return fail(BSPK_ERR_ARG, "device ordinal out of range");
+    void *base = nullptr;
+    {
+        // once per device, with that device current: the host-side symbol is a
+        // stand-in, only the address returned here is valid on the device
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_addr[dev]) {
+            void *addr = nullptr;
+            BSPK_CUDA(cudaGetSymbolAddress(&addr, g_noalloc_scratch));
+            g_noalloc_addr[dev] = addr;
+        }
+        base = g_noalloc_addr[dev];
+    }
+    NoAllocScratch *S = static_cast<NoAllocScratch *>(base);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+
+    DriveDev drive{};
+    drive.pop = 0;
+    drive.lag = drive_delay_steps + 1;  // the reference Simulator's holder lag
+    drive.seed = drive_seed;
+    drive.cdf_off = 0;
+    drive.cdf_n = static_cast<int>(cdf.size());
+    drive.receptor = 0;
+    drive.weight = drive_weight;
+    drive.tmin = 0;
+    drive.tmax = drive_rate_hz > 0 ? (int64_t(1) << 62) : 0;
+    ProjDev<double> proj{};
+    proj.pre_pop = 0;
+    proj.post_pop = 0;
+    proj.post_off = 0;
+    proj.homogeneous = in_w ? 0 : 1;
+    proj.w0 = w_const;
+    proj.cindptr = in_indptr;
+    proj.cedges = in_edges;
+    proj.cw = in_w;
+    const int tables[10] = {0, 2, -1, 0, 0, 1, 0, 0, 0, 0};  // in_ptr, in_list, drv_ptr, drv_list, out
+    BSPK_CUDA(cudaMemcpyAsync(S->cdf, cdf.data(), sizeof(uint64_t) * cdf.size(),
+                              cudaMemcpyHostToDevice, st));
+    BSPK_CUDA(cudaMemcpyAsync(&S->coef, &coef, sizeof(coef), cudaMemcpyHostToDevice, st));
+    BSPK_CUDA(cudaMemcpyAsync(&S->drive, &drive, sizeof(drive), cudaMemcpyHostToDevice, st));
+    BSPK_CUDA(cudaMemcpyAsync(&S->proj, &proj, sizeof(proj), cudaMemcpyHostToDevice, st));
+    BSPK_CUDA(cudaMemcpyAsync(S->in_ptr, tables, sizeof(tables), cudaMemcpyHostToDevice, st));
+    BSPK_CUDA(cudaMemsetAsync(S->hist, 0, sizeof(uint64_t) * n, st));
+    BSPK_CUDA(cudaMemsetAsync(&S->barrier, 0, sizeof(unsigned int) + sizeof(int), st));
+    BSPK_CUDA(cudaMemsetAsync(&S->spk_count, 0, sizeof(unsigned long long), st));
+    // the copies above came from pageable host memory, so they completed
+    // before cudaMemcpyAsync returned; the host tables may go out of scope
+
+    int sm = 0;
+    BSPK_CUDA(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev));
+    int block = ((n + sm - 1) / sm + 31) / 32 * 32;
+    block = block < 64 ? 64 : (block > 256 ? 256 : block);
+    const int grid = (n + block - 1) / block;
+    const int max_lag = max_delay_steps + 1, min_lag = min_delay_steps + 1;
+    int W = min_lag < kMaxWindow ? min_lag : kMaxWindow;
+    if (W > 64 - max_lag) W = 64 - max_lag;
+    if (W < 1) W = 1;
+
+    LifArgs<double> a{};
+    a.N = n;
+    a.npop = 1;
+    a.nproj = 1;
+    a.ndrive = 1;
+    a.coef = &S->coef;
+    for (int i = 0; i < 6; ++i) a.s[i] = state + static_cast<size_t>(i) * n;
+    a.r = refr;
+    a.ring = nullptr;
+    a.L = 1;
+    a.projs = &S->proj;
+    a.pop_out_ptr = S->out_ptr;
+    a.pop_out_list = S->out_list;
+    a.pop_in_ptr = S->in_ptr;
+    a.pop_in_list = S->in_list;
+    a.drives = &S->drive;
+    a.pop_drive_ptr = S->drv_ptr;
+    a.pop_drive_list = S->drv_list;
+    a.cdf = S->cdf;
+    a.cdf_total = static_cast<int>(cdf.size());
+    a.step0 = 0;
+    a.n_steps = n_steps;
+    a.run_step0 = 0;
+    a.W = W;
+    a.tile = block;
+    a.model = BSPK_IAF_PSC_ALPHA;
+    a.spk_step = spike_step;
+    a.spk_gid = spike_gid;
+    a.spk_count = &S->spk_count;
+    a.spk_cap = spike_cap;
+    a.spk_flag = nullptr;
+    a.rec_slot = nullptr;
+    a.v_out = nullptr;
+    a.n_rec = 0;
+    a.hist = S->hist;
+    a.barrier = &S->barrier;
+    a.err = &S->err;
+    if (n_steps > 0) {
+        const cudaError_t e = launch_lif_exact(a, grid, block, st);
+        if (e != cudaSuccess)
+            return fail(BSPK_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    }
+    BSPK_CUDA(cudaMemcpyAsync(spike_count, &S->spk_count, sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
+    BSPK_CUDA(cudaMemcpyAsync(status, &S->err, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    return BSPK_OK;
+}

@@ -155,6 +155,42 @@ int bspk_checkpoint_size(bspk_plan *plan, int64_t *bytes);
 int bspk_checkpoint_save(bspk_plan *plan, void *host_buf, int64_t bytes);
 int bspk_checkpoint_restore(bspk_plan *plan, const void *host_buf, int64_t bytes);
 
+/* No-allocation entry point (no counterpart in the reference).  For callers
+ * that cannot call cudaMalloc -- code running inside another framework's
+ * memory pool or allocation hooks, or a plugin host that forbids device
+ * allocations -- this runs the deterministic FP64 network step for ONE
+ * iaf_psc_alpha population without a plan and allocates nothing: every input
+ * and output is a caller-owned device buffer, and the kernel's scratch
+ * (parameter tables, Poisson CDF, spike-history words, barrier counter,
+ * error flag, spike counter) lives in one fixed-size device array inside
+ * the library, held by every GPU that loads it until the process exits.
+ *
+ * Network: a Poisson drive (rate, weight, delay, seed; created first), then
+ * one recurrent projection given as in-edges per post neuron:
+ * in_indptr[n+1], in_edges[E] = pre | (delay_steps + 1) << 24 in ascending
+ * pre order, per-edge weights in_w[E] or NULL with w_const; min/max delay in
+ * steps.  Reference Simulator timing (a spike of step m arrives at m + D + 1).
+ * state: [6][n] doubles (V_m, I_syn_ex, dI_syn_ex, I_syn_in, dI_syn_in, y0),
+ * refr: [n] refractory counters, both read and written.  Outputs: spikes as
+ * (step within this call, neuron) pairs up to spike_cap, *spike_count, and
+ * *status (0 = ok, nonzero = device error code), all device memory.
+ *
+ * Limits: n <= 65536 neurons, delays <= 61 steps, drive CDF <= 4096 entries;
+ * larger sizes are rejected with BSPK_ERR_ARG.  Each call starts with an
+ * empty spike history (spikes of earlier calls are not delivered).  All
+ * calls on a device share the scratch array, so calls that overlap on the
+ * GPU race; serialise them.  The first call on a device looks up the
+ * scratch array's device address (once per device, with that device
+ * current); make that first call before capturing any stream. */
+int bspk_iaf_exact_run_noalloc(double dt, const double *params, int n_params, int n,
+                               const int64_t *in_indptr, const uint32_t *in_edges,
+                               const double *in_w, double w_const, int min_delay_steps,
+                               int max_delay_steps, double drive_rate_hz, double drive_weight,
+                               int drive_delay_steps, uint32_t drive_seed, double *state,
+                               int32_t *refr, int64_t n_steps, int64_t *spike_step,
+                               int32_t *spike_gid, int64_t spike_cap, int64_t *spike_count,
+                               int *status, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
