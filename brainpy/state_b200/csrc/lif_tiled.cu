@@ -34,45 +34,48 @@ constexpr int kDelivWarps = 5;
 constexpr int kDeliv = 32 * kDelivWarps;      // threads that deliver
 constexpr int kRecPerHalf = 16;               // records per half-warp: G <= 2*5*16 = 160
 constexpr int kListCap = 2048;                // spikes gathered per window and CTA
-constexpr int kEdgeUnroll = 8;                // edge loads in flight per thread
+constexpr int kEdgeUnroll = 16;               // edge loads in flight per thread
 
 __device__ __forceinline__ void named_sync(int id, int nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
-// Exclusive scan of s[0..n) by the first nth threads (named barrier `bar`);
-// returns the total.
+// Exclusive scan of s[0..n) by the first nth threads (named barrier `bar`):
+// thread t scans a run of ceil(n / nth) consecutive elements, the runs' sums
+// are scanned across warps; three barriers whatever n is.  Returns the total.
 __device__ int scan_named(int *s, int n, int *s_warp, int nth, int bar) {
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = nth >> 5;
-    int carry = 0;
-    for (int base = 0; base < n; base += nth) {
-        const int i = base + tid;
-        const int v = i < n ? s[i] : 0;
-        int x = v;
+    const int per = (n + nth - 1) / nth;
+    const int b0 = tid * per, b1 = min(n, b0 + per);
+    int run = 0;
+    for (int i = b0; i < b1; ++i) run += s[i];
+    int x = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[wid] = x;
+    named_sync(bar, nth);
+    if (wid == 0) {
+        int t = lane < nw ? s_warp[lane] : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
         }
-        if (lane == 31) s_warp[wid] = x;
-        named_sync(bar, nth);
-        if (wid == 0) {
-            int t = lane < nw ? s_warp[lane] : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, t, o);
-                if (lane >= o) t += y;
-            }
-            if (lane < nw) s_warp[lane] = t;
-        }
-        named_sync(bar, nth);
-        const int warp_off = wid > 0 ? s_warp[wid - 1] : 0;
-        const int total = s_warp[nw - 1];
-        if (i < n) s[i] = carry + warp_off + x - v;
-        carry += total;
-        named_sync(bar, nth);
+        if (lane < nw) s_warp[lane] = t;
     }
-    return carry;
+    named_sync(bar, nth);
+    int acc = (wid > 0 ? s_warp[wid - 1] : 0) + x - run;
+    const int total = s_warp[nw - 1];
+    for (int i = b0; i < b1; ++i) {
+        const int v = s[i];
+        s[i] = acc;
+        acc += v;
+    }
+    named_sync(bar, nth);
+    return total;
 }
 
 __device__ __forceinline__ int find_pop2(const int *s_off, int npop, int g) {
