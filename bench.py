@@ -158,7 +158,7 @@ def run_ours(args):
     rtf = world * sim_ms / ms_step
     syn_ev_s = world * (nev / args.steps) / (ms_step / 1000.0)
     rate_hz = nspk / args.steps / N
-    drive_ev_s = world * N * p["rate"] / (ms_step / 1000.0)
+    drive_ev_s = world * N * p["rate"] * (sim_ms / 1000.0) / (ms_step / 1000.0)
     kms, launches = pl.kernel_time()
 
     # roofline of the persistent kernel: algorithmic bytes per launch
@@ -171,10 +171,13 @@ def run_ours(args):
     peak, peak_kind = _peaks()
     achieved = alg_bytes / (ms_step / 1000.0) / 1e9
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "traffic_k_lif_fast.json")
+    prof = os.path.join(ROOT, "profiles", "k_lif_tiled_brunel12500_ncu_full.md")
     if os.path.exists(prof):
         with open(prof) as f:
-            traffic = json.load(f).get("bytes_per_launch")
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch ="):
+                    # captured on a 1000-step launch, scaled to this launch's time steps
+                    traffic = int(line.split("=")[1]) * STEPS_PER_BENCH_STEP // 10000
 
     result = {
         "metric": METRIC, "value": round(rtf, 3), "unit": "x real time (simulated s / wall s)",
@@ -194,7 +197,7 @@ def run_ours(args):
         "gpu_launches": int(args.steps) * 1,
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
-                     "peak_kind": peak_kind, "kernel": "k_lif_fast<float>"},
+                     "peak_kind": peak_kind, "kernel": "bspk::k_lif_tiled<float, 0>"},
         "clocks": clk.summary(),
     }
     del pl
