@@ -75,6 +75,31 @@ def lib():
             "bspk_checkpoint_size": (C.c_int, [vp, C.POINTER(i64)]),
             "bspk_checkpoint_save": (C.c_int, [vp, vp, i64]),
             "bspk_checkpoint_restore": (C.c_int, [vp, vp, i64]),
+            "bspk_gen_fixed_indegree": (C.c_int, [C.c_int, i64, C.c_int, C.c_int, C.c_int,
+                                                  C.c_int, C.c_int, C.c_int, vp, vp]),
+            "bspk_batch_create": (C.c_int, [C.POINTER(Config), C.POINTER(vp)]),
+            "bspk_batch_destroy": (C.c_int, [vp]),
+            "bspk_batch_instance_add": (C.c_int, [vp, C.POINTER(C.c_int)]),
+            "bspk_batch_pop_add": (C.c_int, [vp, C.c_int, C.c_int, vp, C.c_int,
+                                             C.POINTER(C.c_int)]),
+            "bspk_batch_fixed_indegree_add": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                        i64, C.c_int, C.c_int, dbl, C.c_int]),
+            "bspk_batch_drive_add_poisson": (C.c_int, [vp, C.c_int, C.c_int, dbl, dbl, C.c_int,
+                                                       u32, i64, i64]),
+            "bspk_batch_record_spikes": (C.c_int, [vp, C.c_int, C.c_int]),
+            "bspk_batch_upload": (C.c_int, [vp, C.c_int, C.c_int, vp]),
+            "bspk_batch_tune": (C.c_int, [vp, i64, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                          C.POINTER(dbl)]),
+            "bspk_batch_shape": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                           C.POINTER(C.c_int), C.POINTER(i64)]),
+            "bspk_batch_run": (C.c_int, [vp, i64, vp]),
+            "bspk_batch_state_set": (C.c_int, [vp, C.c_int, C.c_int, C.c_char_p, vp]),
+            "bspk_batch_state_get": (C.c_int, [vp, C.c_int, C.c_int, C.c_char_p, vp]),
+            "bspk_batch_spike_counts": (C.c_int, [vp, C.c_int, vp]),
+            "bspk_batch_spikes_get": (C.c_int, [vp, C.c_int, i64, vp, vp, C.POINTER(i64)]),
+            "bspk_batch_edges_get": (C.c_int, [vp, C.c_int, i64, vp, vp, vp, C.POINTER(i64)]),
+            "bspk_batch_step_count": (i64, [vp]),
+            "bspk_batch_last_kernel_time": (C.c_int, [vp, C.POINTER(dbl), C.POINTER(i64)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -247,3 +272,131 @@ class Plan:
     def restore(self, buf):
         buf = np.ascontiguousarray(buf, np.uint8)
         check(self._L.bspk_checkpoint_restore(self._h, ptr(buf), int(buf.size)))
+
+
+def gen_fixed_indegree(seed, n_pre, n_post, K, pre_is_post=False, allow_autapses=True, nbits=32,
+                       device=0):
+    """fixed_indegree CSR drawn on the GPU: (indptr int64[n_pre+1], post int32[E])."""
+    L = lib()
+    indptr = np.zeros(int(n_pre) + 1, np.int64)
+    post = np.zeros(max(int(n_post) * int(K), 1), np.int32)
+    check(L.bspk_gen_fixed_indegree(int(device), int(seed), int(n_pre), int(n_post), int(K),
+                                    int(bool(pre_is_post)), int(bool(allow_autapses)),
+                                    int(nbits), ptr(indptr), ptr(post)))
+    return indptr, post[:int(n_post) * int(K)]
+
+
+class Batch:
+    """Owner of one ``bspk_batch``: independent iaf networks of uneven sizes
+    advanced by one persistent launch (instances, populations, fixed_indegree
+    projections with one delay per instance, Poisson drives)."""
+
+    def __init__(self, dt, model="iaf_psc_alpha", precision=32, semantics=LEGACY, device=0,
+                 spike_capacity=1 << 22):
+        self._L = lib()
+        cfg = Config(float(dt), int(precision), int(semantics), 0, MODELS[model], int(device),
+                     int(spike_capacity))
+        h = C.c_void_p()
+        check(self._L.bspk_batch_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self.dt = float(dt)
+        self.precision = precision
+        self.sizes = []      # neurons per instance
+        self.pop_sizes = []  # per instance: list of population sizes
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.bspk_batch_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def add_instance(self):
+        i = C.c_int()
+        check(self._L.bspk_batch_instance_add(self._h, C.byref(i)))
+        self.sizes.append(0)
+        self.pop_sizes.append([])
+        return i.value
+
+    def add_pop(self, inst, n, params):
+        p = np.ascontiguousarray(params, np.float64)
+        out = C.c_int()
+        check(self._L.bspk_batch_pop_add(self._h, int(inst), int(n), ptr(p), p.size,
+                                         C.byref(out)))
+        self.sizes[inst] += int(n)
+        self.pop_sizes[inst].append(int(n))
+        return out.value
+
+    def add_fixed_indegree(self, inst, pre, post, K, seed, weight, delay_steps,
+                           allow_autapses=True, nbits=32):
+        check(self._L.bspk_batch_fixed_indegree_add(self._h, int(inst), int(pre), int(post),
+                                                    int(K), int(seed), int(bool(allow_autapses)),
+                                                    int(nbits), float(weight), int(delay_steps)))
+
+    def add_poisson(self, inst, post, rate_hz, weight, delay_steps, seed, t_min=0,
+                    t_max=(1 << 62)):
+        check(self._L.bspk_batch_drive_add_poisson(self._h, int(inst), int(post), float(rate_hz),
+                                                   float(weight), int(delay_steps),
+                                                   int(seed) & 0xFFFFFFFF, int(t_min), int(t_max)))
+
+    def record_spikes(self, inst, on=True):
+        check(self._L.bspk_batch_record_spikes(self._h, int(inst), int(bool(on))))
+
+    def upload(self, tile=0, ctas_per_sm=0):
+        check(self._L.bspk_batch_upload(self._h, int(tile), int(ctas_per_sm), None))
+
+    def tune(self, pilot_steps=300):
+        t, c, ms = C.c_int(), C.c_int(), C.c_double()
+        check(self._L.bspk_batch_tune(self._h, int(pilot_steps), C.byref(t), C.byref(c),
+                                      C.byref(ms)))
+        return t.value, c.value, ms.value
+
+    def shape(self):
+        t, c, g, n = C.c_int(), C.c_int(), C.c_int(), C.c_int64()
+        check(self._L.bspk_batch_shape(self._h, C.byref(t), C.byref(c), C.byref(g), C.byref(n)))
+        return {"tile": t.value, "ctas_per_sm": c.value, "grid": g.value, "tiles": n.value}
+
+    def run(self, n_steps, stream=None):
+        check(self._L.bspk_batch_run(self._h, int(n_steps), stream))
+
+    def set_state(self, inst, pop, name, values):
+        v = np.ascontiguousarray(values, np.float64)
+        check(self._L.bspk_batch_state_set(self._h, int(inst), int(pop), name.encode(), ptr(v)))
+
+    def get_state(self, inst, pop, name):
+        v = np.zeros(self.pop_sizes[inst][pop], np.float64)
+        check(self._L.bspk_batch_state_get(self._h, int(inst), int(pop), name.encode(), ptr(v)))
+        return v
+
+    def spike_counts(self, inst):
+        c = np.zeros(self.sizes[inst], np.int64)
+        check(self._L.bspk_batch_spike_counts(self._h, int(inst), ptr(c)))
+        return c
+
+    def spikes(self, inst):
+        n = C.c_int64()
+        check(self._L.bspk_batch_spikes_get(self._h, int(inst), 0, None, None, C.byref(n)))
+        st = np.zeros(max(n.value, 1), np.int64)
+        ids = np.zeros(max(n.value, 1), np.int32)
+        check(self._L.bspk_batch_spikes_get(self._h, int(inst), n.value, ptr(st), ptr(ids),
+                                            C.byref(n)))
+        return st[:n.value], ids[:n.value]
+
+    def edges(self, inst):
+        n = C.c_int64()
+        check(self._L.bspk_batch_edges_get(self._h, int(inst), 0, None, None, None, C.byref(n)))
+        pre = np.zeros(max(n.value, 1), np.int32)
+        post = np.zeros_like(pre)
+        proj = np.zeros_like(pre)
+        check(self._L.bspk_batch_edges_get(self._h, int(inst), n.value, ptr(pre), ptr(post),
+                                           ptr(proj), C.byref(n)))
+        return pre[:n.value], post[:n.value], proj[:n.value]
+
+    @property
+    def step(self):
+        return int(self._L.bspk_batch_step_count(self._h))
+
+    def kernel_time(self):
+        ms, n = C.c_double(), C.c_int64()
+        check(self._L.bspk_batch_last_kernel_time(self._h, C.byref(ms), C.byref(n)))
+        return ms.value, n.value

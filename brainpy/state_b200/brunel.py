@@ -79,3 +79,86 @@ def build_plan(order=2500, precision=32, delay_steps=(10, 30), noise_delay=15, s
     pl.set_state(e, "V_m", vr.uniform(v_init[0], v_init[1], p["NE"]))
     pl.set_state(i, "V_m", vr.uniform(v_init[0], v_init[1], p["NI"]))
     return pl, p
+
+
+# ------------------------------------------------------------ sweep batches
+
+def sweep_instances(n=256, seed=1234, ne_range=(500, 8000), g_range=(3.0, 8.0),
+                    eta_range=(0.9, 4.0), delay_steps=15):
+    """Parameter sweep of Brunel networks: NE ~ U[ne_range] (NI = NE / 4,
+    epsilon = 0.1), g ~ U[g_range], eta ~ U[eta_range], instance k seeded k."""
+    rng = np.random.default_rng(seed)
+    ne = rng.integers(ne_range[0], ne_range[1] + 1, size=n)
+    g = rng.uniform(*g_range, size=n)
+    eta = rng.uniform(*eta_range, size=n)
+    return [dict(NE=int(ne[k]), NI=int(ne[k]) // 4, g=float(g[k]), eta=float(eta[k]), seed=k,
+                 delay_steps=delay_steps) for k in range(n)]
+
+
+def _instance_params(spec):
+    p = brunel_params(2500, g=spec["g"], eta=spec["eta"])
+    NE, NI = spec["NE"], spec["NI"]
+    p.update(NE=NE, NI=NI, CE=int(0.1 * NE), CI=int(0.1 * NI))
+    # the drive rate eta * nu_th * CE does not depend on CE (nu_th ~ 1 / CE)
+    return p
+
+
+def _instance_v0(spec, v_init=(0.0, 20.0)):
+    vr = np.random.default_rng(spec["seed"] + 7)
+    return (vr.uniform(v_init[0], v_init[1], spec["NE"]),
+            vr.uniform(v_init[0], v_init[1], spec["NI"]))
+
+
+def _instance_projs(spec, p):
+    """(pre, post, K, seed, weight) in creation order: E->E, E->I, I->E, I->I."""
+    out, ordinal = [], 2
+    for pre, K, w in ((0, p["CE"], p["J_ex"]), (1, p["CI"], p["J_in"])):
+        for post in (0, 1):
+            out.append((pre, post, K, derive_seed(spec["seed"], ordinal), w))
+            ordinal += 1
+    return out
+
+
+def build_batch(instances, precision=32, semantics=_lib.RING, tile=0, ctas_per_sm=0,
+                record=(), noise_delay=15):
+    """All sweep instances in one ``Batch`` (connectivity drawn on the GPU)."""
+    b = _lib.Batch(0.1, "iaf_psc_alpha", precision=precision, semantics=semantics)
+    params = []
+    for spec in instances:
+        p = _instance_params(spec)
+        params.append(p)
+        k = b.add_instance()
+        e = b.add_pop(k, p["NE"], p["neuron"])
+        i = b.add_pop(k, p["NI"], p["neuron"])
+        b.add_poisson(k, e, p["rate"], p["J_ex"], noise_delay, derive_seed(spec["seed"], 0))
+        b.add_poisson(k, i, p["rate"], p["J_ex"], noise_delay, derive_seed(spec["seed"], 1))
+        for pre, post, K, s, w in _instance_projs(spec, p):
+            b.add_fixed_indegree(k, pre, post, K, s, w, spec["delay_steps"], nbits=32)
+        if k in record:
+            b.record_spikes(k)
+    b.upload(tile=tile, ctas_per_sm=ctas_per_sm)
+    for k, spec in enumerate(instances):
+        ve, vi = _instance_v0(spec)
+        b.set_state(k, 0, "V_m", ve)
+        b.set_state(k, 1, "V_m", vi)
+    return b, params
+
+
+def instance_plan(spec, precision=64, semantics=_lib.RING, deterministic=False,
+                  noise_delay=15, spike_capacity=1 << 22):
+    """One sweep instance as a stand-alone plan (host-drawn connectivity,
+    the same seeds and 32-bit draws as ``build_batch``)."""
+    p = _instance_params(spec)
+    pl = _lib.Plan(0.1, "iaf_psc_alpha", precision=precision, semantics=semantics,
+                   deterministic=deterministic, spike_capacity=spike_capacity)
+    e = pl.add_pop(p["NE"], p["neuron"])
+    i = pl.add_pop(p["NI"], p["neuron"])
+    pl.add_poisson(e, p["rate"], p["J_ex"], noise_delay, derive_seed(spec["seed"], 0))
+    pl.add_poisson(i, p["rate"], p["J_ex"], noise_delay, derive_seed(spec["seed"], 1))
+    for pre, post, K, s, w in _instance_projs(spec, p):
+        pl.add_fixed_indegree(pre, post, K, s, w, delay_const=spec["delay_steps"], nbits=32)
+    pl.upload()
+    ve, vi = _instance_v0(spec)
+    pl.set_state(e, "V_m", ve)
+    pl.set_state(i, "V_m", vi)
+    return pl, p

@@ -29,11 +29,14 @@ SOURCES = {
     "lif_exact.cu": ["-fmad=false"],
     "per_step.cu": [],
     "batch.cu": [],
+    "batch_host.cpp": [],
+    "conn_gen.cu": [],
     "adjoint.cu": [],
     "checkpoint.cpp": [],
 }
 HEADERS = ["common.cuh", "device_types.h", "lif_args.h", "aeif_args.h", "stdp_args.h",
-           "host_rng.h", "batch_args.h", "plan_internal.h"]
+           "host_rng.h", "batch_args.h", "plan_internal.h", "conn_gen.h", "conn_gen.cuh",
+           "coef_cast.h"]
 
 
 def _mtime(p):

@@ -17,6 +17,7 @@
 
 #include "../../../include/bspk.h"
 #include "aeif_args.h"
+#include "coef_cast.h"
 #include "device_types.h"
 #include "host_rng.h"
 #include "lif_args.h"
@@ -205,21 +206,6 @@ int make_coef(int model, const std::vector<double> &p, double h, PopCoef<double>
     return fail(BSPK_ERR_ARG, "unknown model");
 }
 
-template <typename Real>
-PopCoef<Real> cast_coef(const PopCoef<double> &d) {
-    PopCoef<Real> c;
-#define C_(f) c.f = static_cast<Real>(d.f);
-    C_(E_L) C_(I_e) C_(lower) C_(theta) C_(vreset) C_(P11ex) C_(P21ex) C_(P22ex) C_(P11in)
-    C_(P21in) C_(P22in) C_(expm1_tm) C_(P30) C_(P31ex) C_(P32ex) C_(P31in) C_(P32in) C_(epsc)
-    C_(ipsc) C_(eP11ex) C_(eP11in) C_(eP22) C_(eP21ex) C_(eP21in) C_(eP20) C_(one_m_eP11ex)
-    C_(V_peak) C_(V_reset) C_(g_L) C_(C_m) C_(E_ex) C_(E_in) C_(Delta_T) C_(tau_w) C_(a) C_(b)
-    C_(V_th) C_(tau_syn_ex) C_(tau_syn_in) C_(atol) C_(pscon_ex) C_(pscon_in) C_(v_peak_detect)
-#undef C_
-    c.ref_count = d.ref_count;
-    c.off = d.off;
-    c.n = d.n;
-    return c;
-}
 
 // CDF table of Poisson(lam): F[0] = exp(-lam), p_k = p_{k-1} * lam / k,
 // F[k] = F[k-1] + p_k, until F stops growing.  The count for a uniform u is

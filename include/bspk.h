@@ -155,6 +155,64 @@ int bspk_checkpoint_size(bspk_plan *plan, int64_t *bytes);
 int bspk_checkpoint_save(bspk_plan *plan, void *host_buf, int64_t bytes);
 int bspk_checkpoint_restore(bspk_plan *plan, const void *host_buf, int64_t bytes);
 
+/* fixed_indegree connectivity drawn on the GPU (one thread per edge, the
+ * same key derivation and bits as bspk_proj_add_fixed_indegree) and sorted
+ * into CSR by a stable radix sort, returned to host buffers indptr[n_pre+1]
+ * and post_local[n_post*K].  Replaces sample_fixed_indegree + csr_structure
+ * (_nest_network/connectivity.py:39-53, :101-135; kernel rule
+ * _kernel/connectivity/rules.py:192-251), whose host build dominates the
+ * reference's network construction. */
+int bspk_gen_fixed_indegree(int device, int64_t seed, int n_pre, int n_post, int K,
+                            int pre_is_post, int allow_autapses, int nbits, int64_t *indptr,
+                            int32_t *post_local);
+
+/* ---------------------------------------------------------------- batches
+ * Many independent iaf networks ("instances") of uneven sizes advanced by
+ * one persistent cooperative launch.  The reference batches only identical
+ * structures (Runner(batch) vmap, _kernel/runner.py:832-863, trial keys
+ * _kernel/rng.py:435-479); an instance here has its own populations,
+ * fixed_indegree projections (built on the GPU at upload), Poisson drives
+ * and seeds.  All projections of one instance share one delay (its
+ * window); config fields as for plans (deterministic must be 0, model an
+ * iaf model shared by all instances). */
+typedef struct bspk_batch bspk_batch;
+int bspk_batch_create(const bspk_config *cfg, bspk_batch **out);
+int bspk_batch_destroy(bspk_batch *batch);
+int bspk_batch_instance_add(bspk_batch *batch, int *inst);
+int bspk_batch_pop_add(bspk_batch *batch, int inst, int n, const double *params, int n_params,
+                       int *pop);
+int bspk_batch_fixed_indegree_add(bspk_batch *batch, int inst, int pre_pop, int post_pop, int K,
+                                  int64_t seed, int allow_autapses, int nbits, double weight,
+                                  int delay_steps);
+int bspk_batch_drive_add_poisson(bspk_batch *batch, int inst, int post_pop, double rate_hz,
+                                 double weight, int delay_steps, uint32_t seed,
+                                 int64_t t_min_step, int64_t t_max_step);
+int bspk_batch_record_spikes(bspk_batch *batch, int inst, int on);
+/* Build the device layout: tile = neurons per tile and threads per CTA
+ * (multiple of 32 in [32, 512]; 0 = 256), ctas_per_sm <= 0 = as many as fit. */
+int bspk_batch_upload(bspk_batch *batch, int tile, int ctas_per_sm, void *stream);
+/* Autotuner: measures every instance's rate on a pilot run, then times
+ * tile sizes x CTAs per SM on the same pilot (tile-to-CTA assignment by
+ * longest-processing-time first over the calibrated cost model) and keeps
+ * the fastest; the state is restored to what it was before the call. */
+int bspk_batch_tune(bspk_batch *batch, int64_t pilot_steps, int *tile, int *ctas_per_sm,
+                    double *pilot_ms);
+int bspk_batch_shape(bspk_batch *batch, int *tile, int *ctas_per_sm, int *grid, int64_t *n_tiles);
+int bspk_batch_run(bspk_batch *batch, int64_t n_steps, void *stream);
+int bspk_batch_state_set(bspk_batch *batch, int inst, int pop, const char *name,
+                         const double *values);
+int bspk_batch_state_get(bspk_batch *batch, int inst, int pop, const char *name, double *values);
+/* Spikes per neuron of an instance since upload. */
+int bspk_batch_spike_counts(bspk_batch *batch, int inst, int64_t *counts);
+/* (step, neuron) spikes of a recorded instance in the last run. */
+int bspk_batch_spikes_get(bspk_batch *batch, int inst, int64_t cap, int64_t *steps, int32_t *ids,
+                          int64_t *n_out);
+/* An instance's edges as (pre, post, projection) in tile-CSR order. */
+int bspk_batch_edges_get(bspk_batch *batch, int inst, int64_t cap, int32_t *pre, int32_t *post,
+                         int32_t *proj, int64_t *n_out);
+int64_t bspk_batch_step_count(bspk_batch *batch);
+int bspk_batch_last_kernel_time(bspk_batch *batch, double *ms, int64_t *launches);
+
 /* No-allocation entry point (no counterpart in the reference).  For callers
  * that cannot call cudaMalloc -- code running inside another framework's
  * memory pool or allocation hooks, or a plugin host that forbids device
