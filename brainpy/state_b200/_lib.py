@@ -28,6 +28,14 @@ class Config(C.Structure):
                 ("spike_capacity", C.c_int64)]
 
 
+class AdjointConfig(C.Structure):
+    _fields_ = [("dt", C.c_double), ("precision", C.c_int), ("n", C.c_int), ("n_in", C.c_int),
+                ("batch", C.c_int), ("n_steps", C.c_int), ("ckpt_every", C.c_int),
+                ("n_readout", C.c_int), ("readout_tau", C.c_double), ("slope", C.c_double),
+                ("relaxed", C.c_int), ("detach_reset", C.c_int), ("device", C.c_int),
+                ("params", C.c_double * 9)]
+
+
 class StdpParams(C.Structure):
     _fields_ = [("tau_plus", C.c_double), ("tau_minus", C.c_double), ("lambda_", C.c_double),
                 ("alpha", C.c_double), ("mu_plus", C.c_double), ("mu_minus", C.c_double),
@@ -100,6 +108,11 @@ def lib():
             "bspk_batch_edges_get": (C.c_int, [vp, C.c_int, i64, vp, vp, vp, C.POINTER(i64)]),
             "bspk_batch_step_count": (i64, [vp]),
             "bspk_batch_last_kernel_time": (C.c_int, [vp, C.POINTER(dbl), C.POINTER(i64)]),
+            "bspk_adjoint_create": (C.c_int, [C.POINTER(AdjointConfig), vp, vp, i64,
+                                              C.POINTER(vp)]),
+            "bspk_adjoint_destroy": (C.c_int, [vp]),
+            "bspk_adjoint_forward": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
+            "bspk_adjoint_backward": (C.c_int, [vp, vp, vp, vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

@@ -31,8 +31,9 @@ SOURCES = {
     "batch.cu": [],
     "batch_host.cpp": [],
     "conn_gen.cu": [],
-    "adjoint.cu": [],
+    "adjoint.cu": ["-fmad=false"],
     "checkpoint.cpp": [],
+    "xla_ffi.cpp": [],
 }
 HEADERS = ["common.cuh", "device_types.h", "lif_args.h", "aeif_args.h", "stdp_args.h",
            "host_rng.h", "batch_args.h", "plan_internal.h", "conn_gen.h", "conn_gen.cuh",

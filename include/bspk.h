@@ -213,6 +213,43 @@ int bspk_batch_edges_get(bspk_batch *batch, int inst, int64_t cap, int32_t *pre,
 int64_t bspk_batch_step_count(bspk_batch *batch);
 int bspk_batch_last_kernel_time(bspk_batch *batch, double *ms, int64_t *launches);
 
+/* ---------------------------------------------------------------- gradients
+ * Surrogate-gradient BPTT through a recurrent iaf_psc_exp network with a
+ * hand-written adjoint: the forward pass stores checkpoints every
+ * ckpt_every steps, the backward pass recomputes each segment from its
+ * checkpoint and sweeps the adjoint through it.  Replaces jax.grad over the
+ * reference's episode scan (BPTT._episode/_objective,
+ * _kernel/learn/bptt.py:437-491) for this model: hard forward with the
+ * count_ste surrogate (_kernel/spiking.py:65-88), soft reset gradient unless
+ * detach_reset (SpikeRule._jump, _kernel/spiking.py:449-466), or the relaxed
+ * forward (_check_relaxed, :422-447); loss = mean (z - y)^2 of readout rates
+ * z_t = alpha z_{t-1} + c s_t (rate_mse, _kernel/learn/bptt.py:142-214).
+ * Surrogate: fast sigmoid of the given slope (1/mV) as a smooth step,
+ * s(m) = (1 + b m / (1 + b|m|)) / 2 with derivative (b/2) / (1 + b|m|)^2.
+ * Structure: W row-major over post neurons (row_ptr[n+1], col[nnz] = pre).
+ * Operands of forward/backward are DEVICE pointers of the precision's type
+ * (float or double): w[nnz], w_in[n][n_in], inputs = uint8 counts
+ * [n_steps][batch][n_in], targets [n_steps][batch][n_readout]; loss is a
+ * device double, n_spikes an optional device int64.  backward writes dL/dw
+ * and dL/dw_in for the operands of the last forward on the handle. */
+typedef struct {
+    double dt;
+    int precision;          /* 32 or 64 */
+    int n, n_in, batch, n_steps, ckpt_every, n_readout;
+    double readout_tau;     /* ms */
+    double slope;           /* 1/mV */
+    int relaxed, detach_reset, device;
+    double params[9];       /* iaf_psc_exp: E_L C_m tau_m t_ref V_th V_reset tau_syn_ex tau_syn_in I_e */
+} bspk_adjoint_config;
+typedef struct bspk_adjoint bspk_adjoint;
+int bspk_adjoint_create(const bspk_adjoint_config *cfg, const int64_t *row_ptr,
+                        const int32_t *col, int64_t nnz, bspk_adjoint **out);
+int bspk_adjoint_destroy(bspk_adjoint *adj);
+int bspk_adjoint_forward(bspk_adjoint *adj, const void *w, const void *w_in,
+                         const uint8_t *inputs, const void *targets, double *loss,
+                         int64_t *n_spikes, void *stream);
+int bspk_adjoint_backward(bspk_adjoint *adj, void *dw, void *dw_in, void *stream);
+
 /* No-allocation entry point (no counterpart in the reference).  For callers
  * that cannot call cudaMalloc -- code running inside another framework's
  * memory pool or allocation hooks, or a plugin host that forbids device

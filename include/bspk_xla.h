@@ -1,0 +1,34 @@
+/*
+ * bspk_xla.h -- XLA GPU custom-call targets exported by libbspk.so.
+ *
+ * Untyped custom-call ABI (register with jax.ffi.register_ffi_target(name,
+ * jax.ffi.pycapsule(fn), platform="CUDA", api_version=0)); `stream` is the
+ * cudaStream_t XLA passes.  The reference has no FFI: its hot path is JAX
+ * with brainevent primitives (_nest_network/projections.py:56-59,
+ * _kernel/delay_scatter.py:243-347); these targets put the library's kernels
+ * inside a jitted JAX program instead.  `opaque` holds the 8-byte address of a
+ * handle made through bspk.h, followed by the per-target integers below.
+ */
+#ifndef BSPK_XLA_H
+#define BSPK_XLA_H
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* buffers [w, w_in, inputs, targets | loss];  opaque: bspk_adjoint* */
+void bspk_xla_adjoint_forward(void *stream, void **buffers, const char *opaque, size_t len);
+/* buffers [w, w_in, inputs, targets | dw, dw_in];  opaque: bspk_adjoint*, double* (device
+ * scratch for the recomputed loss) */
+void bspk_xla_adjoint_backward(void *stream, void **buffers, const char *opaque, size_t len);
+/* buffers [| step];  opaque: bspk_plan*, int64 n_steps (Simulator.simulate/cont,
+ * _nest_network/simulator.py:1790-1883) */
+void bspk_xla_run(void *stream, void **buffers, const char *opaque, size_t len);
+/* buffers [| step];  opaque: bspk_batch*, int64 n_steps */
+void bspk_xla_batch_run(void *stream, void **buffers, const char *opaque, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -91,6 +91,22 @@ int64_t bo_step_count(bo_sim *s);
 int bo_n_total(bo_sim *s);
 int64_t bo_rk_substeps(bo_sim *s);
 
+/* Surrogate-gradient BPTT through a recurrent iaf_psc_exp network
+ * (bspk_oracle_bptt.c).  W is given row-major over post neurons:
+ * row_ptr[n+1], col[nnz] = pre, w[nnz]; w_in is [n][n_in]; inputs are
+ * counts [n_steps][batch][n_in]; targets [n_steps][batch][n_readout].
+ * dw / dw_in may be NULL (forward only). */
+typedef struct {
+    double dt;
+    int n, n_in, batch, n_steps, n_readout;
+    double readout_tau, slope;
+    int relaxed, detach_reset;
+    double params[9]; /* E_L C_m tau_m t_ref V_th V_reset tau_syn_ex tau_syn_in I_e */
+} bo_bptt_cfg;
+int bo_lif_bptt(const bo_bptt_cfg *c, const int64_t *row_ptr, const int32_t *col, int64_t nnz,
+                const double *w, const double *w_in, const uint8_t *inputs, const double *targets,
+                double *loss, double *dw, double *dw_in, int64_t *n_spikes);
+
 #ifdef __cplusplus
 }
 #endif

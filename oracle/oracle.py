@@ -36,6 +36,13 @@ MODEL_IDS = {"iaf_psc_alpha": 0, "iaf_psc_exp": 1, "aeif_cond_alpha": 2}
 LEGACY, RING = 0, 1
 
 
+class BpttCfg(C.Structure):
+    _fields_ = [("dt", C.c_double), ("n", C.c_int), ("n_in", C.c_int), ("batch", C.c_int),
+                ("n_steps", C.c_int), ("n_readout", C.c_int), ("readout_tau", C.c_double),
+                ("slope", C.c_double), ("relaxed", C.c_int), ("detach_reset", C.c_int),
+                ("params", C.c_double * 9)]
+
+
 def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
 
@@ -82,6 +89,8 @@ def lib():
         L.bo_alpha_p31_p32.argtypes = [dbl, dbl, dbl, dbl, vp, vp]
         L.bo_propagator_exp.restype = dbl
         L.bo_propagator_exp.argtypes = [dbl, dbl, dbl, dbl]
+        L.bo_lif_bptt.argtypes = [C.POINTER(BpttCfg), vp, vp, i64, vp, vp, vp, vp, vp, vp, vp,
+                                  vp]
         _LIB = L
     return _LIB
 
@@ -264,3 +273,31 @@ class OracleSim:
     @property
     def rk_substeps(self):
         return self._L.bo_rk_substeps(self._h)
+
+
+def lif_bptt(cfg, row_ptr, col, w, w_in, inputs, targets, grad=True):
+    """Surrogate-gradient BPTT restatement (bspk_oracle_bptt.c): returns
+    (loss, dw, dw_in, n_spikes); dw/dw_in are None when grad is False.
+    cfg: dt, n, n_in, batch, n_steps, n_readout, readout_tau, slope, relaxed,
+    detach_reset, params (9 iaf_psc_exp parameters)."""
+    c = BpttCfg(cfg["dt"], cfg["n"], cfg["n_in"], cfg["batch"], cfg["n_steps"],
+                cfg["n_readout"], cfg["readout_tau"], cfg["slope"], int(cfg.get("relaxed", 0)),
+                int(cfg.get("detach_reset", 0)), (C.c_double * 9)(*cfg["params"]))
+    row_ptr = np.ascontiguousarray(row_ptr, np.int64)
+    col = np.ascontiguousarray(col, np.int32)
+    w = np.ascontiguousarray(w, np.float64)
+    w_in = np.ascontiguousarray(w_in, np.float64)
+    inputs = np.ascontiguousarray(inputs, np.uint8)
+    targets = np.ascontiguousarray(targets, np.float64)
+    loss = np.zeros(1, np.float64)
+    nsp = np.zeros(1, np.int64)
+    dw = np.zeros(max(col.size, 1), np.float64) if grad else None
+    dwi = np.zeros(max(w_in.size, 1), np.float64) if grad else None
+    rc = lib().bo_lif_bptt(C.byref(c), _p(row_ptr), _p(col), int(col.size), _p(w), _p(w_in),
+                           _p(inputs), _p(targets), _p(loss), _p(dw) if grad else None,
+                           _p(dwi) if grad else None, _p(nsp))
+    if rc != 0:
+        raise ValueError("lif_bptt failed")
+    if grad:
+        return float(loss[0]), dw[:col.size], dwi[:w_in.size].reshape(w_in.shape), int(nsp[0])
+    return float(loss[0]), None, None, int(nsp[0])

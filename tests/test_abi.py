@@ -25,6 +25,8 @@ def test_library_exports_every_declared_symbol():
     assert len(names) >= 20
     for n in names:
         assert hasattr(L, n), n
+    for n in _declared("bspk_xla.h"):
+        assert hasattr(L, n), n
     assert b"sm_100a" in L.bspk_version()
 
 
