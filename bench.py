@@ -205,6 +205,9 @@ def run_ours(args):
         result["fp64"] = fp64_numbers(args, stream, flush)
         result["e2e"] = e2e_numbers(args)
         result["cpu_baseline"] = cpu_baseline(args)
+        if not args.no_extras:
+            result["sweep_batch"] = sweep_numbers(args)
+            result["bptt"] = bptt_numbers(args)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -269,6 +272,124 @@ def e2e_numbers(args):
             "api": "Simulator.simulate(1000 ms)", "rate_hz_E": round(res.rate(esr), 3)}
 
 
+def sweep_numbers(args):
+    """Batched parameter sweep: 256 Brunel instances of uneven sizes in one
+    persistent launch, 1 s simulated, FP32, against the FP64 batch of the same
+    instances (same connectivity and drives) for the per-instance rate error."""
+    import numpy as np
+    import torch
+    from brainpy.state_b200 import brunel
+    specs = brunel.sweep_instances()
+    steps = 10000
+    out = {}
+    for prec in (32, 64):
+        t0 = time.perf_counter()
+        b, params = brunel.build_batch(specs, precision=prec)
+        build_s = time.perf_counter() - t0
+        tile, cps, _ = b.tune(pilot_steps=300)
+        b.run(steps)
+        ms, _ = b.kernel_time()
+        cnt = [b.spike_counts(k) for k in range(len(specs))]
+        out[prec] = dict(ms=ms, build_s=build_s, shape=b.shape(), cnt=cnt, params=params)
+        b.close()
+        torch.cuda.synchronize()
+    N = sum(s["NE"] + s["NI"] for s in specs)
+    edges = sum((s["NE"] + s["NI"]) * (p["CE"] + p["CI"]) for s, p in zip(specs, out[32]["params"]))
+    r32, r64, ev = [], [], 0.0
+    for k, (s, p) in enumerate(zip(specs, out[32]["params"])):
+        n = s["NE"] + s["NI"]
+        c32, c64 = out[32]["cnt"][k], out[64]["cnt"][k]
+        r32.append(c32.sum() / n)
+        r64.append(c64.sum() / n)
+        # out-degree of an E (I) neuron: n * CE / NE (n * CI / NI)
+        ev += c32[:s["NE"]].sum() * n * p["CE"] / s["NE"] + c32[s["NE"]:].sum() * n * p["CI"] / s["NI"]
+    r32, r64 = np.array(r32), np.array(r64)
+    err = np.abs(r32 - r64) / np.maximum(r64, 1e-12)
+    ms32 = out[32]["ms"]
+    return {"workload": "256 Brunel instances, NE~U[500,8000], NI=NE/4, eps=0.1, g~U[3,8], "
+                        "eta~U[0.9,4], delay 1.5 ms, 1000 ms each, one persistent launch",
+            "neurons": int(N), "edges": int(edges),
+            "neuron_updates_per_s": round(N * steps / (ms32 / 1000.0), 1),
+            "syn_events_per_s": round(ev / (ms32 / 1000.0), 1),
+            "ms_per_simulated_s": round(ms32, 3), "ms_fp64": round(out[64]["ms"], 3),
+            "shape_fp32": out[32]["shape"], "build_s": round(out[32]["build_s"], 3),
+            "rate_hz_median": round(float(np.median(r64)), 3),
+            "rate_rel_err_median": round(float(np.median(err)), 5),
+            "rate_rel_err_max": round(float(err.max()), 5),
+            "within_1pct": int((err <= 0.01).sum()), "within_5pct": int((err <= 0.05).sum())}
+
+
+def bptt_numbers(args):
+    """Gradient training workload: loss + gradient through the hand-written
+    adjoint (800 E + 200 I iaf_psc_exp, batch 64, 1000 steps, checkpoint 50),
+    and its finite-difference agreement on 64 random weights (FP64, relaxed
+    forward, 200 steps)."""
+    import numpy as np
+    import torch
+    from brainpy.state_b200.autograd import LifAdjoint
+    from brainpy.state_b200.lif_task import make_task
+    T = make_task()
+    res = {"workload": "800E+200I iaf_psc_exp, 10% recurrent, 100 Poisson inputs, batch 64, "
+                       "1000 steps dt=1 ms, 10 readouts, fast-sigmoid slope 25/mV, checkpoint 50"}
+    for prec in (32, 64):
+        dt = torch.float64 if prec == 64 else torch.float32
+        adj = LifAdjoint(T["cfg"], T["row_ptr"], T["col"], precision=prec, ckpt_every=50)
+        w = torch.tensor(T["w"], dtype=dt, device="cuda")
+        wi = torch.tensor(T["w_in"], dtype=dt, device="cuda")
+        inp = torch.tensor(T["inputs"], dtype=torch.uint8, device="cuda")
+        tg = torch.tensor(T["targets"], dtype=dt, device="cuda")
+        for _ in range(2):
+            adj.forward(w, wi, inp, tg)
+            adj.backward()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        k = 3
+        fw = bw = 0.0
+        for _ in range(k):
+            ev[0].record()
+            adj.forward(w, wi, inp, tg)
+            ev[1].record()
+            adj.backward()
+            ev[2].record()
+            torch.cuda.synchronize()
+            fw += ev[0].elapsed_time(ev[1])
+            bw += ev[1].elapsed_time(ev[2])
+        fw, bw = fw / k, bw / k
+        res[f"fp{prec}"] = {"forward_ms": round(fw, 3), "backward_ms": round(bw, 3),
+                            "grads_per_s": round(1000.0 / (fw + bw), 3),
+                            "trial_steps_per_s": round(64 * 1000 * 1000.0 / (fw + bw), 1)}
+        adj.close()
+    # finite differences, h = 1e-3, 64 random weights
+    params = list(T["cfg"]["params"])
+    params[3] = 0.0
+    Tf = make_task(relaxed=True, params=params, n_steps=200)
+    adj = LifAdjoint(Tf["cfg"], Tf["row_ptr"], Tf["col"], precision=64, ckpt_every=50)
+    w = torch.tensor(Tf["w"], dtype=torch.float64, device="cuda")
+    wi = torch.tensor(Tf["w_in"], dtype=torch.float64, device="cuda")
+    inp = torch.tensor(Tf["inputs"], dtype=torch.uint8, device="cuda")
+    tg = torch.tensor(Tf["targets"], dtype=torch.float64, device="cuda")
+    adj.forward(w, wi, inp, tg)
+    dw, dwi = adj.backward()
+    dw, dwi = dw.cpu().numpy(), dwi.cpu().numpy().reshape(-1)
+    rng = np.random.default_rng(7)
+    a_, f_ = [], []
+    for arr, grad in ((w, dw), (wi.reshape(-1), dwi)):
+        for q in rng.choice(arr.numel(), 32, replace=False):
+            wp = arr.clone()
+            wp[q] += 1e-3
+            lp = float(adj.forward(*((wp, wi) if arr is w else (w, wp.reshape(wi.shape))), inp, tg))
+            wp[q] -= 2e-3
+            lm = float(adj.forward(*((wp, wi) if arr is w else (w, wp.reshape(wi.shape))), inp, tg))
+            a_.append(grad[q])
+            f_.append((lp - lm) / 2e-3)
+    a_, f_ = np.array(a_), np.array(f_)
+    rel = np.abs(a_ - f_) / np.maximum(np.abs(f_), 1e-3 * np.abs(f_).max())
+    res["fd_check"] = {"h": 1e-3, "weights": 64, "steps": 200, "batch": 64, "forward": "relaxed",
+                       "max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel))}
+    adj.close()
+    return res
+
+
 def _oracle_network(pl_builder_seed=1234, precision=32):
     """The bench network rebuilt in the float64 oracle (same CSR, drives)."""
     from oracle import oracle as O
@@ -288,17 +409,26 @@ def _oracle_network(pl_builder_seed=1234, precision=32):
     return sim, p
 
 
+def _host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
 def cpu_baseline(args, sample_ms=200.0):
-    """float64 oracle (single thread) on a bounded sample of the workload."""
+    """float64 oracle (all host threads) on a bounded sample of the workload."""
     sim, p = _oracle_network()
+    cores = _host_threads()
+    sim.set_threads(cores)
     n = int(sample_ms / 0.1)
     t0 = time.perf_counter()
     sim.run(n, cap=5_000_000)
     wall = time.perf_counter() - t0
     return {"value": round((sample_ms / 1000.0) / wall, 5), "unit": "x real time",
-            "cores": 1, "kind": "port",
+            "cores": cores, "kind": "port",
             "sample": f"{sample_ms:.0f} ms simulated ({n} steps) of the same network, float64 "
-                      "oracle, one thread"}
+                      f"oracle, {cores} threads (per-neuron phases parallel, delivery serial)"}
 
 
 def run_reference(args):
@@ -308,6 +438,8 @@ def run_reference(args):
     if rank != 0:
         return
     sim, p = _oracle_network()
+    cores = _host_threads()
+    sim.set_threads(cores)
     sample_ms = 50.0
     n = int(sample_ms / 0.1)
     for _ in range(args.warmup):
@@ -326,10 +458,10 @@ def run_reference(args):
            "data": "synthetic (seeded Brunel network)",
            "config": {"workload": "brunel_order2500_per_edge_delay_1.0-3.0ms",
                       "step": f"{sample_ms:.0f} ms simulated (bounded sample)"},
-           "cpu_baseline": {"value": round(rtf, 5), "unit": "x real time", "cores": 1,
+           "cpu_baseline": {"value": round(rtf, 5), "unit": "x real time", "cores": cores,
                             "kind": "port",
                             "sample": f"{sample_ms:.0f} ms simulated per step, float64 "
-                                      "oracle restatement, one thread (the reference is "
+                                      f"oracle restatement, {cores} threads (the reference is "
                                       "JAX, not installable here)"},
            "e2e": {"value": round(rtf, 5), "unit": "x real time (simulated s / wall s)",
                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -343,6 +475,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--quick", action="store_true", help="FP32 headline only")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the sweep-batch and gradient sections")
     ap.add_argument("--sim-ms", type=float, default=1000.0,
                     help="simulated time per bench step (default one second)")
     args = ap.parse_args()

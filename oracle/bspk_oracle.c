@@ -263,6 +263,7 @@ struct bo_sim {
     int32_t *rec;
     int64_t step;
     int64_t rk_substeps;
+    int threads;  /* OpenMP threads of the independent per-neuron phases */
     double *acc; /* [2][ntot] input accumulator */
     double *y;   /* [2][ntot] per-projection vector */
 };
@@ -487,6 +488,11 @@ int64_t bo_step_count(bo_sim *s) { return s->step; }
 int bo_n_total(bo_sim *s) { return s->ntot; }
 int64_t bo_rk_substeps(bo_sim *s) { return s->rk_substeps; }
 
+/* Threads for the per-neuron phases (input take, drives, neuron updates).
+ * Delivery, recording and every sum stay serial in their fixed order, so the
+ * results do not depend on the thread count. */
+void bo_set_threads(bo_sim *s, int n) { s->threads = n > 0 ? n : 1; }
+
 static void alloc_buffers(bo_sim *s) {
     if (s->hist) return;
     int maxd = 0;
@@ -536,6 +542,7 @@ static void legacy_input(bo_sim *s, input_t *in, int64_t n, double *y) {
     for (int t = 0; t < Q->n; ++t) y[t] = 0.0;
     if (in->kind == 1) {
         int64_t emit = n - (in->ddelay + 1);
+#pragma omp parallel for num_threads(s->threads > 0 ? s->threads : 1) schedule(static)
         for (int t = 0; t < Q->n; ++t) {
             int64_t c = drive_count(in, emit, t);
             y[t] = (double)c * in->weight;
@@ -782,6 +789,7 @@ static int step_aeif(bo_sim *s, pop_t *P, int g, double w_ex, double w_in, doubl
         }
         iters++;
     }
+#pragma omp atomic
     s->rk_substeps += iters;
     if (r > 0) r = r - 1;
     /* synaptic jumps after integration (aeif_cond_alpha.py:709-728) */
@@ -844,17 +852,24 @@ int64_t bo_run(bo_sim *s, int64_t n_steps, int64_t *spk_step, int32_t *spk_gid,
                 r1[g] = 0.0;
             }
         }
-        /* phase 2: neurons (NEST order inside each model) */
+        /* phase 2: neurons (NEST order inside each model), independent per
+         * neuron; the spike list is then collected in gid order */
         unsigned char *hrow = s->hist + (size_t)(n % s->H) * (size_t)N;
         for (int p = 0; p < s->npop; ++p) {
             pop_t *P = &s->pops[p];
+            int uns = 0;
+#pragma omp parallel for num_threads(s->threads > 0 ? s->threads : 1) schedule(static) reduction(| : uns)
             for (int k = 0; k < P->n; ++k) {
                 int g = P->off + k, sp;
                 if (s->model == BO_IAF_PSC_ALPHA) sp = step_iaf_alpha(s, P, g, acc0[g], 0.0);
                 else if (s->model == BO_IAF_PSC_EXP) sp = step_iaf_exp(s, P, g, acc0[g], 0.0);
-                else sp = step_aeif(s, P, g, acc0[g], acc1[g], 0.0, &unstable);
+                else sp = step_aeif(s, P, g, acc0[g], acc1[g], 0.0, &uns);
                 hrow[g] = (unsigned char)sp;
-                if (sp) {
+            }
+            unstable |= uns;
+            for (int k = 0; k < P->n; ++k) {
+                int g = P->off + k;
+                if (hrow[g]) {
                     if (nspk < cap) {
                         spk_step[nspk] = n;
                         spk_gid[nspk] = g;
@@ -872,6 +887,7 @@ int64_t bo_run(bo_sim *s, int64_t n_steps, int64_t *spk_step, int32_t *spk_gid,
                 double *rb = s->ring + (size_t)(in->receptor == 1 ? s->L : 0) * (size_t)N;
                 if (in->kind == 1) {
                     size_t slot = (size_t)((n + in->ddelay) % s->L);
+#pragma omp parallel for num_threads(s->threads > 0 ? s->threads : 1) schedule(static)
                     for (int t = 0; t < Q->n; ++t) {
                         int64_t c = drive_count(in, n, t);
                         if (c) rb[slot * (size_t)N + (size_t)(Q->off + t)] += (double)c * in->weight;

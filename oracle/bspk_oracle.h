@@ -90,6 +90,7 @@ int bo_step_neuron(bo_sim *s, int gid, double w0, double w1, double x_next);
 int64_t bo_step_count(bo_sim *s);
 int bo_n_total(bo_sim *s);
 int64_t bo_rk_substeps(bo_sim *s);
+void bo_set_threads(bo_sim *s, int n);
 
 /* Surrogate-gradient BPTT through a recurrent iaf_psc_exp network
  * (bspk_oracle_bptt.c).  W is given row-major over post neurons:

@@ -74,6 +74,7 @@ def lib():
         L.bo_n_total.argtypes = [vp]
         L.bo_rk_substeps.restype = i64
         L.bo_rk_substeps.argtypes = [vp]
+        L.bo_set_threads.argtypes = [vp, C.c_int]
         L.bo_threefry2x32.argtypes = [u32, u32, u32, u32, vp, vp]
         L.bo_jax_key.argtypes = [i64, vp]
         L.bo_jax_fold_in.argtypes = [vp, u32, vp]
@@ -188,6 +189,10 @@ class OracleSim:
         self.model = model
         self._h = self._L.bo_create(self.dt, int(semantics), MODEL_IDS[model])
         self._keep = []
+
+    def set_threads(self, n):
+        """OpenMP threads of the per-neuron phases (results do not change)."""
+        self._L.bo_set_threads(self._h, int(n))
 
     def __del__(self):
         if getattr(self, "_h", None):
