@@ -113,6 +113,10 @@ def lib():
             "bspk_adjoint_destroy": (C.c_int, [vp]),
             "bspk_adjoint_forward": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
             "bspk_adjoint_backward": (C.c_int, [vp, vp, vp, vp]),
+            "bspk_xla_adjoint_forward": (None, [vp, vp, C.c_char_p, C.c_size_t]),
+            "bspk_xla_adjoint_backward": (None, [vp, vp, C.c_char_p, C.c_size_t]),
+            "bspk_xla_run": (None, [vp, vp, C.c_char_p, C.c_size_t]),
+            "bspk_xla_batch_run": (None, [vp, vp, C.c_char_p, C.c_size_t]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

@@ -432,6 +432,7 @@ struct bspk_adjoint {
     uint8_t *tr_a = nullptr;
     void *dwb = nullptr, *dwib = nullptr;
     double *loss_b = nullptr;
+    double *loss_dev = nullptr;  // the loss when the caller passes none
     unsigned long long *nspk = nullptr;
     double coef[16] = {};
     const void *targets = nullptr;  // operands of the last forward (borrowed)
@@ -647,6 +648,7 @@ int bspk_adjoint_create(const bspk_adjoint_config *cfg, const int64_t *row_ptr, 
         {&h->dwb, el * B * n_ie},
         {&h->dwib, el * B * NN * NI},
         {reinterpret_cast<void **>(&h->loss_b), 8 * B},
+        {reinterpret_cast<void **>(&h->loss_dev), 8},
         {reinterpret_cast<void **>(&h->nspk), 8},
     };
     for (const Buf &bf : bufs) {
@@ -682,10 +684,11 @@ int bspk_adjoint_destroy(bspk_adjoint *h) {
 
 int bspk_adjoint_forward(bspk_adjoint *h, const void *w, const void *w_in, const uint8_t *inputs,
                          const void *targets, double *loss, int64_t *n_spikes, void *stream) {
-    if (!h || !loss || (!w && h->nnz > 0) || (!w_in && h->cfg.n_in > 0) || !inputs ||
+    if (!h || (!w && h->nnz > 0) || (!w_in && h->cfg.n_in > 0) || !inputs ||
         (!targets && h->cfg.n_readout > 0))
         return fail(BSPK_ERR_ARG, "null argument");
     BSPK_CUDA(cudaSetDevice(h->cfg.device));
+    if (!loss) loss = h->loss_dev;
     h->inputs = inputs;
     h->targets = targets;
     cudaStream_t st = static_cast<cudaStream_t>(stream);

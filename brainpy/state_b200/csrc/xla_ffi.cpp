@@ -34,14 +34,13 @@ void bspk_xla_adjoint_forward(cudaStream_t stream, void **buffers, const char *o
 }
 
 // buffers: [w, w_in, inputs, targets] -> [dw, dw_in]; the forward pass is
-// recomputed here (XLA does not order this call after a particular forward).
+// recomputed here (XLA does not order this call after a particular forward),
+// its loss kept inside the handle.
 void bspk_xla_adjoint_backward(cudaStream_t stream, void **buffers, const char *opaque, size_t len) {
     bspk_adjoint *h = nullptr;
-    double *scratch = nullptr;
     if (!read_opaque(opaque, len, 0, &h) || !h) return;
-    if (!read_opaque(opaque, len, 8, &scratch) || !scratch) return;  // device f64 for the loss
     if (bspk_adjoint_forward(h, buffers[0], buffers[1], static_cast<const uint8_t *>(buffers[2]),
-                             buffers[3], scratch, nullptr, stream) != BSPK_OK)
+                             buffers[3], nullptr, nullptr, stream) != BSPK_OK)
         return;
     bspk_adjoint_backward(h, buffers[4], buffers[5], stream);
 }

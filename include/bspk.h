@@ -230,8 +230,9 @@ int bspk_batch_last_kernel_time(bspk_batch *batch, double *ms, int64_t *launches
  * Operands of forward/backward are DEVICE pointers of the precision's type
  * (float or double): w[nnz], w_in[n][n_in], inputs = uint8 counts
  * [n_steps][batch][n_in], targets [n_steps][batch][n_readout]; loss is a
- * device double, n_spikes an optional device int64.  backward writes dL/dw
- * and dL/dw_in for the operands of the last forward on the handle. */
+ * device double (NULL: kept inside the handle), n_spikes an optional device
+ * int64.  backward writes dL/dw and dL/dw_in for the operands of the last
+ * forward on the handle. */
 typedef struct {
     double dt;
     int precision;          /* 32 or 64 */

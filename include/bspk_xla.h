@@ -19,8 +19,8 @@ extern "C" {
 
 /* buffers [w, w_in, inputs, targets | loss];  opaque: bspk_adjoint* */
 void bspk_xla_adjoint_forward(void *stream, void **buffers, const char *opaque, size_t len);
-/* buffers [w, w_in, inputs, targets | dw, dw_in];  opaque: bspk_adjoint*, double* (device
- * scratch for the recomputed loss) */
+/* buffers [w, w_in, inputs, targets | dw, dw_in];  opaque: bspk_adjoint* (the forward pass
+ * is recomputed inside the call) */
 void bspk_xla_adjoint_backward(void *stream, void **buffers, const char *opaque, size_t len);
 /* buffers [| step];  opaque: bspk_plan*, int64 n_steps (Simulator.simulate/cont,
  * _nest_network/simulator.py:1790-1883) */

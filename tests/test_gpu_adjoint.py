@@ -136,3 +136,34 @@ def test_autograd_function_backward():
     np.testing.assert_allclose(w.grad.cpu().numpy(), 2.0 * dw, rtol=1e-15, atol=0)
     np.testing.assert_allclose(wi.grad.cpu().numpy(), 2.0 * dwi, rtol=1e-15, atol=0)
     adj.close()
+
+
+def test_xla_custom_call_targets_match_the_c_abi():
+    """Call the XLA targets the way XLA does (stream, buffer array, opaque)."""
+    import ctypes as C
+    import struct
+    from brainpy.state_b200 import _lib
+    from brainpy.state_b200.autograd import LifAdjoint
+    T = _small()
+    adj = LifAdjoint(T["cfg"], T["row_ptr"], T["col"], precision=64)
+    dt = torch.float64
+    w = torch.tensor(T["w"], dtype=dt, device="cuda")
+    wi = torch.tensor(T["w_in"], dtype=dt, device="cuda")
+    inp = torch.tensor(T["inputs"], dtype=torch.uint8, device="cuda")
+    tg = torch.tensor(T["targets"], dtype=dt, device="cuda")
+    loss = torch.zeros((), dtype=dt, device="cuda")
+    dw = torch.zeros_like(w)
+    dwi = torch.zeros_like(wi)
+    L = _lib.lib()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    op = struct.pack("<Q", adj._h.value)
+    bufs = (C.c_void_p * 5)(*[t.data_ptr() for t in (w, wi, inp, tg, loss)])
+    L.bspk_xla_adjoint_forward(st, bufs, op, len(op))
+    bufs = (C.c_void_p * 6)(*[t.data_ptr() for t in (w, wi, inp, tg, dw, dwi)])
+    L.bspk_xla_adjoint_backward(st, bufs, op, len(op))
+    torch.cuda.synchronize()
+    ref = _gpu(T)
+    assert float(loss) == ref[0]
+    np.testing.assert_array_equal(dw.cpu().numpy(), ref[1])
+    np.testing.assert_array_equal(dwi.cpu().numpy(), ref[2])
+    adj.close()
