@@ -194,7 +194,7 @@ def run_ours(args):
         "rate_hz": round(rate_hz / (sim_ms / 1000.0), 3),
         "ms_per_time_step": round(ms_step / STEPS_PER_BENCH_STEP, 6),
         "wall_s_timed": round(wall, 4),
-        "gpu_launches": int(args.steps) * 1,
+        "gpu_launches": int(args.steps) * int(launches),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
                      "peak_kind": peak_kind, "kernel": "bspk::k_lif_tiled<float, 0>"},

@@ -24,6 +24,7 @@ struct LifArgs {
     int cdf_total;
     int64_t step0, n_steps, run_step0;
     int W;
+    int pipe;   // tiled kernel: 1 = window j-1 is delivered after window j's update
     int tile;
     int model;
     int64_t *spk_step;
@@ -43,11 +44,14 @@ struct LifArgs {
 // c a CSR over all pre neurons of the edges that target c's tile,
 // ptr[c * (N + 1) + pre] .. ptr[c * (N + 1) + pre + 1] into `edges` (edge
 // word = post_in_tile | lag << 16 | projection << 24); per-window spike
-// records list[2][G][kRecWords] (tagged count word + kRecInline tagged
-// entries) with an overflow area ovf[2][G][list_cap]; per-CTA spike-record
-// counts rec_count[G].
+// records list[kRecBufs][G][kRecWords] (tagged count word + kRecInline
+// tagged entries) with an overflow area ovf[kRecBufs][G][list_cap];
+// per-CTA spike-record counts rec_count[G] (running across the launches of
+// one run); the Poisson drive of every (step, neuron) of the launch, drawn
+// by a separate kernel, drive[(step - drive_step0) * N + neuron].
 constexpr int kRecWords = 16;
 constexpr int kRecInline = kRecWords - 1;
+constexpr int kRecBufs = 4;
 
 template <typename Real>
 struct TiledArgs {
@@ -59,25 +63,25 @@ struct TiledArgs {
     long long *rec_count;
     int list_cap;
     int smem_ptr;   // 1: the tile's CSR bounds are staged in shared memory
+    const Real *drive;
+    int64_t drive_step0;
 };
 
 struct TiledLayout {
-    size_t coef, drive, proj, cdf, ring, drv, spk, ptr, total;
+    size_t coef, proj, ring, drv, spk, ptr, total;
 };
+// drv: double-buffered drive of one window, [2][W][tile]
 __host__ __device__ inline TiledLayout tiled_layout(size_t coef_sz, size_t proj_sz, size_t real_sz,
-                                                    int npop, int ndrive, int nproj, int cdf_total,
-                                                    int tile, int L, int G, int n_ptr) {
+                                                    int npop, int nproj, int tile, int L, int W,
+                                                    int n_ptr) {
     auto al = [](size_t x) { return (x + 15) & ~size_t(15); };
-    (void)G;
     TiledLayout l;
     l.coef = 0;
-    l.drive = al(l.coef + coef_sz * npop);
-    l.proj = al(l.drive + sizeof(DriveDev) * ndrive);
-    l.cdf = al(l.proj + proj_sz * nproj);
-    l.ring = al(l.cdf + sizeof(uint64_t) * cdf_total);
+    l.proj = al(l.coef + coef_sz * npop);
+    l.ring = al(l.proj + proj_sz * nproj);
     l.drv = al(l.ring + real_sz * static_cast<size_t>(L) * tile);
-    l.spk = al(l.drv + real_sz * static_cast<size_t>(kMaxWindow) * tile);
-    l.ptr = al(l.spk + sizeof(uint32_t) * static_cast<size_t>(tile) * kMaxWindow);
+    l.spk = al(l.drv + real_sz * 2 * static_cast<size_t>(W) * tile);
+    l.ptr = al(l.spk + sizeof(uint32_t) * static_cast<size_t>(tile) * W);
     l.total = al(l.ptr + sizeof(int) * static_cast<size_t>(n_ptr));
     return l;
 }
@@ -85,8 +89,11 @@ __host__ __device__ inline TiledLayout tiled_layout(size_t coef_sz, size_t proj_
 template <typename Real>
 cudaError_t launch_lif_tiled(const LifArgs<Real> &a, const TiledArgs<Real> &t2, int grid,
                              cudaStream_t st);
-size_t lif_tiled_smem(int tile, int L, int G, int N, int npop, int ndrive, int nproj,
-                      int cdf_total, bool dbl, bool smem_ptr);
+// Poisson drive of steps [m0, m0 + n) for every neuron into out[(m - m0) * N + g].
+template <typename Real>
+cudaError_t launch_drive_fill(const LifArgs<Real> &a, int64_t m0, int n, Real *out,
+                              cudaStream_t st);
+size_t lif_tiled_smem(int tile, int L, int W, int N, int npop, int nproj, bool dbl, bool smem_ptr);
 
 // Launchers (cooperative, persistent).  Return the cudaError_t of the launch.
 template <typename Real>

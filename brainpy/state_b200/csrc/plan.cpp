@@ -638,9 +638,9 @@ int build_tiled(bspk_plan *p) {
         }
         if (rc) return rc;
     }
-    p->list_cap = tile * kMaxWindow;
-    rc = dalloc(p, &p->d_tlist, static_cast<size_t>(2) * G * kRecWords);
-    if (!rc) rc = dalloc(p, &p->d_tovf, static_cast<size_t>(2) * G * p->list_cap);
+    p->list_cap = tile * p->tW;
+    rc = dalloc(p, &p->d_tlist, static_cast<size_t>(kRecBufs) * G * kRecWords);
+    if (!rc) rc = dalloc(p, &p->d_tovf, static_cast<size_t>(kRecBufs) * G * p->list_cap);
     if (!rc) rc = dalloc(p, &p->d_trec, static_cast<size_t>(G));
     if (rc) return rc;
     BSPK_CUDA(cudaMemset(p->d_trec, 0, sizeof(long long) * G));
@@ -817,17 +817,19 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
         if (J.post_local.size() >= (size_t(1) << 31))
             return fail(BSPK_ERR_UNSUPPORTED, "projection with >= 2^31 edges");
     // tiled (target-partitioned) path: state in registers, ring in shared memory
+    // the tiled kernel delivers a window one iteration late when every lag is
+    // at least 2 W (W is capped at kMaxWindow, so only long delays allow it);
+    // halving W to get there costs more in per-window latency than it saves
     p->tiled = false;
+    p->tW = p->W;
+    p->tpipe = min_lag >= 2 * p->W ? 1 : 0;
+    const int nproj_t = static_cast<int>(p->projs.size());
     if (!exact && !aeif && !plastic && p->tile <= 256 && p->grid <= 160 &&
-        lif_tiled_smem(p->tile, p->L, p->grid, p->N, npop, static_cast<int>(p->drives.size()),
-                       static_cast<int>(p->projs.size()), p->cdf_total, dbl, false) <= 200 * 1024) {
+        lif_tiled_smem(p->tile, p->L, p->tW, p->N, npop, nproj_t, dbl, false) <= 200 * 1024) {
         rc = build_tiled(p);
         if (rc) return rc;
         p->tiled = true;
-        p->smem_ptr = lif_tiled_smem(p->tile, p->L, p->grid, p->N, npop,
-                                     static_cast<int>(p->drives.size()),
-                                     static_cast<int>(p->projs.size()), p->cdf_total, dbl,
-                                     true) <= 200 * 1024;
+        p->smem_ptr = lif_tiled_smem(p->tile, p->L, p->tW, p->N, npop, nproj_t, dbl, true) <= 200 * 1024;
     }
     p->uploaded = true;
     p->step = 0;
@@ -881,6 +883,51 @@ LifArgs<Real> lif_args(bspk_plan *p, int64_t n_steps) {
 }
 
 
+// Tiled path: the run in launches of at most kDriveBudget bytes of drive;
+// each launch is a drive pass over (step, neuron) then the persistent kernel,
+// with freshly zeroed records (window tags restart per launch).
+constexpr size_t kDriveBudget = size_t(512) << 20;
+
+template <typename Real>
+int run_tiled(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
+    const size_t per_step = sizeof(Real) * static_cast<size_t>(p->N);
+    const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(n_steps, kDriveBudget / per_step));
+    if (p->tdrive_steps < chunk) {
+        if (p->d_tdrive) {
+            cudaFree(p->d_tdrive);
+            p->allocs.erase(std::remove(p->allocs.begin(), p->allocs.end(), p->d_tdrive), p->allocs.end());
+            p->d_tdrive = nullptr;
+        }
+        int rc = dalloc_bytes(p, &p->d_tdrive, per_step * chunk);
+        if (rc) return rc;
+        p->tdrive_steps = chunk;
+    }
+    const int64_t run0 = p->step;
+    int64_t launches = 0;
+    for (int64_t done = 0; done < n_steps; done += chunk) {
+        const int64_t n = std::min<int64_t>(chunk, n_steps - done);
+        LifArgs<Real> a = lif_args<Real>(p, n);
+        a.step0 = run0 + done;
+        a.run_step0 = run0;
+        a.W = p->tW;
+        a.pipe = p->tpipe;
+        BSPK_CUDA(cudaMemsetAsync(p->d_tlist, 0, sizeof(uint32_t) * kRecBufs * p->grid * kRecWords, st));
+        BSPK_CUDA(cudaMemsetAsync(p->d_tovf, 0,
+                                  sizeof(uint32_t) * kRecBufs * static_cast<size_t>(p->grid) * p->list_cap, st));
+        cudaError_t e = launch_drive_fill<Real>(a, a.step0, static_cast<int>(n),
+                                                static_cast<Real *>(p->d_tdrive), st);
+        if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("drive launch: ") + cudaGetErrorString(e));
+        TiledArgs<Real> t2{p->d_tptr, p->d_tedges, static_cast<const Real *>(p->d_tw), p->d_tlist,
+                           p->d_tovf, p->d_trec, p->list_cap, p->smem_ptr ? 1 : 0,
+                           static_cast<const Real *>(p->d_tdrive), a.step0};
+        e = launch_lif_tiled<Real>(a, t2, p->grid, st);
+        if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+        launches += 2;
+    }
+    p->last_launches = launches;
+    return BSPK_OK;
+}
+
 }  // namespace
 
 extern "C" int bspk_run(bspk_plan *p, int64_t n_steps, void *stream) {
@@ -913,12 +960,7 @@ extern "C" int bspk_run(bspk_plan *p, int64_t n_steps, void *stream) {
     cudaError_t e = cudaSuccess;
     bool per_step = p->cfg.model == BSPK_AEIF_COND_ALPHA;
     for (auto &J : p->projs) per_step |= J.plastic;
-    if (p->tiled) {
-        // records of an earlier run must never carry a tag of this one
-        BSPK_CUDA(cudaMemsetAsync(p->d_tlist, 0, sizeof(uint32_t) * 2 * p->grid * kRecWords, st));
-        BSPK_CUDA(cudaMemsetAsync(p->d_tovf, 0,
-                                  sizeof(uint32_t) * 2 * static_cast<size_t>(p->grid) * p->list_cap, st));
-    }
+    if (p->tiled) BSPK_CUDA(cudaMemsetAsync(p->d_trec, 0, sizeof(long long) * p->grid, st));
     if (per_step) {
         int rc = run_per_step(p, n_steps, st);
         if (rc) return rc;
@@ -926,18 +968,9 @@ extern "C" int bspk_run(bspk_plan *p, int64_t n_steps, void *stream) {
         LifArgs<double> a = lif_args<double>(p, n_steps);
         e = launch_lif_exact(a, p->grid, p->block, st);
         p->last_launches = 1;
-    } else if (p->tiled && dbl) {
-        LifArgs<double> a = lif_args<double>(p, n_steps);
-        TiledArgs<double> t2{p->d_tptr, p->d_tedges, static_cast<const double *>(p->d_tw),
-                             p->d_tlist, p->d_tovf, p->d_trec, p->list_cap, p->smem_ptr ? 1 : 0};
-        e = launch_lif_tiled<double>(a, t2, p->grid, st);
-        p->last_launches = 1;
     } else if (p->tiled) {
-        LifArgs<float> a = lif_args<float>(p, n_steps);
-        TiledArgs<float> t2{p->d_tptr, p->d_tedges, static_cast<const float *>(p->d_tw),
-                            p->d_tlist, p->d_tovf, p->d_trec, p->list_cap, p->smem_ptr ? 1 : 0};
-        e = launch_lif_tiled<float>(a, t2, p->grid, st);
-        p->last_launches = 1;
+        int rc = dbl ? run_tiled<double>(p, n_steps, st) : run_tiled<float>(p, n_steps, st);
+        if (rc) return rc;
     } else if (dbl) {
         LifArgs<double> a = lif_args<double>(p, n_steps);
         e = launch_lif_fast<double>(a, p->grid, p->block, st);

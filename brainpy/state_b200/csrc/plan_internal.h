@@ -118,11 +118,15 @@ struct bspk_plan {
     int *d_tptr = nullptr;
     uint32_t *d_tedges = nullptr;
     void *d_tw = nullptr;
-    uint32_t *d_tlist = nullptr;   // spike records [2][G][kRecWords]
-    uint32_t *d_tovf = nullptr;    // record overflow [2][G][list_cap]
+    uint32_t *d_tlist = nullptr;   // spike records [kRecBufs][G][kRecWords]
+    uint32_t *d_tovf = nullptr;    // record overflow [kRecBufs][G][list_cap]
     long long *d_trec = nullptr;   // per-CTA spike-record counts
     int list_cap = 0;
     bool smem_ptr = false;
+    int tW = 1;                    // tiled window (half the smallest lag when pipelined)
+    int tpipe = 0;                 // 1: window j - 1 is delivered after window j's update
+    void *d_tdrive = nullptr;      // Poisson drive of one launch, [steps][N]
+    int64_t tdrive_steps = 0;      // its capacity in steps
 };
 
 namespace bspk {

@@ -118,3 +118,19 @@ def test_empty_and_edge_cases(oracle):
     assert len(st) > 0
     assert _raster(st, g) == _raster(ost, og)
     np.testing.assert_array_equal(pl.v_trace(), ov)
+
+
+def test_tiled_pipelined_long_delays(oracle):
+    """Lags of at least two windows (64-80 steps): the tiled kernel delivers
+    each window one iteration late; spikes must still match the oracle."""
+    net = Net(per_edge_delay=(64, 80), delay=64)
+    rec = np.arange(250)
+    pl = net.to_plan(precision=64, semantics=1, rec=rec)
+    sim = net.to_oracle(oracle, semantics=1, rec=rec)
+    for chunk in (130, 77):
+        pl.run(chunk)
+        st, g = pl.spikes()
+        ost, og, ov = sim.run(chunk)
+        assert len(st) > 0
+        assert _raster(st, g) == _raster(ost, og)
+        np.testing.assert_allclose(pl.v_trace(), ov, rtol=0, atol=1e-9)
