@@ -48,6 +48,7 @@ constexpr int kHalfWarps = kThreads / 16;     // 16 record readers of 16 words e
 constexpr int kRecPerHalf = 10;               // G <= kHalfWarps * kRecPerHalf = 160
 constexpr int kListCap = 2048;                // spikes gathered per window and CTA
 constexpr int kEdgeUnroll = 16;               // edge loads in flight per thread
+constexpr int kEdgeCap = 4096;                // flattened edges mapped per pass
 constexpr int kTagShift = 14;                 // word = tag (18 bits) << 14 | payload
 constexpr uint32_t kPayMask = (1u << kTagShift) - 1u;
 constexpr uint32_t kTagMask = ~kPayMask;
@@ -153,6 +154,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
     __shared__ int s_warp[32];
     __shared__ uint32_t s_list[kListCap];  // gathered spikes: pre gid << 5 | step in window
     __shared__ int s_ibeg[kListCap], s_ioff[kListCap + 1];
+    __shared__ uint16_t s_espk[kEdgeCap];  // spike of each flattened edge of a pass
     __shared__ int s_nsp[2];  // spikes of the window, by window parity
     __shared__ int s_nlist, s_abort;
 
@@ -244,6 +246,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
 #pragma unroll
         for (int i = 0; i < kRecPerHalf; ++i)
             if (hw + kHalfWarps * i < G) pend |= 1u << i;
+        // a first poll issued right after this CTA's own publish mostly finds
+        // the other records not yet written and only adds to the L2 traffic
+        // of the lines being written; waiting about one write latency first
+        // saves a polling round
+        if (!have) __nanosleep(700);
         const uint64_t t_start = gtimer();
         bool first = true;
         while (__any_sync(0xffffffffu, pend != 0u)) {
@@ -327,27 +334,27 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
         const int T = block_scan(s_ioff, S, s_warp);
         if (tid == 0) s_ioff[S] = T;
         __syncthreads();
-        // 3. every edge of the window: thread t takes the contiguous slice
-        //    [t K, (t+1) K) of the flattened edges, finds its first spike once,
-        //    walks forward, and keeps kEdgeUnroll loads in flight
-        const int K = (T + B - 1) / B;
-        const int e_beg = tid * K, e_end = min(T, e_beg + K);
-        if (e_beg < e_end) {
-            int it = 0, hi = S - 1;
-            while (it < hi) {
-                const int mid = (it + hi + 1) >> 1;
-                if (s_ioff[mid] <= e_beg) it = mid; else hi = mid - 1;
+        // 3. every edge of the window, in passes of kEdgeCap flattened edges:
+        //    s_espk maps a flattened edge to its spike, then lane-interleaved
+        //    threads (edge q0 + u B) take 32 consecutive edges per warp
+        //    instruction -- independent index loads, and consecutive targets
+        //    of one bucket for the shared-memory atomics
+        for (int p0 = 0; p0 < T; p0 += kEdgeCap) {
+            const int p1 = min(T, p0 + kEdgeCap);
+            for (int i = tid; i < S; i += B) {
+                const int a0 = max(s_ioff[i], p0), a1 = min(s_ioff[i + 1], p1);
+                for (int q = a0; q < a1; ++q) s_espk[q - p0] = static_cast<uint16_t>(i);
             }
-            int it_end = s_ioff[it + 1];
-            for (int q0 = e_beg; q0 < e_end; q0 += kEdgeUnroll) {
+            __syncthreads();
+            for (int q0 = p0 + tid; q0 < p1; q0 += B * kEdgeUnroll) {
                 int jj[kEdgeUnroll], nm[kEdgeUnroll];
 #pragma unroll
                 for (int u = 0; u < kEdgeUnroll; ++u) {
-                    const int q = q0 + u;
+                    const int q = q0 + u * B;
                     jj[u] = -1;
                     nm[u] = 0;
-                    if (q < e_end) {
-                        while (q >= it_end) it_end = s_ioff[++it + 1];
+                    if (q < p1) {
+                        const int it = s_espk[q - p0];
                         jj[u] = s_ibeg[it] + (q - s_ioff[it]);
                         const int m = slot0 + static_cast<int>(s_list[it] & 31u);
                         nm[u] = m >= L ? m - L : m;
@@ -374,8 +381,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
                     }
                 }
             }
+            __syncthreads();
         }
-        __syncthreads();
     };
 
     uint32_t word[kRecPerHalf];

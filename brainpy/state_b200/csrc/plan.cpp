@@ -824,12 +824,15 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
     p->tW = p->W;
     p->tpipe = min_lag >= 2 * p->W ? 1 : 0;
     const int nproj_t = static_cast<int>(p->projs.size());
+    // dynamic shared memory budget of the tiled kernel: 227 KB minus its ~34 KB
+    // of static arrays
+    const size_t tiled_budget = 190 * 1024;
     if (!exact && !aeif && !plastic && p->tile <= 256 && p->grid <= 160 &&
-        lif_tiled_smem(p->tile, p->L, p->tW, p->N, npop, nproj_t, dbl, false) <= 200 * 1024) {
+        lif_tiled_smem(p->tile, p->L, p->tW, p->N, npop, nproj_t, dbl, false) <= tiled_budget) {
         rc = build_tiled(p);
         if (rc) return rc;
         p->tiled = true;
-        p->smem_ptr = lif_tiled_smem(p->tile, p->L, p->tW, p->N, npop, nproj_t, dbl, true) <= 200 * 1024;
+        p->smem_ptr = lif_tiled_smem(p->tile, p->L, p->tW, p->N, npop, nproj_t, dbl, true) <= tiled_budget;
     }
     p->uploaded = true;
     p->step = 0;
