@@ -53,11 +53,32 @@ constexpr int kRecWords = 16;
 constexpr int kRecInline = kRecWords - 1;
 constexpr int kRecBufs = 4;
 
+// The tiled kernel accumulates arrivals in fixed point: weights are
+// rint(w * 2^k) in int32 (FP32 plans) or int64 (FP64 plans), k chosen per plan
+// so that no ring slot can overflow (|sum| <= max over neurons of the sum of
+// |w| over their in-edges, since an edge contributes at most once per arrival
+// step).  Integer shared-memory atomics are several times faster than
+// floating-point ones here, and integer sums do not depend on the order of
+// the additions.
+template <typename Real>
+struct FixOf;
+template <>
+struct FixOf<float> {
+    using type = int32_t;
+};
+template <>
+struct FixOf<double> {
+    using type = long long;
+};
+
 template <typename Real>
 struct TiledArgs {
+    using Fix = typename FixOf<Real>::type;
     const int *ptr;
     const uint32_t *edges;
-    const Real *w;  // per-edge weights, or nullptr when every projection is homogeneous
+    const Fix *wfix;   // per-edge fixed-point weights, or nullptr when every projection is homogeneous
+    const Fix *wproj;  // per-projection fixed-point weight (homogeneous projections)
+    Real inv_scale;    // 2^-k
     uint32_t *list;
     uint32_t *ovf;
     long long *rec_count;

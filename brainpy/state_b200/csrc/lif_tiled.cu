@@ -47,7 +47,7 @@ constexpr int kThreads = 256;  // one CTA per SM: the whole register file is
 constexpr int kHalfWarps = kThreads / 16;     // 16 record readers of 16 words each
 constexpr int kRecPerHalf = 10;               // G <= kHalfWarps * kRecPerHalf = 160
 constexpr int kListCap = 2048;                // spikes gathered per window and CTA
-constexpr int kEdgeUnroll = 16;               // edge loads in flight per thread
+constexpr int kEdgeUnroll = 8;                // edge loads in flight per thread
 constexpr int kEdgeCap = 4096;                // flattened edges mapped per pass
 constexpr int kTagShift = 14;                 // word = tag (18 bits) << 14 | payload
 constexpr uint32_t kPayMask = (1u << kTagShift) - 1u;
@@ -102,6 +102,11 @@ __device__ __forceinline__ uint64_t gtimer() {
     return t;
 }
 
+__device__ __forceinline__ void fix_add(int32_t *p, int32_t v) { atomicAdd(p, v); }
+__device__ __forceinline__ void fix_add(long long *p, long long v) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(p), static_cast<unsigned long long>(v));
+}
+
 __device__ __forceinline__ uint32_t tag_of(int64_t window) {
     return (static_cast<uint32_t>(window + 1) & 0x3FFFFu) << kTagShift;
 }
@@ -140,17 +145,19 @@ __global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64
 
 template <typename Real, int MODEL>
 __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a, const TiledArgs<Real> t2) {
+    using Fix = typename FixOf<Real>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int W = a.W;
     const TiledLayout lay = tiled_layout(sizeof(PopCoef<Real>), sizeof(ProjDev<Real>), sizeof(Real),
                                          a.npop, a.nproj, a.tile, a.L, W, t2.smem_ptr ? a.N + 1 : 0);
     PopCoef<Real> *s_coef = reinterpret_cast<PopCoef<Real> *>(smem_raw + lay.coef);
     ProjDev<Real> *s_proj = reinterpret_cast<ProjDev<Real> *>(smem_raw + lay.proj);
-    Real *ring_s = reinterpret_cast<Real *>(smem_raw + lay.ring);
+    Fix *ring_s = reinterpret_cast<Fix *>(smem_raw + lay.ring);  // fixed-point arrivals
     Real *drv_s = reinterpret_cast<Real *>(smem_raw + lay.drv);  // [2][W][tile]
     uint32_t *s_spk = reinterpret_cast<uint32_t *>(smem_raw + lay.spk);
     int *s_ptr = reinterpret_cast<int *>(smem_raw + lay.ptr);   // this tile's CSR bounds
     __shared__ int s_off[kMaxPops + 1];
+    __shared__ Fix s_wproj[kMaxInputs];
     __shared__ int s_warp[32];
     __shared__ uint32_t s_list[kListCap];  // gathered spikes: pre gid << 5 | step in window
     __shared__ int s_ibeg[kListCap], s_ioff[kListCap + 1];
@@ -169,13 +176,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
         s_coef[i] = a.coef[i];
         s_off[i] = a.coef[i].off;
     }
-    for (int i = tid; i < a.nproj; i += B) s_proj[i] = a.projs[i];
+    for (int i = tid; i < a.nproj; i += B) {
+        s_proj[i] = a.projs[i];
+        s_wproj[i] = t2.wproj[i];
+    }
     if (t2.smem_ptr)
         for (int i = tid; i <= N; i += B) s_ptr[i] = gptr[i];
-    // arrival ring of this tile: global [L][N] -> shared [L][tile]
+    // arrival ring of this tile (fixed point): global [L][N] -> shared [L][tile]
+    const Fix *ring_g = reinterpret_cast<const Fix *>(a.ring);
     for (int i = tid; i < L * tile; i += B) {
         const int slot = i / tile, tt = i % tile;
-        ring_s[i] = tt < nloc ? a.ring[static_cast<size_t>(slot) * N + cta0 + tt] : Real(0);
+        ring_s[i] = tt < nloc ? ring_g[static_cast<size_t>(slot) * N + cta0 + tt] : Fix(0);
     }
     if (tid == 0) {
         s_abort = 0;
@@ -361,23 +372,23 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
                     }
                 }
                 uint32_t ed[kEdgeUnroll];
-                Real wv[kEdgeUnroll];
+                Fix wv[kEdgeUnroll];
 #pragma unroll
                 for (int u = 0; u < kEdgeUnroll; ++u) {
                     ed[u] = 0u;
-                    wv[u] = Real(0);
+                    wv[u] = Fix(0);
                     if (jj[u] >= 0) {
                         ed[u] = __ldg(t2.edges + jj[u]);
-                        if (t2.w) wv[u] = __ldg(t2.w + jj[u]);
+                        if (t2.wfix) wv[u] = __ldg(t2.wfix + jj[u]);
                     }
                 }
 #pragma unroll
                 for (int u = 0; u < kEdgeUnroll; ++u) {
                     if (jj[u] >= 0) {
-                        if (!t2.w) wv[u] = s_proj[ed[u] >> 24].w0;
+                        if (!t2.wfix) wv[u] = s_wproj[ed[u] >> 24];
                         int slot = nm[u] + static_cast<int>((ed[u] >> 16) & 0xFFu);
                         if (slot >= L) slot -= L;
-                        atomicAdd(ring_s + slot * tile + (ed[u] & 0xFFFFu), wv[u]);
+                        fix_add(ring_s + slot * tile + (ed[u] & 0xFFFFu), wv[u]);
                     }
                 }
             }
@@ -406,8 +417,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
             const Real *drv = drv_s + static_cast<size_t>(j & 1) * W * tile + tid;
             int slot = slot0;
             for (int k = 0; k < Wk; ++k) {
-                const Real x = ring_s[slot * tile + tid] + drv[k * tile];
-                ring_s[slot * tile + tid] = Real(0);
+                const Real x = static_cast<Real>(ring_s[slot * tile + tid]) * t2.inv_scale + drv[k * tile];
+                ring_s[slot * tile + tid] = Fix(0);
                 bool sp;
                 if (MODEL == 0) sp = iaf_alpha_step<Real>(cf, st, r, x);
                 else sp = iaf_exp_step<Real>(cf, st, r, x);
@@ -459,9 +470,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
         for (int i = 0; i < 6; ++i) a.s[i][g] = st[i];
         a.r[g] = r;
     }
+    Fix *ring_out = reinterpret_cast<Fix *>(a.ring);
     for (int i = tid; i < L * nloc; i += B) {
         const int slot = i / nloc, tt = i % nloc;
-        a.ring[static_cast<size_t>(slot) * N + cta0 + tt] = ring_s[slot * tile + tt];
+        ring_out[static_cast<size_t>(slot) * N + cta0 + tt] = ring_s[slot * tile + tt];
     }
     if (tid == 0) t2.rec_count[c] = rec_n;
 }

@@ -625,14 +625,46 @@ int build_tiled(bspk_plan *p) {
     int rc = upload_vec(p, &p->d_tptr, ptr);
     if (!rc) rc = upload_vec(p, &p->d_tedges, edges);
     if (rc) return rc;
+    // fixed-point scale 2^k of the ring: an edge adds at most once per arrival
+    // step, so no slot exceeds the largest per-neuron sum of |w| over in-edges
+    std::vector<double> wsum(N, 0.0);
+    for (auto &J : p->projs) {
+        const int post_off = p->pops[J.post].off;
+        for (size_t e = 0; e < J.post_local.size(); ++e)
+            wsum[post_off + J.post_local[e]] += std::fabs(J.w[e]);
+    }
+    const double wmax = *std::max_element(wsum.begin(), wsum.end());
+    const double limit = p->elt == 8 ? 4.0e18 : 2.0e9;  // below 2^62 / 2^31
+    int k = 40;
+    if (wmax > 0.0) k = static_cast<int>(std::floor(std::log2(limit / wmax)));
+    k = std::max(-60, std::min(k, p->elt == 8 ? 100 : 60));
+    const double scale = std::ldexp(1.0, k);
+    p->tinv_scale = std::ldexp(1.0, -k);
+    std::vector<int64_t> wproj(std::max<size_t>(p->projs.size(), 1), 0);
+    for (size_t j = 0; j < p->projs.size(); ++j) wproj[j] = std::llrint(p->projs[j].w0 * scale);
+    if (p->elt == 8) {
+        std::vector<long long> f(wproj.begin(), wproj.end());
+        long long *d = nullptr;
+        rc = upload_vec(p, &d, f);
+        p->d_twproj = d;
+    } else {
+        std::vector<int32_t> f(wproj.begin(), wproj.end());
+        int32_t *d = nullptr;
+        rc = upload_vec(p, &d, f);
+        p->d_twproj = d;
+    }
+    if (rc) return rc;
     if (hetero) {
         if (p->elt == 8) {
-            double *dw = nullptr;
-            rc = upload_vec(p, &dw, w);
+            std::vector<long long> f(w.size());
+            for (size_t q = 0; q < w.size(); ++q) f[q] = std::llrint(w[q] * scale);
+            long long *dw = nullptr;
+            rc = upload_vec(p, &dw, f);
             p->d_tw = dw;
         } else {
-            std::vector<float> f(w.begin(), w.end());
-            float *dw = nullptr;
+            std::vector<int32_t> f(w.size());
+            for (size_t q = 0; q < w.size(); ++q) f[q] = static_cast<int32_t>(std::llrint(w[q] * scale));
+            int32_t *dw = nullptr;
             rc = upload_vec(p, &dw, f);
             p->d_tw = dw;
         }
@@ -920,8 +952,10 @@ int run_tiled(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
         cudaError_t e = launch_drive_fill<Real>(a, a.step0, static_cast<int>(n),
                                                 static_cast<Real *>(p->d_tdrive), st);
         if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("drive launch: ") + cudaGetErrorString(e));
-        TiledArgs<Real> t2{p->d_tptr, p->d_tedges, static_cast<const Real *>(p->d_tw), p->d_tlist,
-                           p->d_tovf, p->d_trec, p->list_cap, p->smem_ptr ? 1 : 0,
+        using Fix = typename FixOf<Real>::type;
+        TiledArgs<Real> t2{p->d_tptr, p->d_tedges, static_cast<const Fix *>(p->d_tw),
+                           static_cast<const Fix *>(p->d_twproj), static_cast<Real>(p->tinv_scale),
+                           p->d_tlist, p->d_tovf, p->d_trec, p->list_cap, p->smem_ptr ? 1 : 0,
                            static_cast<const Real *>(p->d_tdrive), a.step0};
         e = launch_lif_tiled<Real>(a, t2, p->grid, st);
         if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));

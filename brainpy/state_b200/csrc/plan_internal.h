@@ -117,7 +117,9 @@ struct bspk_plan {
     bool tiled = false;
     int *d_tptr = nullptr;
     uint32_t *d_tedges = nullptr;
-    void *d_tw = nullptr;
+    void *d_tw = nullptr;          // per-edge fixed-point weights (int32 / int64), or null
+    void *d_twproj = nullptr;      // per-projection fixed-point weights
+    double tinv_scale = 1.0;       // 2^-k of the fixed-point ring
     uint32_t *d_tlist = nullptr;   // spike records [kRecBufs][G][kRecWords]
     uint32_t *d_tovf = nullptr;    // record overflow [kRecBufs][G][list_cap]
     long long *d_trec = nullptr;   // per-CTA spike-record counts
