@@ -54,8 +54,10 @@ constexpr uint32_t kPayMask = (1u << kTagShift) - 1u;
 constexpr uint32_t kTagMask = ~kPayMask;
 constexpr uint64_t kPollLimitNs = 2000000000ull;  // 2 s
 
-// Exclusive scan of s[0..n) by the whole block; returns the total.
-__device__ int block_scan(int *s, int n, int *s_warp) {
+// Exclusive scan of s[0..n) by the whole block that also writes s[n] = total
+// and, for the flattened edges below `cap`, the spike of each edge into espk.
+// Returns the total.
+__device__ int block_scan_map(int *s, int n, int *s_warp, uint16_t *espk, int cap) {
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
     const int per = (n + blockDim.x - 1) / blockDim.x;
     const int b0 = tid * per, b1 = min(n, b0 + per);
@@ -84,8 +86,10 @@ __device__ int block_scan(int *s, int n, int *s_warp) {
     for (int i = b0; i < b1; ++i) {
         const int v = s[i];
         s[i] = acc;
+        for (int q = acc; q < min(acc + v, cap); ++q) espk[q] = static_cast<uint16_t>(i);
         acc += v;
     }
+    if (tid == 0) s[n] = total;
     __syncthreads();
     return total;
 }
@@ -115,31 +119,35 @@ __device__ __forceinline__ uint32_t tag_of(int64_t window) {
 // Poisson drive of steps [m0, m0 + n): out[(m - m0) * N + g] = sum over the
 // drives of g's population (creation order) of count * weight, the count
 // drawn by CDF inversion of threefry((seed, 0), (m - lag, index in pop)).
+// Block (x, y) covers neurons [256 x, 256 x + 256) over the steps
+// [y spb, (y + 1) spb): one thread per neuron, its population and drives
+// looked up once, stores coalesced along neurons.
 template <typename Real>
-__global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64_t m0, int n, Real *out) {
+__global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64_t m0, int n, int spb,
+                                                    Real *out) {
     __shared__ int s_off[kMaxPops + 1];
     for (int i = threadIdx.x; i < a.npop; i += blockDim.x) s_off[i] = a.coef[i].off;
     if (threadIdx.x == 0) s_off[a.npop] = a.N;
     __syncthreads();
-    const int64_t total = static_cast<int64_t>(n) * a.N;
-    for (int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; idx < total;
-         idx += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int64_t k = idx / a.N;
-        const int g = static_cast<int>(idx - k * a.N);
-        const int p = find_pop2(s_off, a.npop, g);
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= a.N) return;
+    const int k0 = blockIdx.y * spb, k1 = min(n, k0 + spb);
+    const int p = find_pop2(s_off, a.npop, g);
+    const uint32_t idx = static_cast<uint32_t>(g - s_off[p]);
+    const int q0 = a.pop_drive_ptr[p], q1 = a.pop_drive_ptr[p + 1];
+    for (int k = k0; k < k1; ++k) {
         const int64_t m = m0 + k;
         Real add = Real(0);
-        for (int q = a.pop_drive_ptr[p]; q < a.pop_drive_ptr[p + 1]; ++q) {
-            const DriveDev d = a.drives[a.pop_drive_list[q]];
+        for (int q = q0; q < q1; ++q) {
+            const DriveDev &d = a.drives[a.pop_drive_list[q]];
             const int64_t se = m - d.lag;
             if (d.tmin < se && se <= d.tmax) {
-                const uint64_t u = bits53(d.seed, 0u, static_cast<uint32_t>(se),
-                                          static_cast<uint32_t>(g - s_off[p]));
+                const uint64_t u = bits53(d.seed, 0u, static_cast<uint32_t>(se), idx);
                 const int cnt = poisson_from_table(a.cdf + d.cdf_off, d.cdf_n, u);
                 add += static_cast<Real>(cnt) * static_cast<Real>(d.weight);
             }
         }
-        out[idx] = add;
+        out[static_cast<int64_t>(k) * a.N + g] = add;
     }
 }
 
@@ -247,6 +255,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
         const int64_t e0 = a.step0 + static_cast<int64_t>(e) * W;
         const int slot0 = static_cast<int>(e0 % L);
         const uint32_t *recs = t2.list + static_cast<size_t>(buf) * G * kRecWords;
+        // a gathered spike: its entry and the bounds of its edge bucket
+        auto push = [&](int src, uint32_t word_) {
+            const int pos = atomicAdd(&s_nlist, 1);
+            if (pos < kListCap) {
+                const int pre = src * tile + static_cast<int>((word_ & kPayMask) >> 5);
+                s_list[pos] = (static_cast<uint32_t>(pre) << 5) | (word_ & 31u);
+                const int b0 = t2.smem_ptr ? s_ptr[pre] : __ldg(gptr + pre);
+                const int b1 = t2.smem_ptr ? s_ptr[pre + 1] : __ldg(gptr + pre + 1);
+                s_ibeg[pos] = b0;
+                s_ioff[pos] = b1 - b0;
+            }
+        };
         if (tid == 0) s_nlist = 0;
         __syncthreads();
         // 1. gather: half-warp hw reads records hw + 16 i, lane w word w; every
@@ -284,12 +304,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
                 const unsigned bal = __ballot_sync(0xffffffffu, ok);
                 const bool half_ok = ((lane & 16) ? (bal >> 16) : (bal & 0xFFFFu)) == 0xFFFFu;
                 if (pending && half_ok) {
-                    if (w >= 1 && w <= cnt) {
-                        const int pos = atomicAdd(&s_nlist, 1);
-                        if (pos < kListCap)
-                            s_list[pos] = ((static_cast<uint32_t>(j * tile) +
-                                            ((word[i] & kPayMask) >> 5)) << 5) | (word[i] & 31u);
-                    }
+                    if (w >= 1 && w <= cnt) push(j, word[i]);
                     if (w == 0 && cnt > kRecInline) {  // overflow entries
                         const uint32_t *src =
                             t2.ovf + (static_cast<size_t>(buf) * G + j) * t2.list_cap;
@@ -304,10 +319,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
                                 }
                                 ow = __ldcg(src + q);
                             }
-                            const int pos = atomicAdd(&s_nlist, 1);
-                            if (pos < kListCap)
-                                s_list[pos] = ((static_cast<uint32_t>(j * tile) +
-                                                ((ow & kPayMask) >> 5)) << 5) | (ow & 31u);
+                            push(j, ow);
                         }
                     }
                     pend &= ~(1u << i);
@@ -333,18 +345,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
             __syncthreads();
             return;
         }
-        // 2. bucket bounds of every gathered spike
-        for (int i = tid; i < S; i += B) {
-            const int pre = static_cast<int>(s_list[i] >> 5);
-            const int b0 = t2.smem_ptr ? s_ptr[pre] : __ldg(gptr + pre);
-            const int b1 = t2.smem_ptr ? s_ptr[pre + 1] : __ldg(gptr + pre + 1);
-            s_ibeg[i] = b0;
-            s_ioff[i] = b1 - b0;
-        }
-        __syncthreads();
-        const int T = block_scan(s_ioff, S, s_warp);
-        if (tid == 0) s_ioff[S] = T;
-        __syncthreads();
+        // 2. offsets of the buckets in the flattened edge list (and the
+        //    spike of every edge of the first pass)
+        const int T = block_scan_map(s_ioff, S, s_warp, s_espk, kEdgeCap);
         // 3. every edge of the window, in passes of kEdgeCap flattened edges:
         //    s_espk maps a flattened edge to its spike, then lane-interleaved
         //    threads (edge q0 + u B) take 32 consecutive edges per warp
@@ -352,11 +355,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
         //    of one bucket for the shared-memory atomics
         for (int p0 = 0; p0 < T; p0 += kEdgeCap) {
             const int p1 = min(T, p0 + kEdgeCap);
-            for (int i = tid; i < S; i += B) {
-                const int a0 = max(s_ioff[i], p0), a1 = min(s_ioff[i + 1], p1);
-                for (int q = a0; q < a1; ++q) s_espk[q - p0] = static_cast<uint16_t>(i);
+            if (p0 > 0) {
+                for (int i = tid; i < S; i += B) {
+                    const int a0 = max(s_ioff[i], p0), a1 = min(s_ioff[i + 1], p1);
+                    for (int q = a0; q < a1; ++q) s_espk[q - p0] = static_cast<uint16_t>(i);
+                }
+                __syncthreads();
             }
-            __syncthreads();
             for (int q0 = p0 + tid; q0 < p1; q0 += B * kEdgeUnroll) {
                 int jj[kEdgeUnroll], nm[kEdgeUnroll];
 #pragma unroll
@@ -502,10 +507,12 @@ cudaError_t launch_lif_tiled(const LifArgs<Real> &a, const TiledArgs<Real> &t2, 
 template <typename Real>
 cudaError_t launch_drive_fill(const LifArgs<Real> &a, int64_t m0, int n, Real *out,
                               cudaStream_t st) {
-    const int64_t total = static_cast<int64_t>(n) * a.N;
-    const int grid = static_cast<int>(std::min<int64_t>((total + 255) / 256, 148 * 16));
-    if (grid <= 0) return cudaSuccess;
-    k_drive_fill<Real><<<grid, 256, 0, st>>>(a, m0, n, out);
+    if (n <= 0 || a.N <= 0) return cudaSuccess;
+    const int gx = (a.N + 255) / 256;
+    const int gy = static_cast<int>(std::min<int64_t>(std::max<int64_t>(1, (148 * 16 + gx - 1) / gx),
+                                                      std::min(n, 65535)));
+    const int spb = (n + gy - 1) / gy;
+    k_drive_fill<Real><<<dim3(gx, (n + spb - 1) / spb), 256, 0, st>>>(a, m0, n, spb, out);
     return cudaGetLastError();
 }
 
