@@ -45,6 +45,11 @@ __device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long lon
     return v;
 }
 
+__device__ __forceinline__ void fix_add(int32_t *p, int32_t v) { atomicAdd(p, v); }
+__device__ __forceinline__ void fix_add(long long *p, long long v) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(p), static_cast<unsigned long long>(v));
+}
+
 // Exclusive scan of s[0..n) by the whole block; returns the total.
 __device__ int block_scan_excl(int *s, int n, int *s_warp) {
     const int T = blockDim.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = T >> 5;
@@ -85,12 +90,13 @@ __device__ int block_scan_excl(int *s, int n, int *s_warp) {
 template <typename Real, int MODEL>
 __global__ void __launch_bounds__(kBMaxT) k_lif_batch(const BatchArgs<Real> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Real *acc = reinterpret_cast<Real *>(smem_raw);  // [Wmax][T]
+    using Fix = typename FixOf<Real>::type;
+    Fix *acc = reinterpret_cast<Fix *>(smem_raw);  // [Wmax][T], fixed point
     __shared__ BatchInstDev s_inst;
     __shared__ BatchTileDev s_tile;
     __shared__ DriveDev s_drive[kBatchMaxDrives];
     __shared__ uint64_t s_cdf[kBatchCdfCap];
-    __shared__ Real s_w[kBatchMaxProj];
+    __shared__ Fix s_w[kBatchMaxProj];
     __shared__ uint32_t s_list[kBListCap];  // pre << 6 | arrival step relative to the pass
     __shared__ int s_ibeg[kBListCap], s_ioff[kBListCap + 1];
     __shared__ int s_cnt[kBListCap + 1];    // entries per source tile (then their scan)
@@ -144,7 +150,7 @@ __global__ void __launch_bounds__(kBMaxT) k_lif_batch(const BatchArgs<Real> a) {
                 while (pop + 1 < s_inst.npop && s_inst.pop_off[pop + 1] <= li) ++pop;
                 cf = a.coef[s_inst.coef0 + pop];
             }
-            for (int i = tid; i < Wk * T; i += T) acc[i] = Real(0);
+            for (int i = tid; i < Wk * T; i += T) acc[i] = Fix(0);
             if (tid == 0) {
                 s_nsp = 0;
                 s_nrec = 0;
@@ -252,8 +258,8 @@ __global__ void __launch_bounds__(kBMaxT) k_lif_batch(const BatchArgs<Real> a) {
 #pragma unroll
                             for (int u = 0; u < kBEdgeUnroll; ++u)
                                 if (jj[u] >= 0)
-                                    atomicAdd(acc + sl[u] * T + static_cast<int>(ed[u] & 0xFFFFu),
-                                              s_w[ed[u] >> 16]);
+                                    fix_add(acc + sl[u] * T + static_cast<int>(ed[u] & 0xFFFFu),
+                                            s_w[ed[u] >> 16]);
                         }
                     }
                     __syncthreads();
@@ -271,7 +277,7 @@ __global__ void __launch_bounds__(kBMaxT) k_lif_batch(const BatchArgs<Real> a) {
                 const int pidx = li - s_inst.pop_off[pop];
                 for (int j = 0; j < Wk; ++j) {
                     const int64_t n = sa + j;
-                    Real x = acc[j * T + tid];
+                    Real x = static_cast<Real>(acc[j * T + tid]) * static_cast<Real>(s_inst.inv_scale);
                     for (int d = 0; d < ndr; ++d) {
                         const DriveDev &D = s_drive[d];
                         const int64_t se = n - D.lag;

@@ -15,6 +15,7 @@
 #include <cstdint>
 
 #include "device_types.h"
+#include "lif_args.h"
 
 namespace bspk {
 
@@ -35,7 +36,8 @@ struct BatchInstDev {
     int ndrive, drive0;     // drives; DriveDev.pop is the instance-local pop
     int cdf_n;              // CDF entries of all its drives (DriveDev.cdf_off local)
     int64_t cdf0;
-    int proj0;              // projection weights proj_w[proj0 + slot]
+    int proj0;              // fixed-point projection weights proj_w[proj0 + slot]
+    double inv_scale;       // 2^-k of the instance's fixed-point accumulator
     int rec_cap;            // entries per tile record
     int record;             // keep the spike train (step, neuron) of this instance
     int64_t rec0;           // records of tile t, parity p: rec0 + (2 t + p) * (1 + rec_cap)
@@ -59,7 +61,10 @@ struct BatchArgs {
     const PopCoef<Real> *coef;
     const DriveDev *drives;
     const uint64_t *cdf;
-    const Real *proj_w;
+    // fixed point (int32 for FP32, int64 for FP64): arrivals are accumulated
+    // as integers, w_fix = rint(w 2^k) with k per instance such that no
+    // accumulator slot can overflow
+    const typename FixOf<Real>::type *proj_w;
     Real *s[6];
     int *r;
     const int *ptr;                  // int32 bounds relative to the instance's edge0

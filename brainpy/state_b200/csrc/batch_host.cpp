@@ -54,6 +54,7 @@ struct BInst {
     std::vector<BDrive> drives;
     int n = 0, record = 0, W = 1, ntiles = 0, cdf_n = 0;
     int64_t g0 = 0, edges = 0;
+    double inv_scale = 1.0;
 };
 
 }  // namespace
@@ -176,6 +177,7 @@ int layout(bspk_batch *b, int T) {
         d.cdf_n = I.cdf_n;
         d.cdf0 = cdf0;
         d.proj0 = static_cast<int>(i) * kBatchMaxProj;
+        d.inv_scale = I.inv_scale;
         d.rec_cap = T * std::max(1, per_neuron);
         d.record = I.record;
         d.rec0 = rec_words;
@@ -332,14 +334,14 @@ int launch(bspk_batch *b, int64_t n_steps, cudaStream_t st) {
         BatchArgs<double> a{};
         fill(a);
         a.coef = static_cast<const PopCoef<double> *>(b->d_coef);
-        a.proj_w = static_cast<const double *>(b->d_projw);
+        a.proj_w = static_cast<const long long *>(b->d_projw);
         for (int i = 0; i < 6; ++i) a.s[i] = static_cast<double *>(b->d_s[i]);
         e = launch_lif_batch<double>(a, b->cfg.model, b->G, st);
     } else {
         BatchArgs<float> a{};
         fill(a);
         a.coef = static_cast<const PopCoef<float> *>(b->d_coef);
-        a.proj_w = static_cast<const float *>(b->d_projw);
+        a.proj_w = static_cast<const int32_t *>(b->d_projw);
         for (int i = 0; i < 6; ++i) a.s[i] = static_cast<float *>(b->d_s[i]);
         e = launch_lif_batch<float>(a, b->cfg.model, b->G, st);
     }
@@ -588,7 +590,18 @@ int bspk_batch_upload(bspk_batch *b, int tile, int ctas_per_sm, void *stream) {
             cdf.insert(cdf.end(), D.cdf.begin(), D.cdf.end());
             coff += d.cdf_n;
         }
-        for (size_t p = 0; p < I.projs.size(); ++p) projw[i * kBatchMaxProj + p] = I.projs[p].w;
+        // fixed-point scale: an edge adds at most once per arrival step, so
+        // no slot exceeds the largest per-neuron sum of |w| over in-edges
+        std::vector<double> wsum(I.pops.size(), 0.0);
+        for (const auto &P : I.projs) wsum[P.post] += std::fabs(P.w) * P.K;
+        const double wmax = *std::max_element(wsum.begin(), wsum.end());
+        const double limit = b->elt == 8 ? 4.0e18 : 2.0e9;
+        int k = 40;
+        if (wmax > 0.0) k = static_cast<int>(std::floor(std::log2(limit / wmax)));
+        k = std::max(-60, std::min(k, b->elt == 8 ? 100 : 60));
+        I.inv_scale = std::ldexp(1.0, -k);
+        for (size_t p = 0; p < I.projs.size(); ++p)
+            projw[i * kBatchMaxProj + p] = static_cast<double>(std::llrint(std::ldexp(I.projs[p].w, k)));
     }
     if (lif_batch_smem(tile, b->Wmax, b->elt == 8) > 160 * 1024)
         return fail(BSPK_ERR_UNSUPPORTED, "tile x window accumulator exceeds shared memory");
@@ -607,11 +620,14 @@ int bspk_batch_upload(bspk_batch *b, int tile, int ctas_per_sm, void *stream) {
     if (rc) return rc;
     if (b->elt == 8) {
         BSPK_CUDA(cudaMemcpy(b->d_coef, coef.data(), sizeof(PopCoef<double>) * coef.size(), cudaMemcpyHostToDevice));
-        BSPK_CUDA(cudaMemcpy(b->d_projw, projw.data(), 8 * projw.size(), cudaMemcpyHostToDevice));
+        std::vector<long long> pw(projw.size());
+        for (size_t q = 0; q < projw.size(); ++q) pw[q] = static_cast<long long>(projw[q]);
+        BSPK_CUDA(cudaMemcpy(b->d_projw, pw.data(), 8 * pw.size(), cudaMemcpyHostToDevice));
     } else {
         std::vector<PopCoef<float>> cf;
         for (const auto &c : coef) cf.push_back(cast_coef<float>(c));
-        std::vector<float> pw(projw.begin(), projw.end());
+        std::vector<int32_t> pw(projw.size());
+        for (size_t q = 0; q < projw.size(); ++q) pw[q] = static_cast<int32_t>(projw[q]);
         BSPK_CUDA(cudaMemcpy(b->d_coef, cf.data(), sizeof(PopCoef<float>) * cf.size(), cudaMemcpyHostToDevice));
         BSPK_CUDA(cudaMemcpy(b->d_projw, pw.data(), 4 * pw.size(), cudaMemcpyHostToDevice));
     }
