@@ -21,6 +21,10 @@
 // reading window k, so two record buffers suffice.  Dependencies point to
 // the previous window only and every CTA processes windows in order, so the
 // co-resident grid cannot deadlock; every poll still gives up after 2 s.
+#include <cuda_pipeline.h>
+
+#include <algorithm>
+
 #include "batch_args.h"
 #include "common.cuh"
 
@@ -29,7 +33,7 @@ namespace bspk {
 namespace {
 constexpr int kBMaxT = 512;
 constexpr int kBListCap = 1024;   // gathered spikes per delivery chunk
-constexpr int kBEdgeUnroll = 8;   // edge loads in flight per thread
+constexpr int kBEdgeUnroll = 16;  // edge loads in flight per thread
 constexpr uint64_t kBPollNs = 2000000000ull;
 constexpr uint32_t kCompleteBit = 0x80000000u;
 
@@ -92,10 +96,9 @@ __global__ void __launch_bounds__(kBMaxT) k_lif_batch(const BatchArgs<Real> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using Fix = typename FixOf<Real>::type;
     Fix *acc = reinterpret_cast<Fix *>(smem_raw);  // [Wmax][T], fixed point
+    Real *drv_s = reinterpret_cast<Real *>(smem_raw + sizeof(Fix) * a.Wmax * blockDim.x);  // [Wmax][T]
     __shared__ BatchInstDev s_inst;
     __shared__ BatchTileDev s_tile;
-    __shared__ DriveDev s_drive[kBatchMaxDrives];
-    __shared__ uint64_t s_cdf[kBatchCdfCap];
     __shared__ Fix s_w[kBatchMaxProj];
     __shared__ uint32_t s_list[kBListCap];  // pre << 6 | arrival step relative to the pass
     __shared__ int s_ibeg[kBListCap], s_ioff[kBListCap + 1];
@@ -106,7 +109,7 @@ __global__ void __launch_bounds__(kBMaxT) k_lif_batch(const BatchArgs<Real> a) {
     const int T = blockDim.x, tid = threadIdx.x, c = blockIdx.x;
     const int tb = a.cta_ptr[c], te = a.cta_ptr[c + 1];
     const int64_t n_end = a.step0 + a.n_steps;
-    int64_t rec_n = 0;  // spikes recorded by this CTA in this launch (uniform)
+    int64_t rec_n = a.rec_count ? a.rec_count[c] : 0;  // recorded spikes (uniform), across launches
     int loaded = -1;    // instance whose drives/CDF/weights sit in shared memory
     if (tid == 0) s_abort = 0;
 
@@ -131,8 +134,6 @@ __global__ void __launch_bounds__(kBMaxT) k_lif_batch(const BatchArgs<Real> a) {
             const int n_inst = s_inst.n;
             const int off = static_cast<int>(sa - wa), Wk = static_cast<int>(sb - sa);
             if (tl.inst != loaded) {
-                for (int i = tid; i < s_inst.ndrive; i += T) s_drive[i] = a.drives[s_inst.drive0 + i];
-                for (int i = tid; i < s_inst.cdf_n; i += T) s_cdf[i] = a.cdf[s_inst.cdf0 + i];
                 for (int i = tid; i < kBatchMaxProj; i += T) s_w[i] = a.proj_w[s_inst.proj0 + i];
                 loaded = tl.inst;
             }
@@ -149,7 +150,13 @@ __global__ void __launch_bounds__(kBMaxT) k_lif_batch(const BatchArgs<Real> a) {
                 r = a.r[g];
                 while (pop + 1 < s_inst.npop && s_inst.pop_off[pop + 1] <= li) ++pop;
                 cf = a.coef[s_inst.coef0 + pop];
+                // this window's drive, staged while the window's arrivals are gathered
+                const Real *src = a.drive + (sa - a.drive_step0) * a.n_total + g;
+                for (int j = 0; j < Wk; ++j)
+                    __pipeline_memcpy_async(drv_s + j * T + tid, src + static_cast<int64_t>(j) * a.n_total,
+                                            sizeof(Real));
             }
+            __pipeline_commit();
             for (int i = tid; i < Wk * T; i += T) acc[i] = Fix(0);
             if (tid == 0) {
                 s_nsp = 0;
@@ -272,22 +279,12 @@ __global__ void __launch_bounds__(kBMaxT) k_lif_batch(const BatchArgs<Real> a) {
                 a.recs + s_inst.rec0 + static_cast<int64_t>(2 * tl.tloc + (k & 1)) * (1 + cap);
             const unsigned long long tag = static_cast<unsigned long long>(k + 1) << 32;
             int nsp_local = 0;
+            __pipeline_wait_prior(0);
             if (own) {
-                const int ndr = s_inst.ndrive;
-                const int pidx = li - s_inst.pop_off[pop];
                 for (int j = 0; j < Wk; ++j) {
                     const int64_t n = sa + j;
-                    Real x = static_cast<Real>(acc[j * T + tid]) * static_cast<Real>(s_inst.inv_scale);
-                    for (int d = 0; d < ndr; ++d) {
-                        const DriveDev &D = s_drive[d];
-                        const int64_t se = n - D.lag;
-                        if (D.pop == pop && D.tmin < se && se <= D.tmax) {
-                            const uint64_t u = bits53(D.seed, 0u, static_cast<uint32_t>(se),
-                                                      static_cast<uint32_t>(pidx));
-                            const int cnt = poisson_from_table(s_cdf + D.cdf_off, D.cdf_n, u);
-                            x += static_cast<Real>(cnt) * static_cast<Real>(D.weight);
-                        }
-                    }
+                    const Real x = static_cast<Real>(acc[j * T + tid]) * static_cast<Real>(s_inst.inv_scale) +
+                                   drv_s[j * T + tid];
                     bool sp;
                     if (MODEL == 0) sp = iaf_alpha_step<Real>(cf, st, r, x);
                     else sp = iaf_exp_step<Real>(cf, st, r, x);
@@ -334,8 +331,62 @@ __global__ void __launch_bounds__(kBMaxT) k_lif_batch(const BatchArgs<Real> a) {
 }
 
 size_t lif_batch_smem(int T, int Wmax, int dbl) {
-    return static_cast<size_t>(T) * Wmax * (dbl ? 8 : 4);
+    return static_cast<size_t>(T) * Wmax * (dbl ? 16 : 8);  // fixed-point arrivals + drive
 }
+
+// Drive pass: thread per neuron over a run of steps.  out[(m - m0) N + g] =
+// sum over the drives of g's population (creation order) of count * weight,
+// count by CDF inversion of threefry((seed, 0), (m - lag, index in pop)).
+template <typename Real>
+__global__ void __launch_bounds__(256) k_batch_drive_fill(const BatchArgs<Real> a, int64_t m0, int n,
+                                                          int spb, Real *out) {
+    const int64_t g = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+    if (g >= a.n_total) return;
+    int lo = 0, hi = a.n_inst - 1;  // instance of g: last with g0 <= g
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a.inst[mid].g0 <= g) lo = mid; else hi = mid - 1;
+    }
+    const BatchInstDev &I = a.inst[lo];
+    const int li = static_cast<int>(g - I.g0);
+    int pop = 0;
+    while (pop + 1 < I.npop && I.pop_off[pop + 1] <= li) ++pop;
+    const uint32_t idx = static_cast<uint32_t>(li - I.pop_off[pop]);
+    const int k0 = blockIdx.y * spb, k1 = min(n, k0 + spb);
+    for (int k = k0; k < k1; ++k) {
+        const int64_t m = m0 + k;
+        Real add = Real(0);
+        for (int d = 0; d < I.ndrive; ++d) {
+            const DriveDev &D = a.drives[I.drive0 + d];
+            const int64_t se = m - D.lag;
+            if (D.pop == pop && D.tmin < se && se <= D.tmax) {
+                const uint64_t u = bits53(D.seed, 0u, static_cast<uint32_t>(se), idx);
+                const int cnt = poisson_from_table(a.cdf + I.cdf0 + D.cdf_off, D.cdf_n, u);
+                add += static_cast<Real>(cnt) * static_cast<Real>(D.weight);
+            }
+        }
+        out[static_cast<int64_t>(k) * a.n_total + g] = add;
+    }
+}
+
+template <typename Real>
+cudaError_t launch_batch_drive_fill(const BatchArgs<Real> &a, int64_t m0, int n, Real *out,
+                                    cudaStream_t st) {
+    if (n <= 0 || a.n_total <= 0) return cudaSuccess;
+    const int64_t gx = (a.n_total + 255) / 256;
+    if (gx > 2147483647) return cudaErrorInvalidValue;
+    const int gy = static_cast<int>(std::min<int64_t>(std::max<int64_t>(1, (148 * 16 + gx - 1) / gx),
+                                                      std::min(n, 65535)));
+    const int spb = (n + gy - 1) / gy;
+    k_batch_drive_fill<Real><<<dim3(static_cast<unsigned>(gx), (n + spb - 1) / spb), 256, 0, st>>>(
+        a, m0, n, spb, out);
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_batch_drive_fill<float>(const BatchArgs<float> &, int64_t, int, float *,
+                                                    cudaStream_t);
+template cudaError_t launch_batch_drive_fill<double>(const BatchArgs<double> &, int64_t, int,
+                                                     double *, cudaStream_t);
 
 template <typename Real>
 cudaError_t launch_lif_batch(const BatchArgs<Real> &a, int model, int grid, cudaStream_t st) {

@@ -78,6 +78,9 @@ struct BatchArgs {
     long long *rec_count;            // per CTA
     int64_t spk_cap;
     int64_t step0, n_steps;
+    int64_t n_total;                 // neurons of all instances
+    const Real *drive;               // Poisson drive drive[(step - drive_step0) * n_total + g]
+    int64_t drive_step0;
     int *err;
 };
 
@@ -86,5 +89,9 @@ template <typename Real>
 cudaError_t launch_lif_batch(const BatchArgs<Real> &a, int model, int grid, cudaStream_t st);
 template <typename Real>
 int lif_batch_max_ctas_per_sm(int model, int T, int Wmax);
+// Poisson drive of every neuron of every instance for steps [m0, m0 + n).
+template <typename Real>
+cudaError_t launch_batch_drive_fill(const BatchArgs<Real> &a, int64_t m0, int n, Real *out,
+                                    cudaStream_t st);
 
 }  // namespace bspk

@@ -77,6 +77,8 @@ struct bspk_batch {
     uint64_t *d_cdf = nullptr;
     void *d_projw = nullptr;
     int *d_err = nullptr;
+    void *d_drive = nullptr;       // Poisson drive of one launch, [steps][Ntot]
+    int64_t drive_steps = 0;
     // layout (depends on T) and assignment (depends on G)
     std::vector<void *> lay_allocs, asg_allocs;
     BatchInstDev *d_inst = nullptr;
@@ -299,11 +301,35 @@ int max_cps(bspk_batch *b, int T) {
                        : lif_batch_max_ctas_per_sm<float>(b->cfg.model, T, b->Wmax);
 }
 
-int launch(bspk_batch *b, int64_t n_steps, cudaStream_t st) {
+// One run: in chunks of at most kBatchDriveBudget bytes of drive, each a
+// drive pass over (step, neuron) then the persistent kernel.
+constexpr size_t kBatchDriveBudget = size_t(4) << 30;
+
+template <typename Real>
+int launch_typed(bspk_batch *b, int64_t n_steps, cudaStream_t st) {
+    using Fix = typename FixOf<Real>::type;
+    const size_t per_step = sizeof(Real) * static_cast<size_t>(b->Ntot);
+    int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(n_steps, kBatchDriveBudget / per_step));
+    if (chunk >= b->Wmax && chunk < n_steps) chunk -= chunk % b->Wmax;  // whole windows when they share W
+    if (b->drive_steps < chunk) {
+        for (auto it = b->allocs.begin(); it != b->allocs.end(); ++it)
+            if (*it == b->d_drive) {
+                cudaFree(*it);
+                b->allocs.erase(it);
+                break;
+            }
+        b->d_drive = nullptr;
+        int rc = balloc(b->allocs, &b->d_drive, per_step * chunk);
+        if (rc) return rc;
+        b->drive_steps = chunk;
+    }
     BSPK_CUDA(cudaMemsetAsync(b->d_err, 0, sizeof(int), st));
     if (b->d_rec_count) BSPK_CUDA(cudaMemsetAsync(b->d_rec_count, 0, sizeof(long long) * b->G, st));
-    cudaError_t e;
-    auto fill = [&](auto &a) {
+    BSPK_CUDA(cudaEventRecord(b->ev0, st));
+    int64_t launches = 0;
+    for (int64_t done = 0; done < n_steps; done += chunk) {
+        const int64_t n = std::min<int64_t>(chunk, n_steps - done);
+        BatchArgs<Real> a{};
         a.n_tiles = static_cast<int>(b->h_tiles.size());
         a.n_inst = static_cast<int>(b->inst.size());
         a.T = b->T;
@@ -325,31 +351,30 @@ int launch(bspk_batch *b, int64_t n_steps, cudaStream_t st) {
         a.spk_inst = b->d_spk_inst;
         a.rec_count = b->d_rec_count;
         a.spk_cap = b->spk_cap;
-        a.step0 = b->step;
-        a.n_steps = n_steps;
+        a.step0 = b->step + done;
+        a.n_steps = n;
+        a.n_total = b->Ntot;
+        a.drive = static_cast<const Real *>(b->d_drive);
+        a.drive_step0 = a.step0;
         a.err = b->d_err;
-    };
-    BSPK_CUDA(cudaEventRecord(b->ev0, st));
-    if (b->elt == 8) {
-        BatchArgs<double> a{};
-        fill(a);
-        a.coef = static_cast<const PopCoef<double> *>(b->d_coef);
-        a.proj_w = static_cast<const long long *>(b->d_projw);
-        for (int i = 0; i < 6; ++i) a.s[i] = static_cast<double *>(b->d_s[i]);
-        e = launch_lif_batch<double>(a, b->cfg.model, b->G, st);
-    } else {
-        BatchArgs<float> a{};
-        fill(a);
-        a.coef = static_cast<const PopCoef<float> *>(b->d_coef);
-        a.proj_w = static_cast<const int32_t *>(b->d_projw);
-        for (int i = 0; i < 6; ++i) a.s[i] = static_cast<float *>(b->d_s[i]);
-        e = launch_lif_batch<float>(a, b->cfg.model, b->G, st);
+        a.coef = static_cast<const PopCoef<Real> *>(b->d_coef);
+        a.proj_w = static_cast<const Fix *>(b->d_projw);
+        for (int i = 0; i < 6; ++i) a.s[i] = static_cast<Real *>(b->d_s[i]);
+        cudaError_t e = launch_batch_drive_fill<Real>(a, a.step0, static_cast<int>(n),
+                                                      static_cast<Real *>(b->d_drive), st);
+        if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("drive launch: ") + cudaGetErrorString(e));
+        e = launch_lif_batch<Real>(a, b->cfg.model, b->G, st);
+        if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
+        launches += 2;
     }
-    if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
     BSPK_CUDA(cudaEventRecord(b->ev1, st));
-    b->last_launches = 1;
+    b->last_launches = launches;
     b->step += n_steps;
     return BSPK_OK;
+}
+
+int launch(bspk_batch *b, int64_t n_steps, cudaStream_t st) {
+    return b->elt == 8 ? launch_typed<double>(b, n_steps, st) : launch_typed<float>(b, n_steps, st);
 }
 
 int check_err(bspk_batch *b, cudaStream_t st) {
