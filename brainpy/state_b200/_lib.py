@@ -241,13 +241,16 @@ class Plan:
         self._last_steps = int(n_steps)
 
     def spikes(self, cap=None):
-        if cap is None:
-            cap = 1 << 24
-        st = np.zeros(cap, np.int64)
-        g = np.zeros(cap, np.int32)
+        """(steps, gids) of the last run's recorded spikes, sorted by step then gid."""
         n = C.c_int64()
-        check(self._L.bspk_spikes_get(self._h, int(cap), ptr(st), ptr(g), C.byref(n)))
-        m = n.value
+        if cap is None:  # ask for the count first, then copy exactly that many
+            check(self._L.bspk_spikes_get(self._h, 0, None, None, C.byref(n)))
+            cap = n.value
+        cap = max(int(cap), 1)
+        st = np.empty(cap, np.int64)
+        g = np.empty(cap, np.int32)
+        check(self._L.bspk_spikes_get(self._h, cap, ptr(st), ptr(g), C.byref(n)))
+        m = min(n.value, cap)
         order = np.lexsort((g[:m], st[:m]))
         return st[:m][order], g[:m][order]
 

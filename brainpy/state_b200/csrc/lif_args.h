@@ -115,6 +115,10 @@ template <typename Real>
 cudaError_t launch_drive_fill(const LifArgs<Real> &a, int64_t m0, int n, Real *out,
                               cudaStream_t st);
 size_t lif_tiled_smem(int tile, int L, int W, int N, int npop, int nproj, bool dbl, bool smem_ptr);
+// Recorded spikes of the tiled kernel's per-CTA regions into one list.
+cudaError_t launch_compact_spikes(int G, int64_t region, const long long *rec_count,
+                                  const int64_t *in_step, const int32_t *in_gid, int64_t *out_step,
+                                  int32_t *out_gid, unsigned long long *out_n, cudaStream_t st);
 
 // Launchers (cooperative, persistent).  Return the cudaError_t of the launch.
 template <typename Real>

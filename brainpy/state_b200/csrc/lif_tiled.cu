@@ -516,6 +516,30 @@ cudaError_t launch_drive_fill(const LifArgs<Real> &a, int64_t m0, int n, Real *o
     return cudaGetLastError();
 }
 
+// Recorded spikes of the per-CTA regions into one contiguous list (order
+// free), dropping the holes left for unrecorded neurons (gid < 0).
+__global__ void k_compact_spikes(int64_t region, const long long *rec_count, const int64_t *in_step,
+                                 const int32_t *in_gid, int64_t *out_step, int32_t *out_gid,
+                                 unsigned long long *out_n) {
+    const int c = blockIdx.x;
+    const int64_t k = rec_count[c] < region ? rec_count[c] : region;
+    const int64_t base = static_cast<int64_t>(c) * region;
+    for (int64_t i = threadIdx.x; i < k; i += blockDim.x) {
+        const int32_t gg = in_gid[base + i];
+        if (gg < 0) continue;
+        const unsigned long long pos = atomicAdd(out_n, 1ull);
+        out_step[pos] = in_step[base + i];
+        out_gid[pos] = gg;
+    }
+}
+
+cudaError_t launch_compact_spikes(int G, int64_t region, const long long *rec_count,
+                                  const int64_t *in_step, const int32_t *in_gid, int64_t *out_step,
+                                  int32_t *out_gid, unsigned long long *out_n, cudaStream_t st) {
+    k_compact_spikes<<<G, 256, 0, st>>>(region, rec_count, in_step, in_gid, out_step, out_gid, out_n);
+    return cudaGetLastError();
+}
+
 template cudaError_t launch_lif_tiled<float>(const LifArgs<float> &, const TiledArgs<float> &, int,
                                              cudaStream_t);
 template cudaError_t launch_lif_tiled<double>(const LifArgs<double> &, const TiledArgs<double> &,

@@ -990,6 +990,7 @@ extern "C" int bspk_run(bspk_plan *p, int64_t n_steps, void *stream) {
     BSPK_CUDA(cudaMemsetAsync(p->d_spk_count, 0, sizeof(unsigned long long), st));
     BSPK_CUDA(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
     p->last_run_steps = n_steps;
+    p->cspk_valid = false;
     if (n_steps == 0) return BSPK_OK;
     const bool dbl = p->cfg.precision == 64;
     BSPK_CUDA(cudaMemsetAsync(p->d_barrier, 0, sizeof(unsigned int), st));
@@ -1049,7 +1050,7 @@ int bspk_spikes_get(bspk_plan *p, int64_t cap, int64_t *steps, int32_t *gids, in
         const int64_t region = p->cfg.spike_capacity / G;
         std::vector<long long> counts(G);
         BSPK_CUDA(cudaMemcpy(counts.data(), p->d_trec, sizeof(long long) * G, cudaMemcpyDeviceToHost));
-        int64_t m = 0, total = 0;
+        int64_t total = 0;
         for (int c = 0; c < G; ++c) {
             total += counts[c];
             if (counts[c] > region) {
@@ -1057,23 +1058,27 @@ int bspk_spikes_get(bspk_plan *p, int64_t cap, int64_t *steps, int32_t *gids, in
                 return fail(BSPK_ERR_OVERFLOW, "spike record overflowed its device capacity");
             }
         }
-        std::vector<int64_t> s;
-        std::vector<int32_t> g;
-        for (int c = 0; c < G && m < cap; ++c) {
-            const int64_t k = counts[c];
-            if (k == 0) continue;
-            s.resize(k);
-            g.resize(k);
-            BSPK_CUDA(cudaMemcpy(s.data(), p->d_spk_step + c * region, 8 * k, cudaMemcpyDeviceToHost));
-            BSPK_CUDA(cudaMemcpy(g.data(), p->d_spk_gid + c * region, 4 * k, cudaMemcpyDeviceToHost));
-            for (int64_t i = 0; i < k && m < cap; ++i) {
-                if (g[i] < 0) continue;  // unrecorded neuron
-                steps[m] = s[i];
-                gids[m] = g[i];
-                ++m;
+        if (!p->cspk_valid) {
+            if (!p->d_cspk_step) {
+                int rc2 = dalloc(p, &p->d_cspk_step, static_cast<size_t>(p->cfg.spike_capacity));
+                if (!rc2) rc2 = dalloc(p, &p->d_cspk_gid, static_cast<size_t>(p->cfg.spike_capacity));
+                if (!rc2) rc2 = dalloc(p, &p->d_cspk_n, 1);
+                if (rc2) return rc2;
             }
+            BSPK_CUDA(cudaMemset(p->d_cspk_n, 0, sizeof(unsigned long long)));
+            BSPK_CUDA(launch_compact_spikes(G, region, p->d_trec, p->d_spk_step, p->d_spk_gid,
+                                            p->d_cspk_step, p->d_cspk_gid, p->d_cspk_n, nullptr));
+            unsigned long long n = 0;
+            BSPK_CUDA(cudaMemcpy(&n, p->d_cspk_n, sizeof(n), cudaMemcpyDeviceToHost));
+            p->cspk_n = static_cast<int64_t>(n);
+            p->cspk_valid = true;
         }
-        *n_out = m;
+        const int64_t k = std::min<int64_t>(cap, p->cspk_n);
+        if (k > 0 && steps && gids) {
+            BSPK_CUDA(cudaMemcpy(steps, p->d_cspk_step, 8 * k, cudaMemcpyDeviceToHost));
+            BSPK_CUDA(cudaMemcpy(gids, p->d_cspk_gid, 4 * k, cudaMemcpyDeviceToHost));
+        }
+        *n_out = p->cspk_n;
         return BSPK_OK;
     }
     unsigned long long cnt = 0;

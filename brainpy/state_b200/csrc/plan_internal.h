@@ -128,6 +128,11 @@ struct bspk_plan {
     int tW = 1;                    // tiled window (half the smallest lag when pipelined)
     int tpipe = 0;                 // 1: window j - 1 is delivered after window j's update
     void *d_tdrive = nullptr;      // Poisson drive of one launch, [steps][N]
+    int64_t *d_cspk_step = nullptr;  // compacted spike list of the last run (tiled)
+    int32_t *d_cspk_gid = nullptr;
+    unsigned long long *d_cspk_n = nullptr;
+    bool cspk_valid = false;
+    int64_t cspk_n = 0;
     int64_t tdrive_steps = 0;      // its capacity in steps
 };
 
