@@ -137,7 +137,8 @@ def run_ours(args):
     stream = torch.cuda.current_stream()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
 
-    pl, p = brunel.build_plan(order=2500, precision=32, seed=1234 + rank)
+    from brainpy.state_b200 import dist as D
+    pl, p = brunel.build_plan(order=2500, precision=32, seed=D.replica_seed(1234, rank))
     pl._deg = out_degree(pl, p)
     N = p["NE"] + p["NI"]
     time_runs(pl, args.warmup, stream, flush)
@@ -149,11 +150,7 @@ def run_ours(args):
         times, nspk, nev = time_runs(pl, args.steps, stream, flush)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
-    ms_step = sum(times) / len(times)
-    if world > 1:
-        t = torch.tensor([ms_step], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
+    ms_step = D.max_over_ranks(sum(times) / len(times))  # the slowest replica's time
     sim_ms = STEPS_PER_BENCH_STEP * 0.1
     rtf = world * sim_ms / ms_step
     syn_ev_s = world * (nev / args.steps) / (ms_step / 1000.0)
@@ -201,7 +198,9 @@ def run_ours(args):
         "clocks": clk.summary(),
     }
     del pl
-    if rank == 0 and not args.quick:
+    # the secondary sections run on a single GPU only: with N > 1 the other ranks
+    # would wait on rank 0 for minutes at the final barrier
+    if rank == 0 and not args.quick and world == 1:
         result["fp64"] = fp64_numbers(args, stream, flush)
         result["e2e"] = e2e_numbers(args)
         result["cpu_baseline"] = cpu_baseline(args)
