@@ -39,6 +39,8 @@ namespace bspk {
 
 namespace {
 
+constexpr int kAdjUnroll = 8;   // edge loads in flight per thread
+
 // Edges are kept in a padded column-major ("ELL") layout so that the
 // threads of a warp, one post (or pre) neuron each, touch consecutive words:
 // in-edge k of post i at [k][N] + i (k < deg_in[i]), out-edge k of pre p at
@@ -315,9 +317,19 @@ __global__ void __launch_bounds__(1024) k_adj_backward(const AdjArgs<Real> a) {
             for (int p = threadIdx.x; p < N; p += blockDim.x) {
                 Real l = p < a.R ? a.cz * s.g[p] : Real(0);
                 const int d = a.deg_out[p];
-                for (int k = 0; k < d; ++k) {
-                    const size_t o = static_cast<size_t>(k) * N + p;
-                    l = l + __ldg(a.w_oe + o) * s.lxn[__ldg(a.out_post + o)];
+                for (int k0 = 0; k0 < d; k0 += kAdjUnroll) {
+                    int post[kAdjUnroll];
+                    Real wv[kAdjUnroll];
+#pragma unroll
+                    for (int u = 0; u < kAdjUnroll; ++u) {
+                        const int k = k0 + u;
+                        const size_t o = static_cast<size_t>(k) * N + p;
+                        post[u] = k < d ? __ldg(a.out_post + o) : -1;
+                        wv[u] = k < d ? __ldg(a.w_oe + o) : Real(0);
+                    }
+#pragma unroll
+                    for (int u = 0; u < kAdjUnroll; ++u)
+                        if (post[u] >= 0) l = l + wv[u] * s.lxn[post[u]];
                 }
                 s.ls[p] = l;
             }
@@ -342,10 +354,22 @@ __global__ void __launch_bounds__(1024) k_adj_backward(const AdjArgs<Real> a) {
                 s.lxc[i] = lx;
                 if (t > 0) {
                     const int d = a.deg_in[i];
-                    for (int k = 0; k < d; ++k) {
-                        const size_t o = static_cast<size_t>(k) * N + i;
-                        const Real sv_pre = s.sp[__ldg(a.in_col + o)];
-                        if (sv_pre != Real(0)) dwb[o] = dwb[o] + lx * sv_pre;
+                    for (int k0 = 0; k0 < d; k0 += kAdjUnroll) {
+                        int col[kAdjUnroll];
+#pragma unroll
+                        for (int u = 0; u < kAdjUnroll; ++u) {
+                            const int k = k0 + u;
+                            col[u] = k < d ? __ldg(a.in_col + static_cast<size_t>(k) * N + i) : -1;
+                        }
+#pragma unroll
+                        for (int u = 0; u < kAdjUnroll; ++u) {
+                            if (col[u] < 0) continue;
+                            const Real sv_pre = s.sp[col[u]];
+                            if (sv_pre != Real(0)) {
+                                const size_t o = static_cast<size_t>(k0 + u) * N + i;
+                                dwb[o] = dwb[o] + lx * sv_pre;
+                            }
+                        }
                     }
                 }
                 for (int q = 0; q < nact; ++q) {
