@@ -248,6 +248,64 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
             word[i] = j < G ? __ldcg(recs + j * kRecWords + w) : 0u;
         }
     };
+    // scatter the S gathered spikes in s_list / s_ibeg / s_ioff into the
+    // ring (window slot slot0; all threads, ends with a block barrier)
+    auto scatter = [&](int S, int slot0) {
+        // 2. offsets of the buckets in the flattened edge list (and the
+        //    spike of every edge of the first pass)
+        const int T = block_scan_map(s_ioff, S, s_warp, s_espk, kEdgeCap);
+        // 3. every edge of the window, in passes of kEdgeCap flattened edges:
+        //    s_espk maps a flattened edge to its spike, then lane-interleaved
+        //    threads (edge q0 + u B) take 32 consecutive edges per warp
+        //    instruction -- independent index loads, and consecutive targets
+        //    of one bucket for the shared-memory atomics
+        for (int p0 = 0; p0 < T; p0 += kEdgeCap) {
+            const int p1 = min(T, p0 + kEdgeCap);
+            if (p0 > 0) {
+                for (int i = tid; i < S; i += B) {
+                    const int a0 = max(s_ioff[i], p0), a1 = min(s_ioff[i + 1], p1);
+                    for (int q = a0; q < a1; ++q) s_espk[q - p0] = static_cast<uint16_t>(i);
+                }
+                __syncthreads();
+            }
+            for (int q0 = p0 + tid; q0 < p1; q0 += B * kEdgeUnroll) {
+                int jj[kEdgeUnroll], nm[kEdgeUnroll];
+#pragma unroll
+                for (int u = 0; u < kEdgeUnroll; ++u) {
+                    const int q = q0 + u * B;
+                    jj[u] = -1;
+                    nm[u] = 0;
+                    if (q < p1) {
+                        const int it = s_espk[q - p0];
+                        jj[u] = s_ibeg[it] + (q - s_ioff[it]);
+                        const int m = slot0 + static_cast<int>(s_list[it] & 31u);
+                        nm[u] = m >= L ? m - L : m;
+                    }
+                }
+                uint32_t ed[kEdgeUnroll];
+                Fix wv[kEdgeUnroll];
+#pragma unroll
+                for (int u = 0; u < kEdgeUnroll; ++u) {
+                    ed[u] = 0u;
+                    wv[u] = Fix(0);
+                    if (jj[u] >= 0) {
+                        ed[u] = __ldg(t2.edges + jj[u]);
+                        if (t2.wfix) wv[u] = __ldg(t2.wfix + jj[u]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kEdgeUnroll; ++u) {
+                    if (jj[u] >= 0) {
+                        if (!t2.wfix) wv[u] = s_wproj[ed[u] >> 24];
+                        int slot = nm[u] + static_cast<int>((ed[u] >> 16) & 0xFFu);
+                        if (slot >= L) slot -= L;
+                        fix_add(ring_s + slot * tile + (ed[u] & 0xFFFFu), wv[u]);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    };
     // deliver the spikes of window e into the ring (all threads)
     auto deliver = [&](int e, uint32_t (&word)[kRecPerHalf], bool have) {
         const int buf = e & (kRecBufs - 1);
@@ -256,16 +314,17 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
         const int slot0 = static_cast<int>(e0 % L);
         const uint32_t *recs = t2.list + static_cast<size_t>(buf) * G * kRecWords;
         // a gathered spike: its entry and the bounds of its edge bucket
+        auto put = [&](int pos, int src, uint32_t word_) {
+            const int pre = src * tile + static_cast<int>((word_ & kPayMask) >> 5);
+            s_list[pos] = (static_cast<uint32_t>(pre) << 5) | (word_ & 31u);
+            const int b0 = t2.smem_ptr ? s_ptr[pre] : __ldg(gptr + pre);
+            const int b1 = t2.smem_ptr ? s_ptr[pre + 1] : __ldg(gptr + pre + 1);
+            s_ibeg[pos] = b0;
+            s_ioff[pos] = b1 - b0;
+        };
         auto push = [&](int src, uint32_t word_) {
             const int pos = atomicAdd(&s_nlist, 1);
-            if (pos < kListCap) {
-                const int pre = src * tile + static_cast<int>((word_ & kPayMask) >> 5);
-                s_list[pos] = (static_cast<uint32_t>(pre) << 5) | (word_ & 31u);
-                const int b0 = t2.smem_ptr ? s_ptr[pre] : __ldg(gptr + pre);
-                const int b1 = t2.smem_ptr ? s_ptr[pre + 1] : __ldg(gptr + pre + 1);
-                s_ibeg[pos] = b0;
-                s_ioff[pos] = b1 - b0;
-            }
+            if (pos < kListCap) put(pos, src, word_);
         };
         if (tid == 0) s_nlist = 0;
         __syncthreads();
@@ -336,68 +395,49 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
         }
         __syncthreads();
         if (s_abort) return;
-        const int S = min(s_nlist, kListCap);
-        if (s_nlist > kListCap) {
-            if (tid == 0) {
-                atomicExch(a.err, BSPK_DEV_ERR_OVERFLOW);
-                s_abort = 1;
-            }
-            __syncthreads();
+        const int total = s_nlist;
+        if (total <= kListCap) {
+            scatter(total, slot0);
             return;
         }
-        // 2. offsets of the buckets in the flattened edge list (and the
-        //    spike of every edge of the first pass)
-        const int T = block_scan_map(s_ioff, S, s_warp, s_espk, kEdgeCap);
-        // 3. every edge of the window, in passes of kEdgeCap flattened edges:
-        //    s_espk maps a flattened edge to its spike, then lane-interleaved
-        //    threads (edge q0 + u B) take 32 consecutive edges per warp
-        //    instruction -- independent index loads, and consecutive targets
-        //    of one bucket for the shared-memory atomics
-        for (int p0 = 0; p0 < T; p0 += kEdgeCap) {
-            const int p1 = min(T, p0 + kEdgeCap);
-            if (p0 > 0) {
-                for (int i = tid; i < S; i += B) {
-                    const int a0 = max(s_ioff[i], p0), a1 = min(s_ioff[i + 1], p1);
-                    for (int q = a0; q < a1; ++q) s_espk[q - p0] = static_cast<uint16_t>(i);
-                }
-                __syncthreads();
-            }
-            for (int q0 = p0 + tid; q0 < p1; q0 += B * kEdgeUnroll) {
-                int jj[kEdgeUnroll], nm[kEdgeUnroll];
+        // more spikes than the list holds: deliver them in chunks of kListCap.
+        // Spike x of the window is entry q of record j with x = off_j + q
+        // (off_j = counts of the records before j), so every chunk takes a
+        // fixed set of spikes; the fixed-point sums do not depend on how the
+        // spikes are split.  The records were validated above and stay
+        // unchanged until every CTA has delivered this window.
+        for (int cb = 0; cb < total; cb += kListCap) {
+            const int ce = min(total, cb + kListCap);
+#pragma unroll 1
+            for (int i = 0; i < kRecPerHalf; ++i) {
+                const int j = hw + kHalfWarps * i;
+                int part = 0;
+                if (j < G)
+                    for (int k = w; k < j; k += 16)
+                        part += static_cast<int>(__ldcg(recs + k * kRecWords) & kPayMask);
 #pragma unroll
-                for (int u = 0; u < kEdgeUnroll; ++u) {
-                    const int q = q0 + u * B;
-                    jj[u] = -1;
-                    nm[u] = 0;
-                    if (q < p1) {
-                        const int it = s_espk[q - p0];
-                        jj[u] = s_ibeg[it] + (q - s_ioff[it]);
-                        const int m = slot0 + static_cast<int>(s_list[it] & 31u);
-                        nm[u] = m >= L ? m - L : m;
-                    }
-                }
-                uint32_t ed[kEdgeUnroll];
-                Fix wv[kEdgeUnroll];
-#pragma unroll
-                for (int u = 0; u < kEdgeUnroll; ++u) {
-                    ed[u] = 0u;
-                    wv[u] = Fix(0);
-                    if (jj[u] >= 0) {
-                        ed[u] = __ldg(t2.edges + jj[u]);
-                        if (t2.wfix) wv[u] = __ldg(t2.wfix + jj[u]);
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < kEdgeUnroll; ++u) {
-                    if (jj[u] >= 0) {
-                        if (!t2.wfix) wv[u] = s_wproj[ed[u] >> 24];
-                        int slot = nm[u] + static_cast<int>((ed[u] >> 16) & 0xFFu);
-                        if (slot >= L) slot -= L;
-                        fix_add(ring_s + slot * tile + (ed[u] & 0xFFFFu), wv[u]);
+                for (int o = 8; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o, 16);
+                if (j >= G) continue;
+                const uint32_t head = __ldcg(recs + j * kRecWords);
+                const int cnt = static_cast<int>(head & kPayMask);
+                const uint32_t *ovs = t2.ovf + (static_cast<size_t>(buf) * G + j) * t2.list_cap;
+                const int q1 = min(cnt, ce - part);
+                for (int q = max(0, cb - part) + w; q < q1; q += 16) {
+                    const uint32_t wq = q < kRecInline ? __ldcg(recs + j * kRecWords + 1 + q)
+                                                       : __ldcg(ovs + (q - kRecInline));
+                    const int pos = part + q - cb;
+                    if ((wq & kTagMask) == tag) {
+                        put(pos, j, wq);
+                    } else {  // never expected: an empty bucket and an error
+                        atomicCAS(a.err, 0, BSPK_DEV_ERR_BOUNDS);
+                        s_list[pos] = 0u;
+                        s_ibeg[pos] = 0;
+                        s_ioff[pos] = 0;
                     }
                 }
             }
             __syncthreads();
+            scatter(ce - cb, slot0);
         }
     };
 

@@ -1033,6 +1033,7 @@ int bspk::sync_and_check(bspk_plan *p) {
     if (err == BSPK_DEV_ERR_UNSTABLE) return fail(BSPK_ERR_UNSTABLE, "Numerical instability in aeif_cond_alpha dynamics.");
     if (err == BSPK_DEV_ERR_RKCAP) return fail(BSPK_ERR_RKCAP, "RKF45 iteration cap reached");
     if (err == BSPK_DEV_ERR_BOUNDS) return fail(BSPK_ERR_ARG, "device bounds check failed");
+    if (err == BSPK_DEV_ERR_OVERFLOW) return fail(BSPK_ERR_OVERFLOW, "device list overflow");
     if (err) return fail(BSPK_ERR_CUDA, "device error flag " + std::to_string(err));
     return BSPK_OK;
 }

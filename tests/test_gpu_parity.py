@@ -176,3 +176,19 @@ def test_tiled_fp32_is_deterministic():
     np.testing.assert_array_equal(out[0][0], out[1][0])
     np.testing.assert_array_equal(out[0][1], out[1][1])
     np.testing.assert_array_equal(out[0][2], out[1][2])
+
+
+def test_tiled_large_tiles_drive_pass(oracle):
+    """30 000 neurons: tiles of 203 neurons leave too few idle threads, so
+    the drive comes from the separate drive pass (and the CSR bounds from
+    global memory); spikes must match the oracle."""
+    net = Net(NE=24000, NI=6000, CE=20, CI=5, J=60.0, delay=15, seed=9)
+    rec = np.arange(0, 30000, 997)
+    pl = net.to_plan(precision=64, semantics=1, rec=rec)
+    sim = net.to_oracle(oracle, semantics=1, rec=rec)
+    pl.run(60)
+    st, g = pl.spikes()
+    ost, og, ov = sim.run(60)
+    assert len(st) > 0
+    assert _raster(st, g) == _raster(ost, og)
+    np.testing.assert_allclose(pl.v_trace(), ov, rtol=0, atol=1e-9)
