@@ -18,7 +18,8 @@ ERRORS = {
     -1: ValueError, -2: RuntimeError, -3: RuntimeError, -4: NotImplementedError,
     -5: TimeoutError, -6: FloatingPointError, -7: OverflowError, -8: RuntimeError,
 }
-MODELS = {"iaf_psc_alpha": 0, "iaf_psc_exp": 1, "aeif_cond_alpha": 2}
+MODELS = {"iaf_psc_alpha": 0, "iaf_psc_exp": 1, "aeif_cond_alpha": 2, "iaf_cond_exp": 3,
+          "iaf_cond_alpha": 4}
 LEGACY, RING = 0, 1
 
 

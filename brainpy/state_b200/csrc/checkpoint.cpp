@@ -25,10 +25,10 @@ struct Section {
 
 std::vector<Section> sections(bspk_plan *p) {
     std::vector<Section> s;
-    const int ns = p->cfg.model == BSPK_AEIF_COND_ALPHA ? 8 : 6;
+    const int ns = model_n_slots(p->cfg.model);
     for (int i = 0; i < ns; ++i) s.push_back({p->d_s[i], static_cast<size_t>(p->elt) * p->N});
     s.push_back({p->d_r, sizeof(int) * static_cast<size_t>(p->N)});
-    const int R = p->cfg.model == BSPK_AEIF_COND_ALPHA ? 2 : 1;
+    const int R = model_is_cond(p->cfg.model) ? 2 : 1;
     s.push_back({p->d_ring, static_cast<size_t>(p->elt) * p->L * R * p->N});
     s.push_back({p->d_hist, sizeof(uint64_t) * static_cast<size_t>(p->N)});
     for (auto &J : p->projs) {

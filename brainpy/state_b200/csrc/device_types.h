@@ -18,6 +18,18 @@ enum {
     BSPK_DEV_ERR_RKCAP = 5,
 };
 
+// Conductance models (ids 2..4 of bspk.h: aeif_cond_alpha, iaf_cond_exp,
+// iaf_cond_alpha) run on the RKF45 per-step engine with two receptor ports.
+// Their state slots are the ODE leaves, then the integration step h and the
+// buffered current I_stim.
+__host__ __device__ constexpr bool model_is_cond(int model) { return model >= 2 && model <= 4; }
+__host__ __device__ constexpr int cond_n_ode(int model) {
+    return model == 2 ? 6 : (model == 3 ? 3 : 5);
+}
+__host__ __device__ constexpr int model_n_slots(int model) {
+    return model_is_cond(model) ? cond_n_ode(model) + 2 : 6;
+}
+
 constexpr int kMaxPops = 64;
 constexpr int kMaxInputs = 64;   // drives + projections per plan
 constexpr int kMaxWindow = 32;   // d_min batching window (steps)

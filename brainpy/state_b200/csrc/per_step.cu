@@ -1,5 +1,6 @@
-// per_step.cu -- per-step engine: aeif_cond_alpha with adaptive RKF45, and
-// networks with plastic stdp_synapse projections (any neuron model).
+// per_step.cu -- per-step engine: the conductance models (aeif_cond_alpha,
+// iaf_cond_exp, iaf_cond_alpha) with adaptive RKF45, and networks with
+// plastic stdp_synapse projections (any neuron model).
 //
 // One step n is this kernel sequence (the reference Simulator's phase order,
 // _nest_network/simulator.py:1719-1788):
@@ -78,37 +79,71 @@ __device__ __forceinline__ void aeif_vf(const PopCoef<Real> &c, int r, Real i_st
     dy[5] = (c.a * (v_eff - c.E_L) - y[5]) / c.tau_w;
 }
 
-// One dt of the adaptive RKF45 loop (_nest_base/utils.py:583-718) with the
-// in-loop spike/reset event (aeif_cond_alpha.py:594-625) and the synaptic
-// jumps after integration (aeif_cond_alpha.py:709-728).  s: V, dg_ex, g_ex,
-// dg_in, g_in, w, h, I_stim.  Returns the spike flag.
-template <typename Real>
-__device__ bool aeif_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Real w_in,
+// Vector fields of the iaf conductance models: iaf_cond_exp
+// (_nest_neuron/iaf_cond_exp.py:456-490; y = V, g_ex, g_in) and
+// iaf_cond_alpha (_nest_neuron/iaf_cond_alpha.py:459-491; y = V, dg_ex, g_ex,
+// dg_in, g_in).  The membrane sees min(V, V_th), or V_reset while refractory.
+template <typename Real, int MODEL>
+__device__ __forceinline__ void iaf_cond_vf(const PopCoef<Real> &c, int r, Real i_stim,
+                                            const Real *y, Real *dy) {
+    const bool refr = r > 0;
+    const Real v = y[0];
+    const Real v_eff = refr ? c.V_reset : (v < c.V_th ? v : (v != v ? v : c.V_th));
+    const Real gex = MODEL == 3 ? y[1] : y[2];
+    const Real gin = MODEL == 3 ? y[2] : y[4];
+    const Real i_syn_exc = gex * (v_eff - c.E_ex);
+    const Real i_syn_inh = gin * (v_eff - c.E_in);
+    const Real i_leak = c.g_L * (v_eff - c.E_L);
+    const Real dV = (-i_leak - i_syn_exc - i_syn_inh + c.I_e + i_stim) / c.C_m;
+    dy[0] = refr ? Real(0) : dV;
+    if constexpr (MODEL == 3) {
+        dy[1] = -y[1] / c.tau_syn_ex;
+        dy[2] = -y[2] / c.tau_syn_in;
+    } else {
+        dy[1] = -y[1] / c.tau_syn_ex;
+        dy[2] = y[1] - y[2] / c.tau_syn_ex;
+        dy[3] = -y[3] / c.tau_syn_in;
+        dy[4] = y[3] - y[4] / c.tau_syn_in;
+    }
+}
+
+// One dt of the adaptive RKF45 loop (_nest_base/utils.py:583-718) for a
+// conductance model (MODEL 2: aeif_cond_alpha, 3: iaf_cond_exp,
+// 4: iaf_cond_alpha), with the model's in-loop spike/reset event
+// (aeif_cond_alpha.py:594-625, iaf_cond_exp.py:487-517,
+// iaf_cond_alpha.py:493-521) and the synaptic jumps after integration
+// (aeif_cond_alpha.py:709-728, iaf_cond_exp.py:594-614,
+// iaf_cond_alpha.py:602-624).  s: the NS ODE leaves, then h and I_stim.
+// Returns the spike flag.
+template <typename Real, int MODEL>
+__device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Real w_in,
                           double dt, int *err, unsigned long long *rk_iters) {
+    constexpr int NS = cond_n_ode(MODEL);
+    constexpr int kMaxIters = MODEL == 3 ? 10000 : 100000;  // the models' _MAX_ITERS
     constexpr double min_h = 1e-8;
-    Real y[6];
+    Real y[NS];
 #pragma unroll
-    for (int i = 0; i < 6; ++i) y[i] = s[i];
-    double h = static_cast<double>(s[6]);
-    const Real i_stim = s[7];
+    for (int i = 0; i < NS; ++i) y[i] = s[i];
+    double h = static_cast<double>(s[NS]);
+    const Real i_stim = s[NS + 1];
     const double atol = static_cast<double>(c.atol);
     bool spiked = false, unstable = false;
     double t_loc = 0.0;
     if (h < min_h) h = min_h;
     int iters = 0;
-    Real k[6][6];
-    while (t_loc < dt && iters < 100000) {
+    Real k[6][NS];
+    while (t_loc < dt && iters < kMaxIters) {
         const double hh = h < dt - t_loc ? h : dt - t_loc;
         h = hh > min_h ? hh : min_h;
         const Real hR = static_cast<Real>(h);
         for (int st = 0; st < 6; ++st) {
-            Real yi[6];
+            Real yi[NS];
             if (st == 0) {
 #pragma unroll
-                for (int i = 0; i < 6; ++i) yi[i] = y[i];
+                for (int i = 0; i < NS; ++i) yi[i] = y[i];
             } else {
 #pragma unroll
-                for (int i = 0; i < 6; ++i) {
+                for (int i = 0; i < NS; ++i) {
                     Real acc = Real(0);
                     bool first = true;
                     for (int j = 0; j < st; ++j) {
@@ -121,12 +156,13 @@ __device__ bool aeif_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
                     yi[i] = y[i] + hR * acc;
                 }
             }
-            aeif_vf<Real>(c, r, i_stim, yi, k[st]);
+            if constexpr (MODEL == 2) aeif_vf<Real>(c, r, i_stim, yi, k[st]);
+            else iaf_cond_vf<Real, MODEL>(c, r, i_stim, yi, k[st]);
         }
-        Real yh[6];
+        Real yh[NS];
         double err = 0.0;
 #pragma unroll
-        for (int i = 0; i < 6; ++i) {
+        for (int i = 0; i < NS; ++i) {
             Real acc = Real(0), eacc = Real(0);
             bool first = true, efirst = true;
 #pragma unroll
@@ -155,14 +191,18 @@ __device__ bool aeif_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
         const bool accept = (err <= 1.0) || (h <= min_h);
         if (accept) {
 #pragma unroll
-            for (int i = 0; i < 6; ++i) y[i] = yh[i];
+            for (int i = 0; i < NS; ++i) y[i] = yh[i];
             t_loc = t_loc + h;
-            if (y[0] < Real(-1e3) || y[5] < Real(-1e6) || y[5] > Real(1e6)) unstable = true;
+            if constexpr (MODEL == 2) {
+                if (y[0] < Real(-1e3) || y[5] < Real(-1e6) || y[5] > Real(1e6)) unstable = true;
+            } else if constexpr (MODEL == 3) {
+                if (y[0] < Real(-1e3)) unstable = true;
+            }
             if (r > 0) y[0] = c.V_reset;
             if (r <= 0 && y[0] >= c.v_peak_detect) {
                 spiked = true;
                 y[0] = c.V_reset;
-                y[5] = y[5] + c.b;
+                if constexpr (MODEL == 2) y[5] = y[5] + c.b;
                 if (c.ref_count > 0) r = c.ref_count + 1;
             }
         }
@@ -180,16 +220,21 @@ __device__ bool aeif_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
         h = hn > min_h ? hn : min_h;
         ++iters;
     }
-    if (iters >= 100000 && t_loc < dt) atomicExch(err, BSPK_DEV_ERR_RKCAP);
+    if (iters >= kMaxIters && t_loc < dt) atomicExch(err, BSPK_DEV_ERR_RKCAP);
     if (unstable) atomicExch(err, BSPK_DEV_ERR_UNSTABLE);
     atomicAdd(rk_iters, static_cast<unsigned long long>(iters));
     if (r > 0) r = r - 1;
-    y[1] = y[1] + c.pscon_ex * w_ex;
-    y[3] = y[3] + c.pscon_in * w_in;
+    if constexpr (MODEL == 3) {
+        y[1] = y[1] + w_ex;
+        y[2] = y[2] + w_in;
+    } else {
+        y[1] = y[1] + c.pscon_ex * w_ex;
+        y[3] = y[3] + c.pscon_in * w_in;
+    }
 #pragma unroll
-    for (int i = 0; i < 6; ++i) s[i] = y[i];
-    s[6] = static_cast<Real>(h);
-    s[7] = Real(0);  // no current input on this path: I_stim <- 0
+    for (int i = 0; i < NS; ++i) s[i] = y[i];
+    s[NS] = static_cast<Real>(h);
+    s[NS + 1] = Real(0);  // no current input on this path: I_stim <- 0
     return spiked;
 }
 
@@ -219,19 +264,20 @@ __global__ void __launch_bounds__(128) k_neuron_step(const StepArgs<Real> a, dou
             in[d.receptor < a.R ? d.receptor : 0] += static_cast<Real>(cnt) * static_cast<Real>(d.weight);
         }
     }
+    constexpr int kSlots = model_n_slots(MODEL);
     Real st[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) st[i] = (MODEL == 2 || i < 6) ? a.s[i][g] : Real(0);
+    for (int i = 0; i < 8; ++i) st[i] = i < kSlots ? a.s[i][g] : Real(0);
     int r = a.r[g];
     bool sp;
-    if (MODEL == 0) {
+    if constexpr (MODEL == 0) {
         Real s6[6];
 #pragma unroll
         for (int i = 0; i < 6; ++i) s6[i] = st[i];
         sp = iaf_alpha_step<Real>(c, s6, r, in[0]);
 #pragma unroll
         for (int i = 0; i < 6; ++i) st[i] = s6[i];
-    } else if (MODEL == 1) {
+    } else if constexpr (MODEL == 1) {
         Real s6[6];
 #pragma unroll
         for (int i = 0; i < 6; ++i) s6[i] = st[i];
@@ -239,11 +285,11 @@ __global__ void __launch_bounds__(128) k_neuron_step(const StepArgs<Real> a, dou
 #pragma unroll
         for (int i = 0; i < 6; ++i) st[i] = s6[i];
     } else {
-        sp = aeif_step<Real>(c, st, r, in[0], in[1], dt, a.err, a.rk_iters);
+        sp = cond_step<Real, MODEL>(c, st, r, in[0], in[1], dt, a.err, a.rk_iters);
     }
 #pragma unroll
     for (int i = 0; i < 8; ++i)
-        if (MODEL == 2 || i < 6) a.s[i][g] = st[i];
+        if (i < kSlots) a.s[i][g] = st[i];
     a.r[g] = r;
     const int bit = static_cast<int>(n & 63);
     a.hist[g] = (a.hist[g] & ~(1ull << bit)) | (static_cast<uint64_t>(sp) << bit);
@@ -377,7 +423,7 @@ StepArgs<Real> step_args(bspk_plan *p, int64_t *step_ptr) {
     a.nproj = static_cast<int>(p->projs.size());
     a.ndrive = static_cast<int>(p->drives.size());
     a.model = p->cfg.model;
-    a.R = p->cfg.model == BSPK_AEIF_COND_ALPHA ? 2 : 1;
+    a.R = model_is_cond(p->cfg.model) ? 2 : 1;
     a.L = p->L;
     a.coef = static_cast<const PopCoef<Real> *>(p->d_coef);
     for (int i = 0; i < 8; ++i) a.s[i] = static_cast<Real *>(p->d_s[i]);
@@ -460,7 +506,9 @@ cudaError_t enqueue_step(bspk_plan *p, const StepArgs<Real> &a, const std::vecto
     const double dt = p->cfg.dt;
     if (a.model == 0) k_neuron_step<Real, 0><<<nb, 128, 0, st>>>(a, dt);
     else if (a.model == 1) k_neuron_step<Real, 1><<<nb, 128, 0, st>>>(a, dt);
-    else k_neuron_step<Real, 2><<<nb, 128, 0, st>>>(a, dt);
+    else if (a.model == 2) k_neuron_step<Real, 2><<<nb, 128, 0, st>>>(a, dt);
+    else if (a.model == 3) k_neuron_step<Real, 3><<<nb, 128, 0, st>>>(a, dt);
+    else k_neuron_step<Real, 4><<<nb, 128, 0, st>>>(a, dt);
     k_deliver_static<Real><<<p->sm_count * 4, 256, 0, st>>>(a);
     k_step_end<<<1, 32, 0, st>>>(a.step_ptr);
     return cudaGetLastError();

@@ -72,10 +72,12 @@ int upload_vec(bspk_plan *p, T **ptr, const std::vector<T> &v) {
     return BSPK_OK;
 }
 
-const char *kStateNames[3][9] = {
+const char *kStateNames[5][9] = {
     {"V_m", "I_syn_ex", "dI_syn_ex", "I_syn_in", "dI_syn_in", "y0", "", "", ""},
     {"V_m", "i_syn_ex", "i_syn_in", "i_0", "i_1", "", "", "", ""},
     {"V_m", "dg_ex", "g_ex", "dg_in", "g_in", "w", "h", "I_stim", ""},
+    {"V_m", "g_ex", "g_in", "h", "I_stim", "", "", "", ""},
+    {"V_m", "dg_ex", "g_ex", "dg_in", "g_in", "h", "I_stim", "", ""},
 };
 
 int state_slot(int model, const char *name) {
@@ -85,7 +87,7 @@ int state_slot(int model, const char *name) {
     return -1;
 }
 
-int n_state_slots(int model) { return model == BSPK_AEIF_COND_ALPHA ? 8 : 6; }
+int n_state_slots(int model) { return model_n_slots(model); }
 
 // Float64 propagators and thresholds, following the reference formulas
 // (_nest_neuron/iaf_psc_alpha.py:451-556, iaf_psc_exp.py:492-512,
@@ -203,6 +205,38 @@ int make_coef(int model, const std::vector<double> &p, double h, PopCoef<double>
         c->v_peak_detect = c->Delta_T > 0.0 ? c->V_peak : c->V_th;
         return BSPK_OK;
     }
+    if (model == BSPK_IAF_COND_EXP || model == BSPK_IAF_COND_ALPHA) {
+        if (p.size() < 12) return fail(BSPK_ERR_ARG, "too few parameters");
+        c->E_L = p[0];
+        c->C_m = p[1];
+        const double t_ref = p[2];
+        c->V_th = p[3];
+        c->V_reset = p[4];
+        c->E_ex = p[5];
+        c->E_in = p[6];
+        c->g_L = p[7];
+        c->tau_syn_ex = p[8];
+        c->tau_syn_in = p[9];
+        c->I_e = p[10];
+        c->atol = p[11];
+        // validation (iaf_cond_exp.py:360-379, iaf_cond_alpha.py:368-385)
+        if (!(c->V_reset < c->V_th)) return fail(BSPK_ERR_ARG, "Reset potential must be smaller than threshold.");
+        if (!(c->C_m > 0)) return fail(BSPK_ERR_ARG, "Capacitance must be strictly positive.");
+        if (t_ref < 0) return fail(BSPK_ERR_ARG, "Refractory time cannot be negative.");
+        if (!(c->tau_syn_ex > 0) || !(c->tau_syn_in > 0))
+            return fail(BSPK_ERR_ARG, model == BSPK_IAF_COND_EXP
+                                          ? "All synaptic time constants must be strictly positive."
+                                          : "All time constants must be strictly positive.");
+        if (model == BSPK_IAF_COND_EXP && !(c->atol > 0))
+            return fail(BSPK_ERR_ARG, "The gsl_error_tol must be strictly positive.");
+        c->ref_count = static_cast<int>(std::ceil(t_ref / h));
+        // jumps after integration: g += w (exp), dg += e / tau * w (alpha)
+        c->pscon_ex = model == BSPK_IAF_COND_ALPHA ? kE / c->tau_syn_ex : 1.0;
+        c->pscon_in = model == BSPK_IAF_COND_ALPHA ? kE / c->tau_syn_in : 1.0;
+        c->V_peak = c->V_th;
+        c->v_peak_detect = c->V_th;
+        return BSPK_OK;
+    }
     return fail(BSPK_ERR_ARG, "unknown model");
 }
 
@@ -255,11 +289,11 @@ int bspk_plan_create(const bspk_config *cfg, bspk_plan **out) {
     if (!(cfg->dt > 0)) return fail(BSPK_ERR_ARG, "dt must be > 0");
     if (cfg->precision != 32 && cfg->precision != 64)
         return fail(BSPK_ERR_ARG, "precision must be 32 or 64");
-    if (cfg->model < 0 || cfg->model > 2) return fail(BSPK_ERR_ARG, "unknown model");
+    if (cfg->model < 0 || cfg->model > 4) return fail(BSPK_ERR_ARG, "unknown model");
     if (cfg->semantics != BSPK_LEGACY && cfg->semantics != BSPK_RING)
         return fail(BSPK_ERR_ARG, "unknown delivery semantics");
     if (cfg->deterministic && (cfg->precision != 64 || cfg->semantics != BSPK_LEGACY ||
-                               cfg->model == BSPK_AEIF_COND_ALPHA))
+                               model_is_cond(cfg->model)))
         return fail(BSPK_ERR_UNSUPPORTED,
                     "deterministic mode needs precision 64, LEGACY semantics and an iaf model");
     bspk_plan *p = new bspk_plan();
@@ -312,7 +346,7 @@ int bspk_proj_add_csr(bspk_plan *p, int pre_pop, int post_pop, int64_t n_edges,
     if (n_edges < 0 || (n_edges > 0 && (!post_local || !w || !delay_steps)) || !indptr)
         return fail(BSPK_ERR_ARG, "bad edge arrays");
     if (receptor < 0 || receptor > 1) return fail(BSPK_ERR_ARG, "receptor must be 0 or 1");
-    if (receptor != 0 && p->cfg.model != BSPK_AEIF_COND_ALPHA)
+    if (receptor != 0 && !model_is_cond(p->cfg.model))
         return fail(BSPK_ERR_ARG, "receptor ports are for conductance models; current models sum all inputs");
     if (static_cast<int>(p->input_kind.size()) >= kMaxInputs) return fail(BSPK_ERR_ARG, "too many inputs");
     const int npre = p->pops[pre_pop].n, npost = p->pops[post_pop].n;
@@ -383,7 +417,7 @@ int bspk_drive_add_poisson(bspk_plan *p, int post_pop, double rate_hz, double we
         return fail(BSPK_ERR_ARG, "population index out of range");
     if (static_cast<int>(p->input_kind.size()) >= kMaxInputs) return fail(BSPK_ERR_ARG, "too many inputs");
     if (receptor < 0 || receptor > 1) return fail(BSPK_ERR_ARG, "receptor must be 0 or 1");
-    if (receptor != 0 && p->cfg.model != BSPK_AEIF_COND_ALPHA)
+    if (receptor != 0 && !model_is_cond(p->cfg.model))
         return fail(BSPK_ERR_ARG, "receptor ports are for conductance models; current models sum all inputs");
     const double lam = rate_hz * p->cfg.dt / 1000.0;
     if (!(lam >= 0) || lam > 700.0) return fail(BSPK_ERR_ARG, "rate*dt/1000 must be in [0, 700]");
@@ -692,7 +726,7 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
     p->sm_count = prop.multiProcessorCount;
     const bool dbl = p->cfg.precision == 64;
     const bool exact = p->cfg.deterministic != 0;
-    const bool aeif = p->cfg.model == BSPK_AEIF_COND_ALPHA;
+    const bool aeif = model_is_cond(p->cfg.model);  // RKF45 per-step engine
     bool plastic = false;
     for (auto &J : p->projs) plastic |= J.plastic;
 
@@ -729,8 +763,12 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
         for (auto &P : p->pops)
             for (int k = 0; k < P.n; ++k) {
                 double v = 0.0;
-                if (i == 0) v = aeif ? P.c.E_L : P.c.E_L;
-                if (aeif && i == 6) v = p->cfg.dt;  // integration_step = dt
+                // V_m: E_L for the iaf and AdEx models; the iaf_cond models'
+                // V_initializer is a constant -70 mV (iaf_cond_exp.py:310)
+                if (i == 0) v = (p->cfg.model == BSPK_IAF_COND_EXP || p->cfg.model == BSPK_IAF_COND_ALPHA)
+                                    ? -70.0
+                                    : P.c.E_L;
+                if (aeif && i == cond_n_ode(p->cfg.model)) v = p->cfg.dt;  // integration_step = dt
                 init[P.off + k] = v;
             }
         if (dbl) {
@@ -996,7 +1034,7 @@ extern "C" int bspk_run(bspk_plan *p, int64_t n_steps, void *stream) {
     BSPK_CUDA(cudaMemsetAsync(p->d_barrier, 0, sizeof(unsigned int), st));
     BSPK_CUDA(cudaEventRecord(p->ev0, st));
     cudaError_t e = cudaSuccess;
-    bool per_step = p->cfg.model == BSPK_AEIF_COND_ALPHA;
+    bool per_step = model_is_cond(p->cfg.model);
     for (auto &J : p->projs) per_step |= J.plastic;
     if (p->tiled) BSPK_CUDA(cudaMemsetAsync(p->d_trec, 0, sizeof(long long) * p->grid, st));
     if (per_step) {
@@ -1030,7 +1068,10 @@ int bspk::sync_and_check(bspk_plan *p) {
     int err = 0;
     BSPK_CUDA(cudaMemcpy(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (err == BSPK_DEV_ERR_TIMEOUT) return fail(BSPK_ERR_TIMEOUT, "device barrier timed out");
-    if (err == BSPK_DEV_ERR_UNSTABLE) return fail(BSPK_ERR_UNSTABLE, "Numerical instability in aeif_cond_alpha dynamics.");
+    if (err == BSPK_DEV_ERR_UNSTABLE)
+        return fail(BSPK_ERR_UNSTABLE, p->cfg.model == BSPK_IAF_COND_EXP
+                                           ? "Numerical instability in iaf_cond_exp dynamics."
+                                           : "Numerical instability in aeif_cond_alpha dynamics.");
     if (err == BSPK_DEV_ERR_RKCAP) return fail(BSPK_ERR_RKCAP, "RKF45 iteration cap reached");
     if (err == BSPK_DEV_ERR_BOUNDS) return fail(BSPK_ERR_ARG, "device bounds check failed");
     if (err == BSPK_DEV_ERR_OVERFLOW) return fail(BSPK_ERR_OVERFLOW, "device list overflow");

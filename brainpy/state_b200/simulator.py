@@ -38,6 +38,8 @@ class _Model:
     order: tuple = ()
     units: dict = {}
     defaults: dict = {}
+    conductance = False   # weights in nS into receptor ports, RKF45 per-step engine
+    v_init_const = None   # default V_m when the model's V_initializer is a constant
 
     @classmethod
     def resolve(cls, params):
@@ -97,6 +99,27 @@ class aeif_cond_alpha(_Model):
                     E_in=-85.0, E_L=-70.6, Delta_T=2.0, tau_w=144.0, a=4.0, b=80.5, V_th=-50.4,
                     tau_syn_ex=0.2, tau_syn_in=2.0, I_e=0.0, gsl_error_tol=1e-6)
     v_default = "E_L"
+    conductance = True
+
+
+class iaf_cond_exp(_Model):
+    """NEST iaf_cond_exp with RKF45 (_nest_neuron/iaf_cond_exp.py:295-318 defaults)."""
+    model_name = "iaf_cond_exp"
+    order = ("E_L", "C_m", "t_ref", "V_th", "V_reset", "E_ex", "E_in", "g_L", "tau_syn_ex",
+             "tau_syn_in", "I_e", "gsl_error_tol")
+    units = dict(E_L=mV, C_m=pF, t_ref=ms, V_th=mV, V_reset=mV, E_ex=mV, E_in=mV, g_L=nS,
+                 tau_syn_ex=ms, tau_syn_in=ms, I_e=pA, gsl_error_tol=None)
+    defaults = dict(E_L=-70.0, C_m=250.0, t_ref=2.0, V_th=-55.0, V_reset=-60.0, E_ex=0.0,
+                    E_in=-85.0, g_L=16.6667, tau_syn_ex=0.2, tau_syn_in=2.0, I_e=0.0,
+                    gsl_error_tol=1e-3)
+    v_default = "E_L"
+    v_init_const = -70.0
+    conductance = True
+
+
+class iaf_cond_alpha(iaf_cond_exp):
+    """NEST iaf_cond_alpha with RKF45 (_nest_neuron/iaf_cond_alpha.py:307-329 defaults)."""
+    model_name = "iaf_cond_alpha"
 
 
 class poisson_generator:
@@ -427,7 +450,7 @@ class Simulator:
         if not isinstance(dst, _Population):
             raise TypeError("post must be a neuron population")
         full_post = qs.indices.size == dst.n and np.all(qs.indices == np.arange(dst.n))
-        w_unit = nS if self._model is aeif_cond_alpha else pA
+        w_unit = nS if self._model.conductance else pA
         if synapse is not None:
             weight = synapse.weight if weight is None else weight
             delay = synapse.delay if delay is None else delay
@@ -560,7 +583,9 @@ class Simulator:
         pl = self._plan
         for p in self._pops:
             init = p.v_init
-            if init is None:
+            if init is None and p.spec.v_init_const is not None:
+                v = np.full(p.n, p.spec.v_init_const)
+            elif init is None:
                 v = np.full(p.n, p.params[p.spec.order.index(p.spec.v_default)])
             elif isinstance(init, (Uniform, Normal)):
                 v = init.sample(p.n, np.random.default_rng(1_000_003 + p.pop_id), mV)
@@ -571,7 +596,7 @@ class Simulator:
             pl.set_state(p.pop_id, "V_m", v)
             for name in pl_state_names(self._model):
                 pl.set_state(p.pop_id, name, np.zeros(p.n))
-            if self._model is aeif_cond_alpha:
+            if self._model.conductance:
                 pl.set_state(p.pop_id, "h", np.full(p.n, self.dt))
 
     # -- run
@@ -636,4 +661,8 @@ def pl_state_names(model):
         return ("I_syn_ex", "dI_syn_ex", "I_syn_in", "dI_syn_in", "y0", "r")
     if model is iaf_psc_exp:
         return ("i_syn_ex", "i_syn_in", "i_0", "i_1", "r")
+    if model is iaf_cond_exp:
+        return ("g_ex", "g_in", "I_stim", "r")
+    if model is iaf_cond_alpha:
+        return ("dg_ex", "g_ex", "dg_in", "g_in", "I_stim", "r")
     return ("dg_ex", "g_ex", "dg_in", "g_in", "w", "I_stim", "r")

@@ -30,15 +30,25 @@ enum {
     BSPK_ERR_CUDA = -3,      /* CUDA runtime failure */
     BSPK_ERR_UNSUPPORTED = -4,
     BSPK_ERR_TIMEOUT = -5,   /* a bounded device wait ran out */
-    BSPK_ERR_UNSTABLE = -6,  /* aeif_cond_alpha instability guard */
+    BSPK_ERR_UNSTABLE = -6,  /* aeif_cond_alpha / iaf_cond_exp instability guard */
     BSPK_ERR_OVERFLOW = -7,  /* a device buffer (spike record) overflowed */
     BSPK_ERR_RKCAP = -8      /* RKF45 iteration cap reached */
 };
 
 /* neuron models: iaf_psc_alpha (_nest_neuron/iaf_psc_alpha.py:558),
  * iaf_psc_exp (_nest_neuron/iaf_psc_exp.py:552), aeif_cond_alpha
- * (_nest_neuron/aeif_cond_alpha.py:627) */
-enum { BSPK_IAF_PSC_ALPHA = 0, BSPK_IAF_PSC_EXP = 1, BSPK_AEIF_COND_ALPHA = 2 };
+ * (_nest_neuron/aeif_cond_alpha.py:627), iaf_cond_exp
+ * (_nest_neuron/iaf_cond_exp.py:519), iaf_cond_alpha
+ * (_nest_neuron/iaf_cond_alpha.py:523).  The last three are conductance
+ * models integrated by adaptive RKF45 with receptor ports 0 (g_ex) and
+ * 1 (g_in). */
+enum {
+    BSPK_IAF_PSC_ALPHA = 0,
+    BSPK_IAF_PSC_EXP = 1,
+    BSPK_AEIF_COND_ALPHA = 2,
+    BSPK_IAF_COND_EXP = 3,
+    BSPK_IAF_COND_ALPHA = 4
+};
 
 /* delivery semantics:
  *  LEGACY: Simulator timing, a spike of step m reaches step m + D + 1
@@ -76,7 +86,9 @@ int bspk_plan_destroy(bspk_plan *plan);
  * model's fixed order (see DESIGN: iaf_psc_alpha E_L C_m tau_m t_ref V_th
  * V_reset tau_syn_ex tau_syn_in I_e V_min; iaf_psc_exp the same without V_min;
  * aeif_cond_alpha V_peak V_reset t_ref g_L C_m E_ex E_in E_L Delta_T tau_w a b
- * V_th tau_syn_ex tau_syn_in I_e gsl_error_tol).  Propagators are computed
+ * V_th tau_syn_ex tau_syn_in I_e gsl_error_tol; iaf_cond_exp and
+ * iaf_cond_alpha E_L C_m t_ref V_th V_reset E_ex E_in g_L tau_syn_ex
+ * tau_syn_in I_e gsl_error_tol).  Propagators are computed
  * here in float64.  Replaces Simulator.create (simulator.py:458) and the
  * models' _precompute_propagators (iaf_psc_alpha.py:451-479,
  * iaf_psc_exp.py:492-512). */

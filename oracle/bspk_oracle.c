@@ -268,11 +268,18 @@ struct bo_sim {
     double *y;   /* [2][ntot] per-projection vector */
 };
 
-static const char *state_names[3][NS] = {
+static const char *state_names[5][NS] = {
     {"V_m", "I_syn_ex", "dI_syn_ex", "I_syn_in", "dI_syn_in", "y0", "", "", ""},
     {"V_m", "i_syn_ex", "i_syn_in", "i_0", "i_1", "", "", "", ""},
     {"V_m", "dg_ex", "g_ex", "dg_in", "g_in", "w", "h", "I_stim", ""},
+    {"V_m", "g_ex", "g_in", "h", "I_stim", "", "", "", ""},
+    {"V_m", "dg_ex", "g_ex", "dg_in", "g_in", "h", "I_stim", "", ""},
 };
+
+/* ODE leaves of a conductance model; its slots are the leaves, h, I_stim */
+static int n_ode(int model) {
+    return model == BO_AEIF_COND_ALPHA ? 6 : (model == BO_IAF_COND_EXP ? 3 : 5);
+}
 
 bo_sim *bo_create(double dt, int semantics, int model) {
     bo_sim *s = (bo_sim *)calloc(1, sizeof(bo_sim));
@@ -316,7 +323,9 @@ static void grow_state(bo_sim *s, int old_n, int new_n) {
  * iaf_psc_alpha: E_L C_m tau_m t_ref V_th V_reset tau_syn_ex tau_syn_in I_e V_min
  * iaf_psc_exp:   E_L C_m tau_m t_ref V_th V_reset tau_syn_ex tau_syn_in I_e
  * aeif_cond_alpha: V_peak V_reset t_ref g_L C_m E_ex E_in E_L Delta_T tau_w a b
- *                  V_th tau_syn_ex tau_syn_in I_e gsl_error_tol */
+ *                  V_th tau_syn_ex tau_syn_in I_e gsl_error_tol
+ * iaf_cond_exp, iaf_cond_alpha: E_L C_m t_ref V_th V_reset E_ex E_in g_L
+ *                  tau_syn_ex tau_syn_in I_e gsl_error_tol */
 int bo_add_pop(bo_sim *s, int n, const double *params, int n_params) {
     if (s->npop >= 64 || n_params > 24 || n < 0) return -1;
     pop_t *P = &s->pops[s->npop];
@@ -359,6 +368,9 @@ int bo_add_pop(bo_sim *s, int n, const double *params, int n_params) {
         if (s->model == BO_AEIF_COND_ALPHA) {
             s->st[0][k] = P->p[7]; /* V_m = E_L */
             s->st[6][k] = h;       /* integration_step = dt (aeif_cond_alpha.py:527) */
+        } else if (s->model == BO_IAF_COND_EXP || s->model == BO_IAF_COND_ALPHA) {
+            s->st[0][k] = -70.0;                 /* V_initializer (iaf_cond_exp.py:310) */
+            s->st[n_ode(s->model)][k] = h;       /* integration_step = dt */
         } else {
             s->st[0][k] = P->p[0]; /* V_m = E_L */
         }
@@ -700,29 +712,64 @@ static inline double nanmax(double a, double b) {
     return a > b ? a : b;
 }
 
-static int step_aeif(bo_sim *s, pop_t *P, int g, double w_ex, double w_in, double x_next,
+/* iaf_cond_exp (_nest_neuron/iaf_cond_exp.py:456-490; y = V, g_ex, g_in) and
+ * iaf_cond_alpha (_nest_neuron/iaf_cond_alpha.py:459-491; y = V, dg_ex, g_ex,
+ * dg_in, g_in): the membrane sees min(V, V_th), or V_reset while refractory */
+static void iaf_cond_vf(int model, const pop_t *P, int r, double i_stim, const double *y,
+                        double *dy) {
+    double E_L = P->p[0], C_m = P->p[1], V_th = P->p[3], V_reset = P->p[4], E_ex = P->p[5],
+           E_in = P->p[6], g_L = P->p[7], tex = P->p[8], tin = P->p[9], I_e = P->p[10];
+    int refr = r > 0;
+    double v_eff = refr ? V_reset : (y[0] < V_th ? y[0] : (y[0] != y[0] ? y[0] : V_th));
+    double gex = model == BO_IAF_COND_EXP ? y[1] : y[2];
+    double gin = model == BO_IAF_COND_EXP ? y[2] : y[4];
+    double i_syn_exc = gex * (v_eff - E_ex);
+    double i_syn_inh = gin * (v_eff - E_in);
+    double i_leak = g_L * (v_eff - E_L);
+    double dV = (-i_leak - i_syn_exc - i_syn_inh + I_e + i_stim) / C_m;
+    dy[0] = refr ? 0.0 : dV;
+    if (model == BO_IAF_COND_EXP) {
+        dy[1] = -y[1] / tex;
+        dy[2] = -y[2] / tin;
+    } else {
+        dy[1] = -y[1] / tex;
+        dy[2] = y[1] - y[2] / tex;
+        dy[3] = -y[3] / tin;
+        dy[4] = y[3] - y[4] / tin;
+    }
+}
+
+/* One dt of a conductance model: the adaptive RKF45 loop with the model's
+ * in-loop event (aeif_cond_alpha.py:594-625, iaf_cond_exp.py:487-517,
+ * iaf_cond_alpha.py:493-521), then the refractory countdown and the
+ * synaptic jumps (aeif_cond_alpha.py:709-728, iaf_cond_exp.py:594-614,
+ * iaf_cond_alpha.py:602-624). */
+static int step_cond(bo_sim *s, pop_t *P, int g, double w_ex, double w_in, double x_next,
                      int *unstable) {
-    const double dt = s->dt, min_h = 1e-8, atol = P->p[16];
+    const int model = s->model, ns = n_ode(model);
+    const int aeif = model == BO_AEIF_COND_ALPHA;
+    const double dt = s->dt, min_h = 1e-8, atol = aeif ? P->p[16] : P->p[11];
+    const int max_iters = model == BO_IAF_COND_EXP ? 10000 : 100000; /* _MAX_ITERS */
     double y[6];
-    for (int i = 0; i < 6; ++i) y[i] = s->st[i][g];
-    double h = s->st[6][g], i_stim = s->st[7][g];
+    for (int i = 0; i < ns; ++i) y[i] = s->st[i][g];
+    double h = s->st[ns][g], i_stim = s->st[ns + 1][g];
     int r = s->ref[g];
-    double V_reset = P->p[1], b = P->p[11];
-    double v_peak_detect = P->p[8] > 0.0 ? P->p[0] : P->p[12];
+    double V_reset = aeif ? P->p[1] : P->p[4], b = aeif ? P->p[11] : 0.0;
+    double v_peak_detect = aeif ? (P->p[8] > 0.0 ? P->p[0] : P->p[12]) : P->p[3];
     int spiked = 0;
     double t_loc = 0.0;
     if (h < min_h) h = min_h;
     int iters = 0;
     double k[6][6];
-    while (t_loc < dt && iters < 100000) {
+    while (t_loc < dt && iters < max_iters) {
         double hh = h < dt - t_loc ? h : dt - t_loc;
         h = hh > min_h ? hh : min_h;
         for (int st = 0; st < 6; ++st) {
             double yi[6];
             if (st == 0) {
-                for (int i = 0; i < 6; ++i) yi[i] = y[i];
+                for (int i = 0; i < ns; ++i) yi[i] = y[i];
             } else {
-                for (int i = 0; i < 6; ++i) {
+                for (int i = 0; i < ns; ++i) {
                     double acc = 0.0;
                     int first = 1;
                     for (int j = 0; j < st; ++j) {
@@ -734,10 +781,11 @@ static int step_aeif(bo_sim *s, pop_t *P, int g, double w_ex, double w_in, doubl
                     yi[i] = y[i] + h * acc;
                 }
             }
-            aeif_vf(P, r, i_stim, yi, k[st]);
+            if (aeif) aeif_vf(P, r, i_stim, yi, k[st]);
+            else iaf_cond_vf(model, P, r, i_stim, yi, k[st]);
         }
         double yh[6], ye[6], err = 0.0;
-        for (int i = 0; i < 6; ++i) {
+        for (int i = 0; i < ns; ++i) {
             double acc = 0.0, eacc = 0.0;
             int first = 1, efirst = 1;
             for (int j = 0; j < 6; ++j) {
@@ -762,15 +810,17 @@ static int step_aeif(bo_sim *s, pop_t *P, int g, double w_ex, double w_in, doubl
         if (err != err) err = INFINITY;
         int accept = (err <= 1.0) || (h <= min_h);
         if (accept) {
-            for (int i = 0; i < 6; ++i) y[i] = yh[i];
+            for (int i = 0; i < ns; ++i) y[i] = yh[i];
             t_loc = t_loc + h;
-            /* _event_fn (aeif_cond_alpha.py:594-625) */
-            if (y[0] < -1e3 || y[5] < -1e6 || y[5] > 1e6) *unstable = 1;
+            /* _event_fn: instability guard on the pre-reset state (AdEx:
+             * V and w; iaf_cond_exp: V; iaf_cond_alpha: none) */
+            if (aeif && (y[0] < -1e3 || y[5] < -1e6 || y[5] > 1e6)) *unstable = 1;
+            if (model == BO_IAF_COND_EXP && y[0] < -1e3) *unstable = 1;
             if (r > 0) y[0] = V_reset;
             if (r <= 0 && y[0] >= v_peak_detect) {
                 spiked = 1;
                 y[0] = V_reset;
-                y[5] = y[5] + b;
+                if (aeif) y[5] = y[5] + b;
                 if (P->ref_count > 0) r = P->ref_count + 1;
             }
         }
@@ -792,13 +842,19 @@ static int step_aeif(bo_sim *s, pop_t *P, int g, double w_ex, double w_in, doubl
 #pragma omp atomic
     s->rk_substeps += iters;
     if (r > 0) r = r - 1;
-    /* synaptic jumps after integration (aeif_cond_alpha.py:709-728) */
-    double tex = P->p[13], tin = P->p[14];
-    y[1] = y[1] + (2.718281828459045 / tex) * w_ex;
-    y[3] = y[3] + (2.718281828459045 / tin) * w_in;
-    for (int i = 0; i < 6; ++i) s->st[i][g] = y[i];
-    s->st[6][g] = h;
-    s->st[7][g] = x_next;
+    /* synaptic jumps after integration: g += w (iaf_cond_exp), dg += e / tau * w
+     * (alpha kernels) */
+    if (model == BO_IAF_COND_EXP) {
+        y[1] = y[1] + w_ex;
+        y[2] = y[2] + w_in;
+    } else {
+        double tex = aeif ? P->p[13] : P->p[8], tin = aeif ? P->p[14] : P->p[9];
+        y[1] = y[1] + (2.718281828459045 / tex) * w_ex;
+        y[3] = y[3] + (2.718281828459045 / tin) * w_in;
+    }
+    for (int i = 0; i < ns; ++i) s->st[i][g] = y[i];
+    s->st[ns][g] = h;
+    s->st[ns + 1][g] = x_next;
     s->ref[g] = r;
     return spiked;
 }
@@ -816,7 +872,7 @@ int bo_step_neuron(bo_sim *s, int gid, double w0, double w1, double x_next) {
     int unstable = 0;
     if (s->model == BO_IAF_PSC_ALPHA) return step_iaf_alpha(s, P, gid, w0, x_next);
     if (s->model == BO_IAF_PSC_EXP) return step_iaf_exp(s, P, gid, w0, x_next);
-    int sp = step_aeif(s, P, gid, w0, w1, x_next, &unstable);
+    int sp = step_cond(s, P, gid, w0, w1, x_next, &unstable);
     return unstable ? -2 : sp;
 }
 
@@ -863,7 +919,7 @@ int64_t bo_run(bo_sim *s, int64_t n_steps, int64_t *spk_step, int32_t *spk_gid,
                 int g = P->off + k, sp;
                 if (s->model == BO_IAF_PSC_ALPHA) sp = step_iaf_alpha(s, P, g, acc0[g], 0.0);
                 else if (s->model == BO_IAF_PSC_EXP) sp = step_iaf_exp(s, P, g, acc0[g], 0.0);
-                else sp = step_aeif(s, P, g, acc0[g], acc1[g], 0.0, &uns);
+                else sp = step_cond(s, P, g, acc0[g], acc1[g], 0.0, &uns);
                 hrow[g] = (unsigned char)sp;
             }
             unstable |= uns;

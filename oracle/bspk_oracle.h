@@ -24,7 +24,13 @@ extern "C" {
 #endif
 
 /* neuron models (same ids as the product library) */
-enum { BO_IAF_PSC_ALPHA = 0, BO_IAF_PSC_EXP = 1, BO_AEIF_COND_ALPHA = 2 };
+enum {
+    BO_IAF_PSC_ALPHA = 0,
+    BO_IAF_PSC_EXP = 1,
+    BO_AEIF_COND_ALPHA = 2,
+    BO_IAF_COND_EXP = 3,
+    BO_IAF_COND_ALPHA = 4
+};
 
 /* delivery semantics
  *  LEGACY: reference Simulator -- a spike of step m reaches the update of

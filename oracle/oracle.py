@@ -32,7 +32,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 
-MODEL_IDS = {"iaf_psc_alpha": 0, "iaf_psc_exp": 1, "aeif_cond_alpha": 2}
+MODEL_IDS = {"iaf_psc_alpha": 0, "iaf_psc_exp": 1, "aeif_cond_alpha": 2, "iaf_cond_exp": 3,
+             "iaf_cond_alpha": 4}
 LEGACY, RING = 0, 1
 
 
@@ -260,7 +261,7 @@ class OracleSim:
         v = np.zeros((n_steps, n_rec), np.float64)
         n = self._L.bo_run(self._h, int(n_steps), _p(st), _p(gid), int(cap), _p(v))
         if n == -2:
-            raise FloatingPointError("Numerical instability in aeif_cond_alpha dynamics.")
+            raise FloatingPointError(f"Numerical instability in {self.model} dynamics.")
         if n > cap:
             raise OverflowError("spike buffer too small")
         return st[:n], gid[:n], v
@@ -268,7 +269,7 @@ class OracleSim:
     def step_neuron(self, gid, w0=0.0, w1=0.0, x_next=0.0):
         r = self._L.bo_step_neuron(self._h, int(gid), float(w0), float(w1), float(x_next))
         if r == -2:
-            raise FloatingPointError("Numerical instability in aeif_cond_alpha dynamics.")
+            raise FloatingPointError(f"Numerical instability in {self.model} dynamics.")
         return r
 
     @property
