@@ -43,6 +43,12 @@ class StdpParams(C.Structure):
                 ("Wmax", C.c_double)]
 
 
+class StdpTripletParams(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("tau_plus", "tau_plus_triplet", "tau_minus",
+                                          "tau_minus_triplet", "Aplus", "Aplus_triplet",
+                                          "Aminus", "Aminus_triplet", "Wmax")]
+
+
 _lib = None
 
 
@@ -69,6 +75,7 @@ def lib():
             "bspk_drive_add_poisson": (C.c_int, [vp, C.c_int, dbl, dbl, C.c_int, u32, i64, i64,
                                                  C.c_int, C.POINTER(C.c_int)]),
             "bspk_stdp_attach": (C.c_int, [vp, C.c_int, C.POINTER(StdpParams)]),
+            "bspk_stdp_triplet_attach": (C.c_int, [vp, C.c_int, C.POINTER(StdpTripletParams)]),
             "bspk_proj_csr_get": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
             "bspk_record_v": (C.c_int, [vp, C.c_int, vp]),
             "bspk_record_spikes_of": (C.c_int, [vp, C.c_int, vp]),
@@ -223,6 +230,13 @@ class Plan:
                     mu_plus=1.0, mu_minus=1.0, Wmax=100.0):
         sp = StdpParams(tau_plus, tau_minus, lambda_, alpha, mu_plus, mu_minus, Wmax)
         check(self._L.bspk_stdp_attach(self._h, proj, C.byref(sp)))
+
+    def attach_stdp_triplet(self, proj, tau_plus=16.8, tau_plus_triplet=101.0, tau_minus=20.0,
+                            tau_minus_triplet=110.0, Aplus=5e-10, Aplus_triplet=0.0062,
+                            Aminus=0.007, Aminus_triplet=0.00023, Wmax=100.0):
+        tp = StdpTripletParams(tau_plus, tau_plus_triplet, tau_minus, tau_minus_triplet, Aplus,
+                               Aplus_triplet, Aminus, Aminus_triplet, Wmax)
+        check(self._L.bspk_stdp_triplet_attach(self._h, proj, C.byref(tp)))
 
     def record_v(self, gids):
         g = np.ascontiguousarray(gids, np.int32)

@@ -48,13 +48,16 @@ struct StdpDev {
     int pre_off, post_off, n_pre, n_post, lag;  // lag: arrival lag of the pre spike
     int receptor;
     double tau_plus, tau_minus, lambda_, alpha, mu_plus, mu_minus, Wmax, dec_pre, dec_post;
+    int rule;  // 0: pair stdp_synapse, 1: stdp_triplet_synapse
+    double a2p, a3p, a2m, a3m, dec_pre2, dec_post2;  // triplet amplitudes, slow-trace decays
     const int64_t *indptr;   // CSR over pre
     const uint32_t *edges;   // post_local | lag << 24
     double *w;               // FP64 weights, CSR order
     const int64_t *cindptr;  // CSC over post
     const int64_t *cperm;    // CSC position -> CSR edge id
     const uint32_t *cedges;  // pre_local | lag << 24
-    double *pre_trace, *post_trace;
+    double *pre_trace, *post_trace;    // fast traces
+    double *pre_trace2, *post_trace2;  // slow traces (triplet rule)
     int *pre_list, *post_list, *counts;  // counts[0] pres, counts[1] posts of this step
 };
 

@@ -34,8 +34,8 @@ std::vector<Section> sections(bspk_plan *p) {
     for (auto &J : p->projs) {
         if (!J.plastic) continue;
         s.push_back({J.d_wplastic, sizeof(double) * J.post_local.size()});
-        s.push_back({J.d_pre_trace, sizeof(double) * p->pops[J.pre].n});
-        s.push_back({J.d_post_trace, sizeof(double) * p->pops[J.post].n});
+        s.push_back({J.d_pre_trace, sizeof(double) * p->pops[J.pre].n * J.trace_cols()});
+        s.push_back({J.d_post_trace, sizeof(double) * p->pops[J.post].n * J.trace_cols()});
     }
     return s;
 }

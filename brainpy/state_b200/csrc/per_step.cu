@@ -352,11 +352,13 @@ __global__ void k_stdp_traces(StdpDev s, const uint64_t *hist, const int64_t *st
     if (i < s.n_pre) {
         const bool x = fired(hist, s.pre_off + i, n - s.lag);
         s.pre_trace[i] = s.pre_trace[i] * s.dec_pre + (x ? 1.0 : 0.0);
+        if (s.rule == 1) s.pre_trace2[i] = s.pre_trace2[i] * s.dec_pre2 + (x ? 1.0 : 0.0);
         if (x) s.pre_list[atomicAdd(&s.counts[0], 1)] = i;
     }
     if (i < s.n_post) {
         const bool y = fired(hist, s.post_off + i, n - 1);
         s.post_trace[i] = s.post_trace[i] * s.dec_post + (y ? 1.0 : 0.0);
+        if (s.rule == 1) s.post_trace2[i] = s.post_trace2[i] * s.dec_post2 + (y ? 1.0 : 0.0);
         if (y) s.post_list[atomicAdd(&s.counts[1], 1)] = i;
     }
 }
@@ -368,6 +370,19 @@ __device__ __forceinline__ double stdp_facilitate(const StdpDev &s, double w, do
 __device__ __forceinline__ double stdp_depress(const StdpDev &s, double w, double kminus) {
     const double nw = w / s.Wmax - s.alpha * s.lambda_ * pow(w / s.Wmax, s.mu_minus) * kminus;
     return nw > 0.0 ? nw * s.Wmax : 0.0;
+}
+// stdp_triplet_synapse.py:179-197: potentiation reads the fast pre trace r1
+// weighted by the slow post trace o2, depression the fast post trace o1
+// weighted by the slow pre trace r2 (each excluding this step's spike)
+__device__ __forceinline__ double triplet_facilitate(const StdpDev &s, double w, double r1,
+                                                     double o2) {
+    const double nw = w + r1 * (s.a2p + s.a3p * o2);
+    return nw < s.Wmax ? nw : s.Wmax;
+}
+__device__ __forceinline__ double triplet_depress(const StdpDev &s, double w, double o1,
+                                                  double r2) {
+    const double nw = w - o1 * (s.a2m + s.a3m * r2);
+    return nw > 0.0 ? nw : 0.0;
 }
 
 // STDP 2: facilitation on the in-edges of posts that fired at n - 1
@@ -385,7 +400,9 @@ __global__ void k_stdp_facilitate(StdpDev s, const uint64_t *hist, const int64_t
             const double x = fired(hist, s.pre_off + pre, n - s.lag) ? 1.0 : 0.0;
             const double kplus = s.pre_trace[pre] - x;
             const int64_t eid = s.cperm[e];
-            s.w[eid] = stdp_facilitate(s, s.w[eid], kplus);
+            // the post fired at n - 1, so its own spike is 1 in every post trace
+            s.w[eid] = s.rule == 1 ? triplet_facilitate(s, s.w[eid], kplus, s.post_trace2[j] - 1.0)
+                                   : stdp_facilitate(s, s.w[eid], kplus);
         }
     }
 }
@@ -407,7 +424,9 @@ __global__ void k_stdp_depress(StdpDev s, const StepArgs<Real> a) {
             const int j = static_cast<int>(s.edges[e] & kEdgePostMask);
             const double y = fired(a.hist, s.post_off + j, n - 1) ? 1.0 : 0.0;
             const double kminus = s.post_trace[j] - y;
-            const double w = stdp_depress(s, s.w[e], kminus);
+            // the pre's delayed spike arrives now: 1 in every pre trace
+            const double w = s.rule == 1 ? triplet_depress(s, s.w[e], kminus, s.pre_trace2[i] - 1.0)
+                                         : stdp_depress(s, s.w[e], kminus);
             s.w[e] = w;
             atomicAdd(a.ring + (static_cast<size_t>(slot_n) * a.R + s.receptor) * a.N + s.post_off + j,
                       static_cast<Real>(w));
@@ -474,6 +493,19 @@ std::vector<StdpDev> stdp_descs(bspk_plan *p) {
         s.Wmax = J.stdp.Wmax;
         s.dec_pre = std::exp(-p->cfg.dt / J.stdp.tau_plus);
         s.dec_post = std::exp(-p->cfg.dt / J.stdp.tau_minus);
+        s.rule = J.rule;
+        if (J.rule == 1) {
+            const bspk_stdp_triplet_params &t = J.trip;
+            s.Wmax = t.Wmax;
+            s.a2p = t.Aplus;
+            s.a3p = t.Aplus_triplet;
+            s.a2m = t.Aminus;
+            s.a3m = t.Aminus_triplet;
+            s.dec_pre = std::exp(-p->cfg.dt / t.tau_plus);
+            s.dec_post = std::exp(-p->cfg.dt / t.tau_minus);
+            s.dec_pre2 = std::exp(-p->cfg.dt / t.tau_plus_triplet);
+            s.dec_post2 = std::exp(-p->cfg.dt / t.tau_minus_triplet);
+        }
         s.indptr = J.d_indptr;
         s.edges = J.d_edges;
         s.w = J.d_wplastic;
@@ -482,6 +514,8 @@ std::vector<StdpDev> stdp_descs(bspk_plan *p) {
         s.cedges = J.d_cedges;
         s.pre_trace = static_cast<double *>(J.d_pre_trace);
         s.post_trace = static_cast<double *>(J.d_post_trace);
+        s.pre_trace2 = J.rule == 1 ? s.pre_trace + s.n_pre : nullptr;
+        s.post_trace2 = J.rule == 1 ? s.post_trace + s.n_post : nullptr;
         s.pre_list = J.d_pre_list;
         s.post_list = J.d_post_list;
         s.counts = p->d_step_counters + 2 + 2 * k;

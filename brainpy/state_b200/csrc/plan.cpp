@@ -454,23 +454,56 @@ int bspk_proj_csr_get(bspk_plan *p, int proj_id, int64_t *indptr, int32_t *post_
     return BSPK_OK;
 }
 
-int bspk_stdp_attach(bspk_plan *p, int proj_id, const bspk_stdp_params *sp) {
-    if (!p || !sp) return fail(BSPK_ERR_ARG, "null argument");
+}  // extern "C"
+
+namespace {
+// Checks shared by the plastic rules: an existing CSR projection of a plan
+// that is not uploaded, one homogeneous delay (the substrate's InputDelay).
+int plastic_checks(bspk_plan *p, int proj_id) {
     if (p->uploaded) return fail(BSPK_ERR_STATE, "plan already uploaded");
     if (proj_id < 0 || proj_id >= static_cast<int>(p->projs.size())) return fail(BSPK_ERR_ARG, "bad projection");
-    if (!(sp->tau_plus > 0)) return fail(BSPK_ERR_ARG, "'tau_plus' must be > 0.");
-    if (!(sp->tau_minus > 0)) return fail(BSPK_ERR_ARG, "'tau_minus' must be > 0.");
     if (p->cfg.deterministic) return fail(BSPK_ERR_UNSUPPORTED, "STDP is not available in deterministic mode");
-    Proj &J = p->projs[proj_id];
+    const Proj &J = p->projs[proj_id];
     for (size_t e = 1; e < J.delay.size(); ++e)
         if (J.delay[e] != J.delay[0])
             return fail(BSPK_ERR_UNSUPPORTED, "a plastic projection needs one homogeneous delay");
+    return BSPK_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int bspk_stdp_attach(bspk_plan *p, int proj_id, const bspk_stdp_params *sp) {
+    if (!p || !sp) return fail(BSPK_ERR_ARG, "null argument");
+    if (!(sp->tau_plus > 0)) return fail(BSPK_ERR_ARG, "'tau_plus' must be > 0.");
+    if (!(sp->tau_minus > 0)) return fail(BSPK_ERR_ARG, "'tau_minus' must be > 0.");
+    int rc = plastic_checks(p, proj_id);
+    if (rc) return rc;
+    Proj &J = p->projs[proj_id];
     for (double w : J.w)
         if ((w > 0) != (sp->Wmax > 0) && w != 0.0)
             return fail(BSPK_ERR_ARG, "Weight and Wmax must have same sign.");
     J.plastic = true;
     J.homogeneous = false;
+    J.rule = 0;
     J.stdp = *sp;
+    return BSPK_OK;
+}
+
+int bspk_stdp_triplet_attach(bspk_plan *p, int proj_id, const bspk_stdp_triplet_params *tp) {
+    if (!p || !tp) return fail(BSPK_ERR_ARG, "null argument");
+    // stdp_triplet_synapse.py:152-155
+    const double taus[4] = {tp->tau_plus, tp->tau_plus_triplet, tp->tau_minus, tp->tau_minus_triplet};
+    const char *names[4] = {"tau_plus", "tau_plus_triplet", "tau_minus", "tau_minus_triplet"};
+    for (int i = 0; i < 4; ++i)
+        if (!(taus[i] > 0)) return fail(BSPK_ERR_ARG, std::string("'") + names[i] + "' must be > 0.");
+    int rc = plastic_checks(p, proj_id);
+    if (rc) return rc;
+    Proj &J = p->projs[proj_id];
+    J.plastic = true;
+    J.homogeneous = false;
+    J.rule = 1;
+    J.trip = *tp;
     return BSPK_OK;
 }
 
@@ -563,13 +596,14 @@ int upload_projs(bspk_plan *p) {
         }
         if (J.plastic) {
             void *t1 = nullptr, *t2 = nullptr;
-            int rc2 = dalloc_bytes(p, &t1, sizeof(double) * npre);
-            if (!rc2) rc2 = dalloc_bytes(p, &t2, sizeof(double) * npost);
+            const size_t cols = static_cast<size_t>(J.trace_cols());
+            int rc2 = dalloc_bytes(p, &t1, sizeof(double) * npre * cols);
+            if (!rc2) rc2 = dalloc_bytes(p, &t2, sizeof(double) * npost * cols);
             if (!rc2) rc2 = dalloc(p, &J.d_pre_list, npre);
             if (!rc2) rc2 = dalloc(p, &J.d_post_list, npost);
             if (rc2) return rc2;
-            BSPK_CUDA(cudaMemset(t1, 0, sizeof(double) * npre));
-            BSPK_CUDA(cudaMemset(t2, 0, sizeof(double) * npost));
+            BSPK_CUDA(cudaMemset(t1, 0, sizeof(double) * npre * cols));
+            BSPK_CUDA(cudaMemset(t2, 0, sizeof(double) * npost * cols));
             J.d_pre_trace = t1;
             J.d_post_trace = t2;
         }

@@ -35,6 +35,9 @@ struct Proj {
     double w0 = 0.0;
     bool plastic = false;
     bspk_stdp_params stdp{};
+    int rule = 0;  // 0: pair stdp_synapse, 1: stdp_triplet_synapse
+    bspk_stdp_triplet_params trip{};
+    int trace_cols() const { return rule == 1 ? 2 : 1; }  // traces per side
     int input_order = 0;
     // device
     int64_t *d_indptr = nullptr;
@@ -45,7 +48,7 @@ struct Proj {
     double *d_cw = nullptr;
     double *d_wplastic = nullptr;   // FP64 plastic weights (CSR order)
     int64_t *d_cperm = nullptr;     // CSC position -> CSR edge id
-    void *d_pre_trace = nullptr, *d_post_trace = nullptr;
+    void *d_pre_trace = nullptr, *d_post_trace = nullptr;  // [trace_cols][n]
     int *d_pre_list = nullptr, *d_post_list = nullptr;  // per-step STDP work lists
 };
 

@@ -204,6 +204,46 @@ class stdp_synapse:
         if Kplus < 0:
             raise ValueError("Kplus must be non-negative.")
 
+    def attach(self, pl, proj):
+        pl.attach_stdp(proj, self.tau_plus, self.tau_minus, self.lambda_, self.alpha,
+                       self.mu_plus, self.mu_minus, self.Wmax)
+
+
+class stdp_synapse_hom(stdp_synapse):
+    """NEST stdp_synapse_hom: the pair rule with parameters shared by every
+    edge of the projection, which is already how every rule here is held
+    (_nest_plasticity/stdp_synapse_hom.py:24-69)."""
+
+
+class stdp_triplet_synapse:
+    """Pfister-Gerstner triplet STDP spec (_nest_plasticity/stdp_triplet_synapse.py:126-158,
+    NEST defaults)."""
+
+    def __init__(self, weight=1.0, delay=1.0, tau_plus=16.8, tau_plus_triplet=101.0,
+                 tau_minus=20.0, tau_minus_triplet=110.0, Aplus=5e-10, Aplus_triplet=0.0062,
+                 Aminus=0.007, Aminus_triplet=0.00023, Wmax=100.0, Kplus=0.0,
+                 Kplus_triplet=0.0):
+        self.weight = weight
+        self.delay = delay
+        self.taus = {}
+        for name, q in (("tau_plus", tau_plus), ("tau_plus_triplet", tau_plus_triplet),
+                        ("tau_minus", tau_minus), ("tau_minus_triplet", tau_minus_triplet)):
+            v = float(mantissa(q, ms))
+            if v <= 0.0:
+                raise ValueError(f"'{name}' must be > 0.")
+            self.taus[name] = v
+        self.Aplus, self.Aplus_triplet = float(Aplus), float(Aplus_triplet)
+        self.Aminus, self.Aminus_triplet = float(Aminus), float(Aminus_triplet)
+        self.Wmax = float(Wmax)
+        if Kplus != 0.0 or Kplus_triplet != 0.0:
+            raise NotImplementedError("the substrate seeds the traces at 0")
+
+    def attach(self, pl, proj):
+        pl.attach_stdp_triplet(proj, self.taus["tau_plus"], self.taus["tau_plus_triplet"],
+                               self.taus["tau_minus"], self.taus["tau_minus_triplet"],
+                               self.Aplus, self.Aplus_triplet, self.Aminus,
+                               self.Aminus_triplet, self.Wmax)
+
 
 # ----------------------------------------------------------- distributions
 
@@ -576,8 +616,7 @@ class Simulator:
     @staticmethod
     def _attach(pl, j, syn):
         if syn is not None:
-            pl.attach_stdp(j, syn.tau_plus, syn.tau_minus, syn.lambda_, syn.alpha, syn.mu_plus,
-                           syn.mu_minus, syn.Wmax)
+            syn.attach(pl, j)
 
     def _init_state(self):
         pl = self._plan

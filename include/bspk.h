@@ -73,6 +73,14 @@ typedef struct {
     double tau_plus, tau_minus, lambda_, alpha, mu_plus, mu_minus, Wmax;
 } bspk_stdp_params;
 
+/* stdp_triplet_synapse parameters (_nest_plasticity/stdp_triplet_synapse.py:
+ * 126-141): fast/slow trace constants per side and the pair (A2) and
+ * triplet (A3) amplitudes; weights stay in [0, Wmax]. */
+typedef struct {
+    double tau_plus, tau_plus_triplet, tau_minus, tau_minus_triplet;
+    double Aplus, Aplus_triplet, Aminus, Aminus_triplet, Wmax;
+} bspk_stdp_triplet_params;
+
 /* Library version string and build arch. */
 const char *bspk_version(void);
 const char *bspk_last_error(void);
@@ -132,6 +140,13 @@ int bspk_proj_csr_get(bspk_plan *plan, int proj_id, int64_t *indptr, int32_t *po
  * _nest_plasticity/stdp_synapse.py:163-179 driven by the eager substrate of
  * _nest_network/event_plastic.py:390-518 (weights kept in FP64). */
 int bspk_stdp_attach(bspk_plan *plan, int proj_id, const bspk_stdp_params *p);
+
+/* Make a CSR projection plastic with the triplet rule of
+ * _nest_plasticity/stdp_triplet_synapse.py:179-197 (two traces per side) on
+ * the same eager substrate and FP64 weights as bspk_stdp_attach.
+ * stdp_synapse_hom (_nest_plasticity/stdp_synapse_hom.py) is the pair rule
+ * of bspk_stdp_attach under another name. */
+int bspk_stdp_triplet_attach(bspk_plan *plan, int proj_id, const bspk_stdp_triplet_params *p);
 
 /* Recording taps (simulator.py:645-662, :1858-1870): V_m of the listed
  * neurons every step; spikes of all neurons (or of the flagged ones). */

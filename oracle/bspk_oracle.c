@@ -241,8 +241,12 @@ typedef struct {
     int64_t tmin, tmax;
     /* stdp */
     int plastic;
+    int rule; /* 0: stdp_synapse (pair), 1: stdp_triplet_synapse */
     double tau_plus, tau_minus, lambda_, alpha, mu_plus, mu_minus, wmax, dec_pre, dec_post;
     double *pre_trace, *post_trace;
+    /* triplet: slow traces r2 / o2 and the four amplitudes */
+    double dec_pre2, dec_post2, a2p, a3p, a2m, a3m;
+    double *pre_trace2, *post_trace2;
 } input_t;
 
 struct bo_sim {
@@ -306,6 +310,8 @@ void bo_destroy(bo_sim *s) {
         free(in->w);
         free(in->pre_trace);
         free(in->post_trace);
+        free(in->pre_trace2);
+        free(in->post_trace2);
     }
     free(s);
 }
@@ -479,6 +485,53 @@ int bo_set_stdp(bo_sim *s, int proj, double tau_plus, double tau_minus, double l
     return 0;
 }
 
+/* stdp_triplet_synapse (_nest_plasticity/stdp_triplet_synapse.py:160-197):
+ * fast and slow traces per side (r1, r2 with tau_plus, tau_plus_triplet;
+ * o1, o2 with tau_minus, tau_minus_triplet), all decay-then-add. */
+int bo_set_stdp_triplet(bo_sim *s, int proj, double tau_plus, double tau_plus_triplet,
+                        double tau_minus, double tau_minus_triplet, double a2p, double a3p,
+                        double a2m, double a3m, double wmax) {
+    if (proj < 0 || proj >= s->nin || s->ins[proj].kind != 0) return -1;
+    input_t *in = &s->ins[proj];
+    in->plastic = 1;
+    in->rule = 1;
+    in->tau_plus = tau_plus;
+    in->tau_minus = tau_minus;
+    in->a2p = a2p;
+    in->a3p = a3p;
+    in->a2m = a2m;
+    in->a3m = a3m;
+    in->wmax = wmax;
+    in->dec_pre = exp(-s->dt / tau_plus);
+    in->dec_post = exp(-s->dt / tau_minus);
+    in->dec_pre2 = exp(-s->dt / tau_plus_triplet);
+    in->dec_post2 = exp(-s->dt / tau_minus_triplet);
+    in->pre_trace = (double *)calloc((size_t)s->pops[in->pre_pop].n, sizeof(double));
+    in->post_trace = (double *)calloc((size_t)s->pops[in->post_pop].n, sizeof(double));
+    in->pre_trace2 = (double *)calloc((size_t)s->pops[in->pre_pop].n, sizeof(double));
+    in->post_trace2 = (double *)calloc((size_t)s->pops[in->post_pop].n, sizeof(double));
+    return 0;
+}
+
+/* The triplet rule on one edge (stdp_triplet_synapse.py:179-197): every trace
+ * excludes this step's own spike; potentiation on a post spike reads the fast
+ * pre trace weighted by the slow post trace, then depression on a pre spike
+ * reads the fast post trace weighted by the slow pre trace; w in [0, Wmax]. */
+double bo_triplet_update(double w, double pre_s, double post_s, double r1_tr, double r2_tr,
+                         double o1_tr, double o2_tr, double a2p, double a3p, double a2m,
+                         double a3m, double wmax) {
+    double r1 = r1_tr - pre_s, r2 = r2_tr - pre_s, o1 = o1_tr - post_s, o2 = o2_tr - post_s;
+    if (post_s > 0.0) {
+        double nw = w + r1 * (a2p + a3p * o2);
+        w = nw < wmax ? nw : wmax;
+    }
+    if (pre_s > 0.0) {
+        double nw = w - o1 * (a2m + a3m * r2);
+        w = nw > 0.0 ? nw : 0.0;
+    }
+    return w;
+}
+
 int bo_get_weights(bo_sim *s, int proj, double *w_out) {
     if (proj < 0 || proj >= s->nin || s->ins[proj].kind != 0) return -1;
     memcpy(w_out, s->ins[proj].w, sizeof(double) * (size_t)s->ins[proj].n_edges);
@@ -573,10 +626,12 @@ static void legacy_input(bo_sim *s, input_t *in, int64_t n, double *y) {
     for (int i = 0; i < P->n; ++i) {
         double x = (double)fired(s, n - (D + 1), P->off + i);
         in->pre_trace[i] = in->pre_trace[i] * in->dec_pre + x;
+        if (in->rule == 1) in->pre_trace2[i] = in->pre_trace2[i] * in->dec_pre2 + x;
     }
     for (int j = 0; j < Q->n; ++j) {
         double x = (double)fired(s, n - 1, Q->off + j);
         in->post_trace[j] = in->post_trace[j] * in->dec_post + x;
+        if (in->rule == 1) in->post_trace2[j] = in->post_trace2[j] * in->dec_post2 + x;
     }
     for (int i = 0; i < P->n; ++i) {
         double pre_f = (double)fired(s, n - (D + 1), P->off + i);
@@ -584,10 +639,16 @@ static void legacy_input(bo_sim *s, input_t *in, int64_t n, double *y) {
             int j = in->post[e];
             double post_f = (double)fired(s, n - 1, Q->off + j);
             double w = in->w[e];
-            double kplus = in->pre_trace[i] - pre_f;
-            double kminus = in->post_trace[j] - post_f;
-            if (post_f > 0.0) w = stdp_facilitate(in, w, kplus);
-            if (pre_f > 0.0) w = stdp_depress(in, w, kminus);
+            if (in->rule == 1) {
+                w = bo_triplet_update(w, pre_f, post_f, in->pre_trace[i], in->pre_trace2[i],
+                                      in->post_trace[j], in->post_trace2[j], in->a2p, in->a3p,
+                                      in->a2m, in->a3m, in->wmax);
+            } else {
+                double kplus = in->pre_trace[i] - pre_f;
+                double kminus = in->post_trace[j] - post_f;
+                if (post_f > 0.0) w = stdp_facilitate(in, w, kplus);
+                if (pre_f > 0.0) w = stdp_depress(in, w, kminus);
+            }
             in->w[e] = w;
             if (pre_f != 0.0) y[j] += w;
         }

@@ -86,6 +86,12 @@ int bo_add_drive(bo_sim *s, int post_pop, double rate_hz, double weight, int del
                  uint32_t seed, int64_t t_min_step, int64_t t_max_step, int receptor);
 int bo_set_stdp(bo_sim *s, int proj, double tau_plus, double tau_minus, double lambda_,
                 double alpha, double mu_plus, double mu_minus, double wmax);
+int bo_set_stdp_triplet(bo_sim *s, int proj, double tau_plus, double tau_plus_triplet,
+                        double tau_minus, double tau_minus_triplet, double a2p, double a3p,
+                        double a2m, double a3m, double wmax);
+double bo_triplet_update(double w, double pre_s, double post_s, double r1_tr, double r2_tr,
+                         double o1_tr, double o2_tr, double a2p, double a3p, double a2m,
+                         double a3m, double wmax);
 int bo_get_weights(bo_sim *s, int proj, double *w_out);
 int bo_record_v(bo_sim *s, int n, const int32_t *gids);
 /* run n_steps; spikes appended as (step, gid) pairs up to cap; returns the

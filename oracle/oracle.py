@@ -65,6 +65,9 @@ def lib():
         L.bo_add_proj.argtypes = [vp, C.c_int, C.c_int, i64, vp, vp, vp, vp, C.c_int]
         L.bo_add_drive.argtypes = [vp, C.c_int, dbl, dbl, C.c_int, u32, i64, i64, C.c_int]
         L.bo_set_stdp.argtypes = [vp, C.c_int] + [dbl] * 7
+        L.bo_set_stdp_triplet.argtypes = [vp, C.c_int] + [dbl] * 9
+        L.bo_triplet_update.restype = dbl
+        L.bo_triplet_update.argtypes = [dbl] * 12
         L.bo_get_weights.argtypes = [vp, C.c_int, vp]
         L.bo_record_v.argtypes = [vp, C.c_int, vp]
         L.bo_run.restype = i64
@@ -243,6 +246,13 @@ class OracleSim:
                                mu_minus, wmax) != 0:
             raise ValueError("set_stdp failed")
 
+    def set_stdp_triplet(self, proj, tau_plus, tau_plus_triplet, tau_minus, tau_minus_triplet,
+                         Aplus, Aplus_triplet, Aminus, Aminus_triplet, Wmax):
+        if self._L.bo_set_stdp_triplet(self._h, proj, tau_plus, tau_plus_triplet, tau_minus,
+                                       tau_minus_triplet, Aplus, Aplus_triplet, Aminus,
+                                       Aminus_triplet, Wmax) != 0:
+            raise ValueError("set_stdp_triplet failed")
+
     def weights(self, proj, n_edges):
         w = np.zeros(n_edges, np.float64)
         self._L.bo_get_weights(self._h, proj, _p(w))
@@ -307,3 +317,12 @@ def lif_bptt(cfg, row_ptr, col, w, w_in, inputs, targets, grad=True):
     if grad:
         return float(loss[0]), dw[:col.size], dwi[:w_in.size].reshape(w_in.shape), int(nsp[0])
     return float(loss[0]), None, None, int(nsp[0])
+
+
+def triplet_update(w, pre_s, post_s, r, o, Aplus, Aplus_triplet, Aminus, Aminus_triplet, Wmax):
+    """The oracle's triplet rule on one edge; r = (r1, r2), o = (o1, o2) are the
+    substrate-fed traces that include this step's own spike."""
+    return lib().bo_triplet_update(float(w), float(pre_s), float(post_s), float(r[0]),
+                                    float(r[1]), float(o[0]), float(o[1]), float(Aplus),
+                                    float(Aplus_triplet), float(Aminus), float(Aminus_triplet),
+                                    float(Wmax))

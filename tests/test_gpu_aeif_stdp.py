@@ -132,3 +132,68 @@ def test_stdp_network_fp64_matches_oracle(oracle):
     w_cpu = sim.weights(0 + 2, E)  # oracle ids count drives too
     assert np.any(w_cpu != 20.68)
     np.testing.assert_allclose(w_gpu, w_cpu, rtol=1e-12, atol=0)
+
+
+def test_stdp_triplet_network_fp64_matches_oracle(oracle):
+    """stdp_triplet_synapse on E -> E (fast and slow traces per side):
+    rasters identical and FP64 weights within 1e-12 of the oracle."""
+    rng = np.random.default_rng(19)
+    params = [0.0, 250.0, 20.0, 2.0, 20.0, 10.0, 0.5, 0.5, 0.0, -math.inf]
+    NE, NI = 200, 50
+    pieces = []
+    for pre, K, w in ((0, 20, 20.68), (1, 5, -103.4)):
+        for post in (0, 1):
+            n_pre, n_post = (NE if pre == 0 else NI), (NE if post == 0 else NI)
+            pieces.append((pre, post) + random_csr(rng, n_pre, n_post, K, w, 15))
+    v0 = rng.uniform(0.0, 20.0, NE + NI)
+    trip = dict(tau_plus=16.8, tau_plus_triplet=101.0, tau_minus=20.0, tau_minus_triplet=110.0,
+                Aplus=0.5, Aplus_triplet=0.2, Aminus=0.6, Aminus_triplet=0.1, Wmax=3 * 20.68)
+
+    def build(s, is_plan):
+        s.add_pop(NE, params)
+        s.add_pop(NI, params)
+        (s.add_poisson if is_plan else s.add_drive)(0, 17789.0, 20.68, 15, 5)
+        (s.add_poisson if is_plan else s.add_drive)(1, 17789.0, 20.68, 15, 6)
+        ids = [(s.add_csr if is_plan else s.add_proj)(pre, post, indptr, idx, w, d)
+               for pre, post, indptr, idx, w, d in pieces]
+        (s.attach_stdp_triplet if is_plan else s.set_stdp_triplet)(ids[0], **trip)
+        return ids
+
+    pl = _lib.Plan(0.1, precision=64)
+    ids = build(pl, True)
+    pl.upload()
+    pl.set_state(0, "V_m", v0[:NE])
+    pl.set_state(1, "V_m", v0[NE:])
+    sim = oracle.OracleSim(0.1)
+    build(sim, False)
+    sim.set_state(0, "V_m", v0[:NE])
+    sim.set_state(1, "V_m", v0[NE:])
+    pl.run(300)
+    st, g = pl.spikes()
+    ost, og, _ = sim.run(300)
+    assert len(ost) > 0
+    assert set(zip(st.tolist(), g.tolist())) == set(zip(ost.tolist(), og.tolist()))
+    E = pieces[0][3].size
+    w_cpu = sim.weights(0 + 2, E)  # oracle ids count drives too
+    assert np.any(w_cpu > 20.68) and np.any(w_cpu < 20.68)
+    np.testing.assert_allclose(pl.weights(ids[0]), w_cpu, rtol=1e-12, atol=0)
+
+
+def test_stdp_synapse_hom_is_the_pair_rule():
+    """Simulator facade: stdp_synapse_hom gives the weights stdp_synapse gives."""
+    import brainpy.state_b200 as bs
+    from brainpy.state_b200.units import Hz, mV, ms, pA
+    out = []
+    for syn_cls in (bs.stdp_synapse, bs.stdp_synapse_hom):
+        sim = bs.Simulator(dt=0.1 * ms, precision=64)
+        npar = dict(C_m=250.0, tau_m=20.0, tau_syn_ex=0.5, tau_syn_in=0.5, t_ref=2.0,
+                    E_L=0.0, V_reset=10.0, V_th=20.0)
+        ne = sim.create(bs.iaf_psc_alpha, 100, params=npar)
+        noise = sim.create(bs.poisson_generator, rate=20000.0 * Hz)
+        sim.connect(noise, ne, weight=20.68 * pA, delay=1.5 * ms, rule=bs.all_to_all)
+        syn = syn_cls(weight=20.68, delay=1.5, lambda_=0.05, Wmax=3 * 20.68)
+        proj = sim.connect(ne, ne, rule=bs.fixed_indegree(10), synapse=syn, seed=3)
+        sim.simulate(50.0 * ms)
+        out.append(sim._plan.weights(proj.proj_id))
+    assert np.any(out[0] != 20.68)
+    np.testing.assert_array_equal(out[0], out[1])
