@@ -19,7 +19,7 @@ ERRORS = {
     -5: TimeoutError, -6: FloatingPointError, -7: OverflowError, -8: RuntimeError,
 }
 MODELS = {"iaf_psc_alpha": 0, "iaf_psc_exp": 1, "aeif_cond_alpha": 2, "iaf_cond_exp": 3,
-          "iaf_cond_alpha": 4}
+          "iaf_cond_alpha": 4, "iaf_psc_exp_multisynapse": 5}
 LEGACY, RING = 0, 1
 
 

@@ -14,6 +14,11 @@ PopCoef<Real> cast_coef(const PopCoef<double> &d) {
     C_(V_peak) C_(V_reset) C_(g_L) C_(C_m) C_(E_ex) C_(E_in) C_(Delta_T) C_(tau_w) C_(a) C_(b)
     C_(V_th) C_(tau_syn_ex) C_(tau_syn_in) C_(atol) C_(pscon_ex) C_(pscon_in) C_(v_peak_detect)
 #undef C_
+    for (int k = 0; k < 4; ++k) {
+        c.msP11[k] = static_cast<Real>(d.msP11[k]);
+        c.msP21[k] = static_cast<Real>(d.msP21[k]);
+    }
+    c.nrec = d.nrec;
     c.ref_count = d.ref_count;
     c.off = d.off;
     c.n = d.n;

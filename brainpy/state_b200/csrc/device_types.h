@@ -26,8 +26,17 @@ __host__ __device__ constexpr bool model_is_cond(int model) { return model >= 2 
 __host__ __device__ constexpr int cond_n_ode(int model) {
     return model == 2 ? 6 : (model == 3 ? 3 : 5);
 }
+// iaf_psc_exp_multisynapse (id 5): V_m, i_const, then one synaptic current
+// per receptor (kMaxReceptors slots whatever the population's count)
+constexpr int kMaxReceptors = 4;
 __host__ __device__ constexpr int model_n_slots(int model) {
-    return model_is_cond(model) ? cond_n_ode(model) + 2 : 6;
+    return model_is_cond(model) ? cond_n_ode(model) + 2 : (model == 5 ? 2 + kMaxReceptors : 6);
+}
+// models stepped by the per-step engine (one launch sequence per step)
+__host__ __device__ constexpr bool model_per_step(int model) { return model >= 2; }
+// input channels of the ring: the receptor ports of the model
+__host__ __device__ constexpr int model_n_receptors(int model) {
+    return model_is_cond(model) ? 2 : (model == 5 ? kMaxReceptors : 1);
 }
 
 constexpr int kMaxPops = 64;
@@ -48,6 +57,10 @@ struct PopCoef {
     // aeif_cond_alpha
     Real V_peak, V_reset, g_L, C_m, E_ex, E_in, Delta_T, tau_w, a, b, V_th, tau_syn_ex,
         tau_syn_in, atol, pscon_ex, pscon_in, v_peak_detect;
+    // iaf_psc_exp_multisynapse: per-receptor decay and membrane coupling
+    // (eP22 / eP20 hold the membrane propagators)
+    Real msP11[4], msP21[4];
+    int nrec;
     int ref_count;
     int off, n;  // gid range of the population
 };

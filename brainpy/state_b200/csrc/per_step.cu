@@ -1,6 +1,7 @@
 // per_step.cu -- per-step engine: the conductance models (aeif_cond_alpha,
-// iaf_cond_exp, iaf_cond_alpha) with adaptive RKF45, and networks with
-// plastic stdp_synapse projections (any neuron model).
+// iaf_cond_exp, iaf_cond_alpha) with adaptive RKF45, iaf_psc_exp_multisynapse
+// (one input channel per receptor), and networks with plastic
+// stdp_synapse / stdp_triplet_synapse projections (any neuron model).
 //
 // One step n is this kernel sequence (the reference Simulator's phase order,
 // _nest_network/simulator.py:1719-1788):
@@ -238,6 +239,36 @@ __device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
     return spiked;
 }
 
+// iaf_psc_exp_multisynapse (_nest_neuron/iaf_psc_exp_multisynapse.py:716-790):
+// exact membrane propagation summing every receptor's current, refractory
+// countdown, receptor decay plus this step's weights, threshold and reset.
+// s: V_m, i_const, i_syn[kMaxReceptors]; w: weight per receptor (pA).
+template <typename Real>
+__device__ __forceinline__ bool iaf_ms_step(const PopCoef<Real> &c, Real *s, int &r,
+                                            const Real *w) {
+    Real v = s[0] - c.E_L;
+    if (r == 0) {
+        Real syn = c.msP21[0] * s[2];
+#pragma unroll
+        for (int k = 1; k < kMaxReceptors; ++k)
+            if (k < c.nrec) syn = syn + c.msP21[k] * s[2 + k];
+        v = v * c.eP22 + (c.I_e + s[1]) * c.eP20 + syn;
+    } else {
+        r = r - 1;
+    }
+#pragma unroll
+    for (int k = 0; k < kMaxReceptors; ++k)
+        if (k < c.nrec) s[2 + k] = s[2 + k] * c.msP11[k] + w[k];
+    const bool spike = v >= c.theta;
+    if (spike) {
+        r = c.ref_count;
+        v = c.vreset;
+    }
+    s[0] = v + c.E_L;
+    s[1] = Real(0);  // no current input on this path: i_const <- 0
+    return spike;
+}
+
 // ------------------------------------------------------------- kernels
 
 template <typename Real, int MODEL>
@@ -248,7 +279,7 @@ __global__ void __launch_bounds__(128) k_neuron_step(const StepArgs<Real> a, dou
     const int p = find_pop_t(a.coef, a.npop, g);
     const PopCoef<Real> c = a.coef[p];
     const int slot = static_cast<int>(n % a.L);
-    Real in[2] = {Real(0), Real(0)};
+    Real in[kMaxReceptors] = {Real(0), Real(0), Real(0), Real(0)};
     for (int ch = 0; ch < a.R; ++ch) {
         Real *cell = a.ring + (static_cast<size_t>(slot) * a.R + ch) * a.N + g;
         in[ch] = *cell;
@@ -284,6 +315,8 @@ __global__ void __launch_bounds__(128) k_neuron_step(const StepArgs<Real> a, dou
         sp = iaf_exp_step<Real>(c, s6, r, in[0]);
 #pragma unroll
         for (int i = 0; i < 6; ++i) st[i] = s6[i];
+    } else if constexpr (MODEL == 5) {
+        sp = iaf_ms_step<Real>(c, st, r, in);
     } else {
         sp = cond_step<Real, MODEL>(c, st, r, in[0], in[1], dt, a.err, a.rk_iters);
     }
@@ -442,7 +475,7 @@ StepArgs<Real> step_args(bspk_plan *p, int64_t *step_ptr) {
     a.nproj = static_cast<int>(p->projs.size());
     a.ndrive = static_cast<int>(p->drives.size());
     a.model = p->cfg.model;
-    a.R = model_is_cond(p->cfg.model) ? 2 : 1;
+    a.R = model_n_receptors(p->cfg.model);
     a.L = p->L;
     a.coef = static_cast<const PopCoef<Real> *>(p->d_coef);
     for (int i = 0; i < 8; ++i) a.s[i] = static_cast<Real *>(p->d_s[i]);
@@ -542,7 +575,8 @@ cudaError_t enqueue_step(bspk_plan *p, const StepArgs<Real> &a, const std::vecto
     else if (a.model == 1) k_neuron_step<Real, 1><<<nb, 128, 0, st>>>(a, dt);
     else if (a.model == 2) k_neuron_step<Real, 2><<<nb, 128, 0, st>>>(a, dt);
     else if (a.model == 3) k_neuron_step<Real, 3><<<nb, 128, 0, st>>>(a, dt);
-    else k_neuron_step<Real, 4><<<nb, 128, 0, st>>>(a, dt);
+    else if (a.model == 4) k_neuron_step<Real, 4><<<nb, 128, 0, st>>>(a, dt);
+    else k_neuron_step<Real, 5><<<nb, 128, 0, st>>>(a, dt);
     k_deliver_static<Real><<<p->sm_count * 4, 256, 0, st>>>(a);
     k_step_end<<<1, 32, 0, st>>>(a.step_ptr);
     return cudaGetLastError();

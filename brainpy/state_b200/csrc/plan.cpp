@@ -72,12 +72,13 @@ int upload_vec(bspk_plan *p, T **ptr, const std::vector<T> &v) {
     return BSPK_OK;
 }
 
-const char *kStateNames[5][9] = {
+const char *kStateNames[6][9] = {
     {"V_m", "I_syn_ex", "dI_syn_ex", "I_syn_in", "dI_syn_in", "y0", "", "", ""},
     {"V_m", "i_syn_ex", "i_syn_in", "i_0", "i_1", "", "", "", ""},
     {"V_m", "dg_ex", "g_ex", "dg_in", "g_in", "w", "h", "I_stim", ""},
     {"V_m", "g_ex", "g_in", "h", "I_stim", "", "", "", ""},
     {"V_m", "dg_ex", "g_ex", "dg_in", "g_in", "h", "I_stim", "", ""},
+    {"V_m", "i_const", "i_syn_0", "i_syn_1", "i_syn_2", "i_syn_3", "", "", ""},
 };
 
 int state_slot(int model, const char *name) {
@@ -237,6 +238,40 @@ int make_coef(int model, const std::vector<double> &p, double h, PopCoef<double>
         c->v_peak_detect = c->V_th;
         return BSPK_OK;
     }
+    if (model == BSPK_IAF_PSC_EXP_MULTISYNAPSE) {
+        if (p.size() < 9) return fail(BSPK_ERR_ARG, "too few parameters");
+        const double E_L = p[0], C_m = p[1], tau_m = p[2], t_ref = p[3], V_th = p[4],
+                     V_reset = p[5], I_e = p[6];
+        const int nrec = static_cast<int>(p[7]);
+        if (nrec < 1 || nrec > kMaxReceptors || static_cast<double>(nrec) != p[7])
+            return fail(BSPK_ERR_UNSUPPORTED, "n_receptors must be 1..4");
+        if (p.size() < static_cast<size_t>(8 + nrec)) return fail(BSPK_ERR_ARG, "too few parameters");
+        // validation (iaf_psc_exp_multisynapse.py:463-477)
+        if (!(V_reset < V_th)) return fail(BSPK_ERR_ARG, "Reset potential must be smaller than threshold.");
+        if (!(C_m > 0)) return fail(BSPK_ERR_ARG, "Capacitance must be > 0.");
+        if (!(tau_m > 0)) return fail(BSPK_ERR_ARG, "Membrane time constant must be strictly positive.");
+        for (int k = 0; k < nrec; ++k)
+            if (!(p[8 + k] > 0))
+                return fail(BSPK_ERR_ARG, "All synaptic time constants must be strictly positive.");
+        for (int k = 0; k < nrec; ++k)  // numpy isclose: |a - b| <= 1e-8 + 1e-5 |b|
+            if (std::fabs(p[8 + k] - tau_m) <= 1e-8 + 1e-5 * std::fabs(tau_m))
+                return fail(BSPK_ERR_ARG, "Membrane and synapse time constants must differ.");
+        if (t_ref < 0) return fail(BSPK_ERR_ARG, "Refractory time must not be negative.");
+        // propagators (iaf_psc_exp_multisynapse.py:523-552)
+        c->E_L = E_L;
+        c->I_e = I_e;
+        c->theta = V_th - E_L;
+        c->vreset = V_reset - E_L;
+        c->ref_count = static_cast<int>(std::ceil(t_ref / h));
+        c->eP22 = std::exp(-h / tau_m);
+        c->eP20 = tau_m / C_m * (1.0 - c->eP22);
+        c->nrec = nrec;
+        for (int k = 0; k < nrec; ++k) {
+            c->msP11[k] = std::exp(-h / p[8 + k]);
+            c->msP21[k] = propagator_exp(p[8 + k], tau_m, C_m, h);
+        }
+        return BSPK_OK;
+    }
     return fail(BSPK_ERR_ARG, "unknown model");
 }
 
@@ -279,6 +314,26 @@ std::vector<uint64_t> bspk::host_poisson_thresholds(double lam) {
 
 // =================================================================== C ABI
 
+namespace {
+// Receptor ports: 0 for the iaf_psc models (all inputs summed), 0/1 (g_ex /
+// g_in) for the conductance models, 0..n_receptors-1 of the post population
+// for iaf_psc_exp_multisynapse.
+int check_receptor(const bspk_plan *p, int post_pop, int receptor) {
+    const int model = p->cfg.model;
+    if (model == BSPK_IAF_PSC_EXP_MULTISYNAPSE) {
+        const int n = p->pops[post_pop].c.nrec;
+        if (receptor < 0 || receptor >= n)
+            return fail(BSPK_ERR_ARG, "receptor must be below the population's n_receptors (" +
+                                          std::to_string(n) + ")");
+        return BSPK_OK;
+    }
+    if (receptor < 0 || receptor > 1) return fail(BSPK_ERR_ARG, "receptor must be 0 or 1");
+    if (receptor != 0 && !model_is_cond(model))
+        return fail(BSPK_ERR_ARG, "receptor ports are for conductance models; current models sum all inputs");
+    return BSPK_OK;
+}
+}  // namespace
+
 extern "C" {
 
 const char *bspk_version(void) { return "bspk 0.1 (sm_100a)"; }
@@ -289,11 +344,11 @@ int bspk_plan_create(const bspk_config *cfg, bspk_plan **out) {
     if (!(cfg->dt > 0)) return fail(BSPK_ERR_ARG, "dt must be > 0");
     if (cfg->precision != 32 && cfg->precision != 64)
         return fail(BSPK_ERR_ARG, "precision must be 32 or 64");
-    if (cfg->model < 0 || cfg->model > 4) return fail(BSPK_ERR_ARG, "unknown model");
+    if (cfg->model < 0 || cfg->model > 5) return fail(BSPK_ERR_ARG, "unknown model");
     if (cfg->semantics != BSPK_LEGACY && cfg->semantics != BSPK_RING)
         return fail(BSPK_ERR_ARG, "unknown delivery semantics");
     if (cfg->deterministic && (cfg->precision != 64 || cfg->semantics != BSPK_LEGACY ||
-                               model_is_cond(cfg->model)))
+                               model_per_step(cfg->model)))
         return fail(BSPK_ERR_UNSUPPORTED,
                     "deterministic mode needs precision 64, LEGACY semantics and an iaf model");
     bspk_plan *p = new bspk_plan();
@@ -345,9 +400,8 @@ int bspk_proj_add_csr(bspk_plan *p, int pre_pop, int post_pop, int64_t n_edges,
         return fail(BSPK_ERR_ARG, "population index out of range");
     if (n_edges < 0 || (n_edges > 0 && (!post_local || !w || !delay_steps)) || !indptr)
         return fail(BSPK_ERR_ARG, "bad edge arrays");
-    if (receptor < 0 || receptor > 1) return fail(BSPK_ERR_ARG, "receptor must be 0 or 1");
-    if (receptor != 0 && !model_is_cond(p->cfg.model))
-        return fail(BSPK_ERR_ARG, "receptor ports are for conductance models; current models sum all inputs");
+    const int rc0 = check_receptor(p, post_pop, receptor);
+    if (rc0) return rc0;
     if (static_cast<int>(p->input_kind.size()) >= kMaxInputs) return fail(BSPK_ERR_ARG, "too many inputs");
     const int npre = p->pops[pre_pop].n, npost = p->pops[post_pop].n;
     if (npost >= (1 << kEdgeDelayShift) || npre >= (1 << kEdgeDelayShift))
@@ -416,9 +470,8 @@ int bspk_drive_add_poisson(bspk_plan *p, int post_pop, double rate_hz, double we
     if (post_pop < 0 || post_pop >= static_cast<int>(p->pops.size()))
         return fail(BSPK_ERR_ARG, "population index out of range");
     if (static_cast<int>(p->input_kind.size()) >= kMaxInputs) return fail(BSPK_ERR_ARG, "too many inputs");
-    if (receptor < 0 || receptor > 1) return fail(BSPK_ERR_ARG, "receptor must be 0 or 1");
-    if (receptor != 0 && !model_is_cond(p->cfg.model))
-        return fail(BSPK_ERR_ARG, "receptor ports are for conductance models; current models sum all inputs");
+    const int rc0 = check_receptor(p, post_pop, receptor);
+    if (rc0) return rc0;
     const double lam = rate_hz * p->cfg.dt / 1000.0;
     if (!(lam >= 0) || lam > 700.0) return fail(BSPK_ERR_ARG, "rate*dt/1000 must be in [0, 700]");
     const int lag = lag_of(p, delay_steps);
@@ -760,7 +813,7 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
     p->sm_count = prop.multiProcessorCount;
     const bool dbl = p->cfg.precision == 64;
     const bool exact = p->cfg.deterministic != 0;
-    const bool aeif = model_is_cond(p->cfg.model);  // RKF45 per-step engine
+    const bool aeif = model_per_step(p->cfg.model);  // per-step engine (RKF45, multisynapse)
     bool plastic = false;
     for (auto &J : p->projs) plastic |= J.plastic;
 
@@ -799,10 +852,12 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
                 double v = 0.0;
                 // V_m: E_L for the iaf and AdEx models; the iaf_cond models'
                 // V_initializer is a constant -70 mV (iaf_cond_exp.py:310)
-                if (i == 0) v = (p->cfg.model == BSPK_IAF_COND_EXP || p->cfg.model == BSPK_IAF_COND_ALPHA)
+                if (i == 0) v = (p->cfg.model == BSPK_IAF_COND_EXP || p->cfg.model == BSPK_IAF_COND_ALPHA ||
+                                 p->cfg.model == BSPK_IAF_PSC_EXP_MULTISYNAPSE)
                                     ? -70.0
                                     : P.c.E_L;
-                if (aeif && i == cond_n_ode(p->cfg.model)) v = p->cfg.dt;  // integration_step = dt
+                if (model_is_cond(p->cfg.model) && i == cond_n_ode(p->cfg.model))
+                    v = p->cfg.dt;  // integration_step = dt
                 init[P.off + k] = v;
             }
         if (dbl) {
@@ -813,7 +868,7 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
         }
     }
     // ring: [L][R][N], R = 2 for conductance models
-    const int R = aeif ? 2 : 1;
+    const int R = model_n_receptors(p->cfg.model);
     const size_t ring_bytes = static_cast<size_t>(p->elt) * p->L * R * p->N;
     rc = dalloc_bytes(p, &p->d_ring, ring_bytes);
     if (rc) return rc;
@@ -1068,7 +1123,7 @@ extern "C" int bspk_run(bspk_plan *p, int64_t n_steps, void *stream) {
     BSPK_CUDA(cudaMemsetAsync(p->d_barrier, 0, sizeof(unsigned int), st));
     BSPK_CUDA(cudaEventRecord(p->ev0, st));
     cudaError_t e = cudaSuccess;
-    bool per_step = model_is_cond(p->cfg.model);
+    bool per_step = model_per_step(p->cfg.model);
     for (auto &J : p->projs) per_step |= J.plastic;
     if (p->tiled) BSPK_CUDA(cudaMemsetAsync(p->d_trec, 0, sizeof(long long) * p->grid, st));
     if (per_step) {

@@ -117,6 +117,29 @@ class iaf_cond_exp(_Model):
     conductance = True
 
 
+class iaf_psc_exp_multisynapse(_Model):
+    """NEST iaf_psc_exp_multisynapse: one exponential current per receptor, each
+    with its own tau_syn (_nest_neuron/iaf_psc_exp_multisynapse.py:395-421
+    defaults).  ``receptor_type`` k in 1..len(tau_syn) feeds receptor k; the
+    library holds at most 4 receptors."""
+    model_name = "iaf_psc_exp_multisynapse"
+    order = ("E_L", "C_m", "tau_m", "t_ref", "V_th", "V_reset", "I_e")
+    units = dict(E_L=mV, C_m=pF, tau_m=ms, t_ref=ms, V_th=mV, V_reset=mV, I_e=pA)
+    defaults = dict(E_L=-70.0, C_m=250.0, tau_m=10.0, t_ref=2.0, V_th=-55.0, V_reset=-70.0,
+                    I_e=0.0)
+    v_default = "E_L"
+    v_init_const = -70.0
+
+    @classmethod
+    def resolve(cls, params):
+        params = dict(params or {})
+        tau = np.atleast_1d(np.asarray(mantissa(params.pop("tau_syn", (2.0,)), ms),
+                                       dtype=np.float64))
+        if tau.ndim != 1 or not 1 <= tau.size <= 4:
+            raise NotImplementedError("1 to 4 receptors (tau_syn entries) are supported")
+        return super().resolve(params) + [float(tau.size)] + [float(t) for t in tau]
+
+
 class iaf_cond_alpha(iaf_cond_exp):
     """NEST iaf_cond_alpha with RKF45 (_nest_neuron/iaf_cond_alpha.py:307-329 defaults)."""
     model_name = "iaf_cond_alpha"
@@ -480,6 +503,10 @@ class Simulator:
         if receptor_type is None:
             return 0
         k = int(receptor_type)
+        if self._model is iaf_psc_exp_multisynapse:
+            if k < 1:
+                raise ValueError("receptor_type must be >= 1")
+            return k - 1  # the library checks it against the population's receptors
         if k not in (1, 2):
             raise ValueError("receptor_type must be 1 (excitatory) or 2 (inhibitory)")
         return k - 1
@@ -702,6 +729,8 @@ def pl_state_names(model):
         return ("i_syn_ex", "i_syn_in", "i_0", "i_1", "r")
     if model is iaf_cond_exp:
         return ("g_ex", "g_in", "I_stim", "r")
+    if model is iaf_psc_exp_multisynapse:
+        return ("i_const", "i_syn_0", "i_syn_1", "i_syn_2", "i_syn_3", "r")
     if model is iaf_cond_alpha:
         return ("dg_ex", "g_ex", "dg_in", "g_in", "I_stim", "r")
     return ("dg_ex", "g_ex", "dg_in", "g_in", "w", "I_stim", "r")

@@ -39,15 +39,18 @@ enum {
  * iaf_psc_exp (_nest_neuron/iaf_psc_exp.py:552), aeif_cond_alpha
  * (_nest_neuron/aeif_cond_alpha.py:627), iaf_cond_exp
  * (_nest_neuron/iaf_cond_exp.py:519), iaf_cond_alpha
- * (_nest_neuron/iaf_cond_alpha.py:523).  The last three are conductance
+ * (_nest_neuron/iaf_cond_alpha.py:523), iaf_psc_exp_multisynapse
+ * (_nest_neuron/iaf_psc_exp_multisynapse.py:651).  Models 2-4 are conductance
  * models integrated by adaptive RKF45 with receptor ports 0 (g_ex) and
- * 1 (g_in). */
+ * 1 (g_in); model 5 has up to 4 current receptors (ports 0..n-1), each with
+ * its own exponential synaptic time constant. */
 enum {
     BSPK_IAF_PSC_ALPHA = 0,
     BSPK_IAF_PSC_EXP = 1,
     BSPK_AEIF_COND_ALPHA = 2,
     BSPK_IAF_COND_EXP = 3,
-    BSPK_IAF_COND_ALPHA = 4
+    BSPK_IAF_COND_ALPHA = 4,
+    BSPK_IAF_PSC_EXP_MULTISYNAPSE = 5
 };
 
 /* delivery semantics:
@@ -96,7 +99,9 @@ int bspk_plan_destroy(bspk_plan *plan);
  * aeif_cond_alpha V_peak V_reset t_ref g_L C_m E_ex E_in E_L Delta_T tau_w a b
  * V_th tau_syn_ex tau_syn_in I_e gsl_error_tol; iaf_cond_exp and
  * iaf_cond_alpha E_L C_m t_ref V_th V_reset E_ex E_in g_L tau_syn_ex
- * tau_syn_in I_e gsl_error_tol).  Propagators are computed
+ * tau_syn_in I_e gsl_error_tol; iaf_psc_exp_multisynapse E_L C_m tau_m t_ref
+ * V_th V_reset I_e n_receptors tau_syn[0..n_receptors-1], n_receptors <= 4).
+ * Propagators are computed
  * here in float64.  Replaces Simulator.create (simulator.py:458) and the
  * models' _precompute_propagators (iaf_psc_alpha.py:451-479,
  * iaf_psc_exp.py:492-512). */

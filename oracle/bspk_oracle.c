@@ -213,7 +213,8 @@ double bo_propagator_exp(double tau_syn, double tau_m, double c_m, double h) {
 
 /* ------------------------------------------------------------- simulator */
 
-#define NS 9 /* state slots per neuron */
+#define NS 9  /* state slots per neuron */
+#define RCH 4 /* input channels (receptor ports) per neuron */
 
 typedef struct {
     int n, off;
@@ -223,6 +224,10 @@ typedef struct {
         P31in, P32in, epsc, ipsc;
     /* iaf_psc_exp coefficients (_nest_neuron/iaf_psc_exp.py:492-512) */
     double eP11ex, eP11in, eP22, eP21ex, eP21in, eP20;
+    /* iaf_psc_exp_multisynapse (_nest_neuron/iaf_psc_exp_multisynapse.py:523-552):
+     * per-receptor decay and membrane coupling (eP22 / eP20 are the membrane's) */
+    double msP11[RCH], msP21[RCH];
+    int nrec;
     int ref_count;
 } pop_t;
 
@@ -268,16 +273,17 @@ struct bo_sim {
     int64_t step;
     int64_t rk_substeps;
     int threads;  /* OpenMP threads of the independent per-neuron phases */
-    double *acc; /* [2][ntot] input accumulator */
+    double *acc; /* [RCH][ntot] input accumulator */
     double *y;   /* [2][ntot] per-projection vector */
 };
 
-static const char *state_names[5][NS] = {
+static const char *state_names[6][NS] = {
     {"V_m", "I_syn_ex", "dI_syn_ex", "I_syn_in", "dI_syn_in", "y0", "", "", ""},
     {"V_m", "i_syn_ex", "i_syn_in", "i_0", "i_1", "", "", "", ""},
     {"V_m", "dg_ex", "g_ex", "dg_in", "g_in", "w", "h", "I_stim", ""},
     {"V_m", "g_ex", "g_in", "h", "I_stim", "", "", "", ""},
     {"V_m", "dg_ex", "g_ex", "dg_in", "g_in", "h", "I_stim", "", ""},
+    {"V_m", "i_const", "i_syn_0", "i_syn_1", "i_syn_2", "i_syn_3", "", "", ""},
 };
 
 /* ODE leaves of a conductance model; its slots are the leaves, h, I_stim */
@@ -331,7 +337,9 @@ static void grow_state(bo_sim *s, int old_n, int new_n) {
  * aeif_cond_alpha: V_peak V_reset t_ref g_L C_m E_ex E_in E_L Delta_T tau_w a b
  *                  V_th tau_syn_ex tau_syn_in I_e gsl_error_tol
  * iaf_cond_exp, iaf_cond_alpha: E_L C_m t_ref V_th V_reset E_ex E_in g_L
- *                  tau_syn_ex tau_syn_in I_e gsl_error_tol */
+ *                  tau_syn_ex tau_syn_in I_e gsl_error_tol
+ * iaf_psc_exp_multisynapse: E_L C_m tau_m t_ref V_th V_reset I_e n_receptors
+ *                  tau_syn[0..n_receptors-1] (n_receptors <= 4) */
 int bo_add_pop(bo_sim *s, int n, const double *params, int n_params) {
     if (s->npop >= 64 || n_params > 24 || n < 0) return -1;
     pop_t *P = &s->pops[s->npop];
@@ -364,6 +372,17 @@ int bo_add_pop(bo_sim *s, int n, const double *params, int n_params) {
         P->eP21in = bo_propagator_exp(tin, tau_m, c_m, h);
         P->eP20 = tau_m / c_m * (1.0 - exp(-h / tau_m));
         P->ref_count = (int)ceil(P->p[3] / h);
+    } else if (s->model == BO_IAF_PSC_EXP_MULTISYNAPSE) {
+        double tau_m = P->p[2], c_m = P->p[1];
+        P->nrec = (int)P->p[7];
+        if (P->nrec < 1 || P->nrec > RCH || n_params < 8 + P->nrec) return -1;
+        P->eP22 = exp(-h / tau_m);
+        P->eP20 = tau_m / c_m * (1.0 - P->eP22);
+        for (int k = 0; k < P->nrec; ++k) {
+            P->msP11[k] = exp(-h / P->p[8 + k]);
+            P->msP21[k] = bo_propagator_exp(P->p[8 + k], tau_m, c_m, h);
+        }
+        P->ref_count = (int)ceil(P->p[3] / h);
     } else {
         P->ref_count = (int)ceil(P->p[2] / h);
     }
@@ -374,6 +393,8 @@ int bo_add_pop(bo_sim *s, int n, const double *params, int n_params) {
         if (s->model == BO_AEIF_COND_ALPHA) {
             s->st[0][k] = P->p[7]; /* V_m = E_L */
             s->st[6][k] = h;       /* integration_step = dt (aeif_cond_alpha.py:527) */
+        } else if (s->model == BO_IAF_PSC_EXP_MULTISYNAPSE) {
+            s->st[0][k] = -70.0; /* V_initializer (iaf_psc_exp_multisynapse.py:406) */
         } else if (s->model == BO_IAF_COND_EXP || s->model == BO_IAF_COND_ALPHA) {
             s->st[0][k] = -70.0;                 /* V_initializer (iaf_cond_exp.py:310) */
             s->st[n_ode(s->model)][k] = h;       /* integration_step = dt */
@@ -417,6 +438,7 @@ int bo_add_proj(bo_sim *s, int pre_pop, int post_pop, int64_t n_edges,
     if (s->nin >= 256 || pre_pop < 0 || pre_pop >= s->npop || post_pop < 0 ||
         post_pop >= s->npop)
         return -1;
+    if (receptor < 0 || receptor >= RCH) return -1;
     input_t *in = &s->ins[s->nin];
     memset(in, 0, sizeof(*in));
     in->kind = 0;
@@ -447,6 +469,7 @@ int bo_add_proj(bo_sim *s, int pre_pop, int post_pop, int64_t n_edges,
 int bo_add_drive(bo_sim *s, int post_pop, double rate_hz, double weight, int delay_steps,
                  uint32_t seed, int64_t t_min_step, int64_t t_max_step, int receptor) {
     if (s->nin >= 256 || post_pop < 0 || post_pop >= s->npop) return -1;
+    if (receptor < 0 || receptor >= RCH) return -1;
     input_t *in = &s->ins[s->nin];
     memset(in, 0, sizeof(*in));
     in->kind = 1;
@@ -566,8 +589,8 @@ static void alloc_buffers(bo_sim *s) {
     s->H = maxd + 3;
     s->hist = (unsigned char *)calloc((size_t)s->H * (size_t)s->ntot, 1);
     s->L = maxd + 1;
-    s->ring = (double *)calloc((size_t)2 * (size_t)s->L * (size_t)s->ntot, sizeof(double));
-    s->acc = (double *)calloc((size_t)2 * (size_t)s->ntot, sizeof(double));
+    s->ring = (double *)calloc((size_t)RCH * (size_t)s->L * (size_t)s->ntot, sizeof(double));
+    s->acc = (double *)calloc((size_t)RCH * (size_t)s->ntot, sizeof(double));
     s->y = (double *)calloc((size_t)2 * (size_t)s->ntot, sizeof(double));
 }
 
@@ -727,6 +750,34 @@ static int step_iaf_exp(bo_sim *s, pop_t *P, int g, double w_all, double x_next)
     s->st[2][g] = iin;
     s->st[3][g] = x_next;
     s->st[4][g] = 0.0;
+    s->ref[g] = r;
+    return spike;
+}
+
+/* _nest_neuron/iaf_psc_exp_multisynapse.py:716-790: exact membrane step with
+ * every receptor's current summed in receptor order, refractory countdown,
+ * receptor decay plus this step's weights, threshold and reset.  Slots:
+ * V_m, i_const, i_syn_0..3. */
+static int step_iaf_ms(bo_sim *s, pop_t *P, int g, const double *w, double x_next) {
+    double E_L = P->p[0], I_e = P->p[6];
+    double V_rel = s->st[0][g] - E_L, i_const = s->st[1][g];
+    double theta = P->p[4] - E_L, V_reset_rel = P->p[5] - E_L;
+    int r = s->ref[g];
+    if (r == 0) {
+        double syn = P->msP21[0] * s->st[2][g];
+        for (int k = 1; k < P->nrec; ++k) syn = syn + P->msP21[k] * s->st[2 + k][g];
+        V_rel = V_rel * P->eP22 + (I_e + i_const) * P->eP20 + syn;
+    } else {
+        r = r - 1;
+    }
+    for (int k = 0; k < P->nrec; ++k) s->st[2 + k][g] = s->st[2 + k][g] * P->msP11[k] + w[k];
+    int spike = V_rel >= theta;
+    if (spike) {
+        r = P->ref_count;
+        V_rel = V_reset_rel;
+    }
+    s->st[0][g] = V_rel + E_L;
+    s->st[1][g] = x_next;
     s->ref[g] = r;
     return spike;
 }
@@ -925,6 +976,13 @@ static int step_cond(bo_sim *s, pop_t *P, int g, double w_ex, double w_in, doubl
  * w0 = summed delta input (current models) or the excitatory conductance
  * jump (aeif), w1 = inhibitory conductance jump (aeif only), x_next =
  * current input buffered for the next step. */
+int bo_step_neuron_ms(bo_sim *s, int gid, const double *w, double x_next) {
+    if (gid < 0 || gid >= s->ntot || s->model != BO_IAF_PSC_EXP_MULTISYNAPSE) return -1;
+    int p = 0;
+    while (p + 1 < s->npop && s->pops[p + 1].off <= gid) ++p;
+    return step_iaf_ms(s, &s->pops[p], gid, w, x_next);
+}
+
 int bo_step_neuron(bo_sim *s, int gid, double w0, double w1, double x_next) {
     if (gid < 0 || gid >= s->ntot) return -1;
     int p = 0;
@@ -948,25 +1006,25 @@ int64_t bo_run(bo_sim *s, int64_t n_steps, int64_t *spk_step, int32_t *spk_gid,
         double *acc0 = s->acc, *acc1 = s->acc + N;
         if (s->sem == BO_LEGACY) {
             /* phase 1: every input's contribution, summed in creation order
-             * (simulator.py:1728-1731, _base.py:312-382) */
-            for (int g = 0; g < N; ++g) acc0[g] = acc1[g] = 0.0;
+             * (simulator.py:1728-1731, _base.py:312-382), per receptor port */
+            for (size_t q = 0; q < (size_t)RCH * (size_t)N; ++q) s->acc[q] = 0.0;
             for (int i = 0; i < s->nin; ++i) {
                 input_t *in = &s->ins[i];
                 pop_t *Q = &s->pops[in->post_pop];
                 legacy_input(s, in, n, s->y);
-                double *acc = in->receptor == 1 ? acc1 : acc0;
+                double *acc = s->acc + (size_t)in->receptor * (size_t)N;
                 for (int t = 0; t < Q->n; ++t) acc[Q->off + t] = acc[Q->off + t] + s->y[t];
             }
         } else {
             /* PostRing.take: read slot n mod L and clear it (delays.py:291-306) */
             size_t slot = (size_t)(n % s->L);
-            double *r0 = s->ring + slot * (size_t)N;
-            double *r1 = s->ring + ((size_t)s->L + slot) * (size_t)N;
-            for (int g = 0; g < N; ++g) {
-                acc0[g] = r0[g];
-                acc1[g] = r1[g];
-                r0[g] = 0.0;
-                r1[g] = 0.0;
+            for (int c = 0; c < RCH; ++c) {
+                double *rc = s->ring + ((size_t)c * (size_t)s->L + slot) * (size_t)N;
+                double *ac = s->acc + (size_t)c * (size_t)N;
+                for (int g = 0; g < N; ++g) {
+                    ac[g] = rc[g];
+                    rc[g] = 0.0;
+                }
             }
         }
         /* phase 2: neurons (NEST order inside each model), independent per
@@ -980,7 +1038,11 @@ int64_t bo_run(bo_sim *s, int64_t n_steps, int64_t *spk_step, int32_t *spk_gid,
                 int g = P->off + k, sp;
                 if (s->model == BO_IAF_PSC_ALPHA) sp = step_iaf_alpha(s, P, g, acc0[g], 0.0);
                 else if (s->model == BO_IAF_PSC_EXP) sp = step_iaf_exp(s, P, g, acc0[g], 0.0);
-                else sp = step_cond(s, P, g, acc0[g], acc1[g], 0.0, &uns);
+                else if (s->model == BO_IAF_PSC_EXP_MULTISYNAPSE) {
+                    double w[RCH];
+                    for (int c = 0; c < RCH; ++c) w[c] = s->acc[(size_t)c * (size_t)N + (size_t)g];
+                    sp = step_iaf_ms(s, P, g, w, 0.0);
+                } else sp = step_cond(s, P, g, acc0[g], acc1[g], 0.0, &uns);
                 hrow[g] = (unsigned char)sp;
             }
             unstable |= uns;
@@ -1001,7 +1063,7 @@ int64_t bo_run(bo_sim *s, int64_t n_steps, int64_t *spk_step, int32_t *spk_gid,
             for (int i = 0; i < s->nin; ++i) {
                 input_t *in = &s->ins[i];
                 pop_t *Q = &s->pops[in->post_pop];
-                double *rb = s->ring + (size_t)(in->receptor == 1 ? s->L : 0) * (size_t)N;
+                double *rb = s->ring + (size_t)in->receptor * (size_t)s->L * (size_t)N;
                 if (in->kind == 1) {
                     size_t slot = (size_t)((n + in->ddelay) % s->L);
 #pragma omp parallel for num_threads(s->threads > 0 ? s->threads : 1) schedule(static)

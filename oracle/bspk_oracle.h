@@ -29,7 +29,8 @@ enum {
     BO_IAF_PSC_EXP = 1,
     BO_AEIF_COND_ALPHA = 2,
     BO_IAF_COND_EXP = 3,
-    BO_IAF_COND_ALPHA = 4
+    BO_IAF_COND_ALPHA = 4,
+    BO_IAF_PSC_EXP_MULTISYNAPSE = 5
 };
 
 /* delivery semantics
@@ -99,6 +100,9 @@ int bo_record_v(bo_sim *s, int n, const int32_t *gids);
 int64_t bo_run(bo_sim *s, int64_t n_steps, int64_t *spk_step, int32_t *spk_gid,
                int64_t cap, double *v_out);
 int bo_step_neuron(bo_sim *s, int gid, double w0, double w1, double x_next);
+/* One iaf_psc_exp_multisynapse update of gid with one weight per receptor
+ * (w[0..3], pA) and the current buffered for the next step. */
+int bo_step_neuron_ms(bo_sim *s, int gid, const double *w, double x_next);
 int64_t bo_step_count(bo_sim *s);
 int bo_n_total(bo_sim *s);
 int64_t bo_rk_substeps(bo_sim *s);

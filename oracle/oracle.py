@@ -33,7 +33,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 
 MODEL_IDS = {"iaf_psc_alpha": 0, "iaf_psc_exp": 1, "aeif_cond_alpha": 2, "iaf_cond_exp": 3,
-             "iaf_cond_alpha": 4}
+             "iaf_cond_alpha": 4, "iaf_psc_exp_multisynapse": 5}
 LEGACY, RING = 0, 1
 
 
@@ -73,6 +73,7 @@ def lib():
         L.bo_run.restype = i64
         L.bo_run.argtypes = [vp, i64, vp, vp, i64, vp]
         L.bo_step_neuron.argtypes = [vp, C.c_int, dbl, dbl, dbl]
+        L.bo_step_neuron_ms.argtypes = [vp, C.c_int, vp, dbl]
         L.bo_step_count.restype = i64
         L.bo_step_count.argtypes = [vp]
         L.bo_n_total.argtypes = [vp]
@@ -275,6 +276,15 @@ class OracleSim:
         if n > cap:
             raise OverflowError("spike buffer too small")
         return st[:n], gid[:n], v
+
+    def step_neuron_ms(self, gid, w, x_next=0.0):
+        """One iaf_psc_exp_multisynapse update with weight w[k] into receptor k."""
+        wv = np.zeros(4, np.float64)
+        wv[:len(w)] = w
+        r = self._L.bo_step_neuron_ms(self._h, int(gid), _p(wv), float(x_next))
+        if r < 0:
+            raise ValueError("step_neuron_ms failed")
+        return r
 
     def step_neuron(self, gid, w0=0.0, w1=0.0, x_next=0.0):
         r = self._L.bo_step_neuron(self._h, int(gid), float(w0), float(w1), float(x_next))
