@@ -78,6 +78,7 @@ def lib():
             "bspk_stdp_triplet_attach": (C.c_int, [vp, C.c_int, C.POINTER(StdpTripletParams)]),
             "bspk_proj_csr_get": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
             "bspk_record_v": (C.c_int, [vp, C.c_int, vp]),
+            "bspk_debug_withhold_record": (C.c_int, [vp, C.c_int, C.c_int]),
             "bspk_record_spikes_of": (C.c_int, [vp, C.c_int, vp]),
             "bspk_plan_upload": (C.c_int, [vp, vp]),
             "bspk_run": (C.c_int, [vp, i64, vp]),
@@ -237,6 +238,12 @@ class Plan:
         tp = StdpTripletParams(tau_plus, tau_plus_triplet, tau_minus, tau_minus_triplet, Aplus,
                                Aplus_triplet, Aminus, Aminus_triplet, Wmax)
         check(self._L.bspk_stdp_triplet_attach(self._h, proj, C.byref(tp)))
+
+    def debug_withhold_record(self, cta, window):
+        """Test hook: in the next run, tiled-kernel CTA `cta` withholds its
+        record of `window`, so the run's next synchronising call (spikes(),
+        v_trace(), ...) raises TimeoutError after about 2 s."""
+        check(self._L.bspk_debug_withhold_record(self._h, int(cta), int(window)))
 
     def record_v(self, gids):
         g = np.ascontiguousarray(gids, np.int32)

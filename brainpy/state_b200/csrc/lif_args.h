@@ -86,6 +86,9 @@ struct TiledArgs {
     int smem_ptr;   // 1: the tile's CSR bounds are staged in shared memory
     const Real *drive;
     int64_t drive_step0;
+    // test hook: CTA hold_cta does not publish the header of its record of
+    // window hold_win (-1: none), so every bounded wait for it runs out
+    int hold_cta, hold_win;
 };
 
 struct TiledLayout {

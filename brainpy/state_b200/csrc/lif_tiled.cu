@@ -367,18 +367,22 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
                     if (w == 0 && cnt > kRecInline) {  // overflow entries
                         const uint32_t *src =
                             t2.ovf + (static_cast<size_t>(buf) * G + j) * t2.list_cap;
-                        for (int q = 0; q < cnt - kRecInline; ++q) {
+                        bool gave_up = false;
+                        for (int q = 0; q < cnt - kRecInline && !gave_up; ++q) {
                             uint32_t ow = __ldcg(src + q);
                             const uint64_t tq = gtimer();
                             while ((ow & kTagMask) != tag) {
-                                if (gtimer() - tq > kPollLimitNs) {
-                                    atomicExch(a.err, BSPK_DEV_ERR_TIMEOUT);
+                                // give up after the limit, or at once when any
+                                // CTA has already raised the error flag
+                                if (gtimer() - tq > kPollLimitNs || *(volatile int *)a.err != 0) {
+                                    atomicCAS(a.err, 0, BSPK_DEV_ERR_TIMEOUT);
                                     s_abort = 1;
+                                    gave_up = true;
                                     break;
                                 }
                                 ow = __ldcg(src + q);
                             }
-                            push(j, ow);
+                            if (!gave_up) push(j, ow);
                         }
                     }
                     pend &= ~(1u << i);
@@ -483,7 +487,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
         const int nsp = s_nsp[j & 1];
         // the other parity's counter was last read before this barrier
         if (tid == 0) s_nsp[(j + 1) & 1] = 0;
-        if (tid == 0) rec[0] = tag | static_cast<uint32_t>(nsp);
+        if (tid == 0) {
+            if (c != t2.hold_cta || j != t2.hold_win) rec[0] = tag | static_cast<uint32_t>(nsp);
+        }
         else if (tid <= kRecInline && tid - 1 >= nsp) rec[tid] = tag | kPayMask;  // unused slots
 
         // ---- spike record into this CTA's region (holes for unrecorded neurons)

@@ -560,6 +560,17 @@ int bspk_stdp_triplet_attach(bspk_plan *p, int proj_id, const bspk_stdp_triplet_
     return BSPK_OK;
 }
 
+int bspk_debug_withhold_record(bspk_plan *p, int cta, int window) {
+    if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    if (!p->uploaded) return fail(BSPK_ERR_STATE, "plan not uploaded");
+    if (!p->tiled) return fail(BSPK_ERR_UNSUPPORTED, "the record hook needs a plan on the tiled path");
+    if (cta < 0 || cta >= p->grid || window < 0)
+        return fail(BSPK_ERR_ARG, "cta must be in [0, grid) and window >= 0");
+    p->hold_cta = cta;
+    p->hold_win = window;
+    return BSPK_OK;
+}
+
 int bspk_record_v(bspk_plan *p, int n, const int32_t *gids) {
     if (!p || n < 0 || (n > 0 && !gids)) return fail(BSPK_ERR_ARG, "bad record list");
     for (int i = 0; i < n; ++i)
@@ -1083,11 +1094,13 @@ int run_tiled(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
         TiledArgs<Real> t2{p->d_tptr, p->d_tedges, static_cast<const Fix *>(p->d_tw),
                            static_cast<const Fix *>(p->d_twproj), static_cast<Real>(p->tinv_scale),
                            p->d_tlist, p->d_tovf, p->d_trec, p->list_cap, p->smem_ptr ? 1 : 0,
-                           static_cast<const Real *>(p->d_tdrive), a.step0};
+                           static_cast<const Real *>(p->d_tdrive), a.step0,
+                           done == 0 ? p->hold_cta : -1, done == 0 ? p->hold_win : -1};
         e = launch_lif_tiled<Real>(a, t2, p->grid, st);
         if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
         launches += 2;
     }
+    p->hold_cta = p->hold_win = -1;  // the test hook covers one run
     p->last_launches = launches;
     return BSPK_OK;
 }

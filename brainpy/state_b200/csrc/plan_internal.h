@@ -128,6 +128,7 @@ struct bspk_plan {
     long long *d_trec = nullptr;   // per-CTA spike-record counts
     int list_cap = 0;
     bool smem_ptr = false;
+    int hold_cta = -1, hold_win = -1;  // test hook of the next run (tiled path)
     int tW = 1;                    // tiled window (half the smallest lag when pipelined)
     int tpipe = 0;                 // 1: window j - 1 is delivered after window j's update
     void *d_tdrive = nullptr;      // Poisson drive of one launch, [steps][N]

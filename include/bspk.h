@@ -153,6 +153,16 @@ int bspk_stdp_attach(bspk_plan *plan, int proj_id, const bspk_stdp_params *p);
  * of bspk_stdp_attach under another name. */
 int bspk_stdp_triplet_attach(bspk_plan *plan, int proj_id, const bspk_stdp_triplet_params *p);
 
+/* Test hook for failure detection (no counterpart in the reference): in the
+ * next bspk_run of a plan on the tiled path, CTA `cta` does not publish the
+ * header of its spike record of window `window` (windows of the run's first
+ * launch, from 0).  No other CTA can then complete that window: each one's
+ * bounded wait gives up after 2 s, the kernel returns, and the first
+ * synchronising call after the run (bspk_spikes_get, bspk_v_get, ...)
+ * returns BSPK_ERR_TIMEOUT.  The CUDA context stays usable; the plan's state after
+ * such a run is not meaningful.  The hook applies to one run only. */
+int bspk_debug_withhold_record(bspk_plan *plan, int cta, int window);
+
 /* Recording taps (simulator.py:645-662, :1858-1870): V_m of the listed
  * neurons every step; spikes of all neurons (or of the flagged ones). */
 int bspk_record_v(bspk_plan *plan, int n, const int32_t *gids);
