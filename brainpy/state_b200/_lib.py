@@ -79,6 +79,9 @@ def lib():
             "bspk_proj_csr_get": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
             "bspk_record_v": (C.c_int, [vp, C.c_int, vp]),
             "bspk_debug_withhold_record": (C.c_int, [vp, C.c_int, C.c_int]),
+            "bspk_plan_set_ports": (C.c_int, [vp, C.c_int]),
+            "bspk_kernel_fixed_indegree": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
+                                                     vp, vp, vp, vp, vp, C.c_int64, C.c_int, vp]),
             "bspk_record_spikes_of": (C.c_int, [vp, C.c_int, vp]),
             "bspk_plan_upload": (C.c_int, [vp, vp]),
             "bspk_run": (C.c_int, [vp, i64, vp]),
@@ -133,6 +136,27 @@ def lib():
             f.argtypes = args
         _lib = L
     return _lib
+
+
+def kernel_fixed_indegree(seed, proj_id, parts, n_pre, self_pos, K):
+    """Source positions (n_post, K) in the pre view of the kernel front end's
+    fixed_indegree with multapses; parts = [((hi, lo) population name id, local
+    ids), ...] of the post view in order, self_pos = each post neuron's
+    position in the pre view (-1 none) or None."""
+    parts = list(parts)
+    hi = np.array([p[0][0] for p in parts], np.uint32)
+    lo = np.array([p[0][1] for p in parts], np.uint32)
+    ln = np.array([len(p[1]) for p in parts], np.int64)
+    loc = (np.ascontiguousarray(np.concatenate([np.asarray(p[1], np.int64) for p in parts]))
+           if parts else np.zeros(0, np.int64))
+    n_post = int(ln.sum())
+    out = np.zeros(max(n_post * int(K), 1), np.int32)
+    sp = None if self_pos is None else np.ascontiguousarray(self_pos, np.int64)
+    check(lib().bspk_kernel_fixed_indegree(int(seed) & 0xFFFFFFFF, int(proj_id[0]), int(proj_id[1]),
+                                          len(parts), ptr(hi), ptr(lo), ptr(ln), ptr(loc),
+                                          ptr(sp) if sp is not None else None, int(n_pre), int(K),
+                                          ptr(out)))
+    return out[:n_post * int(K)].reshape(n_post, int(K)).astype(np.int64)
 
 
 def check(rc):
@@ -238,6 +262,11 @@ class Plan:
         tp = StdpTripletParams(tau_plus, tau_plus_triplet, tau_minus, tau_minus_triplet, Aplus,
                                Aplus_triplet, Aminus, Aminus_triplet, Wmax)
         check(self._L.bspk_stdp_triplet_attach(self._h, proj, C.byref(tp)))
+
+    def set_ports(self, separate):
+        """iaf models: keep receptor ports 0 ('ex') and 1 ('in_') apart, signs
+        kept (before any input is added)."""
+        check(self._L.bspk_plan_set_ports(self._h, int(bool(separate))))
 
     def debug_withhold_record(self, cta, window):
         """Test hook: in the next run, tiled-kernel CTA `cta` withholds its

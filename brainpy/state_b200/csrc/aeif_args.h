@@ -17,6 +17,7 @@ namespace bspk {
 template <typename Real>
 struct StepArgs {
     int N, npop, nproj, ndrive, model, R, L;
+    int ports;  // iaf models: 1 = receptor ports 0 / 1 kept apart (no sign split)
     const PopCoef<Real> *coef;
     Real *s[8];
     int *r;

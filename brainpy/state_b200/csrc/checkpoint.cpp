@@ -28,7 +28,7 @@ std::vector<Section> sections(bspk_plan *p) {
     const int ns = model_n_slots(p->cfg.model);
     for (int i = 0; i < ns; ++i) s.push_back({p->d_s[i], static_cast<size_t>(p->elt) * p->N});
     s.push_back({p->d_r, sizeof(int) * static_cast<size_t>(p->N)});
-    const int R = model_n_receptors(p->cfg.model);
+    const int R = plan_n_receptors(p);
     s.push_back({p->d_ring, static_cast<size_t>(p->elt) * p->L * R * p->N});
     s.push_back({p->d_hist, sizeof(uint64_t) * static_cast<size_t>(p->N)});
     for (auto &J : p->projs) {

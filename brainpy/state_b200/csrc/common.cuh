@@ -136,11 +136,12 @@ __device__ __forceinline__ bool grid_barrier(unsigned int *counter, unsigned int
 
 // iaf_psc_alpha, NEST order (_nest_neuron/iaf_psc_alpha.py:558-684).
 // s: V, I_ex, dI_ex, I_in, dI_in, y0.  w_all: summed delta input (pA).
+// Two-port form: w_ex / w_in are the jumps of this step's excitatory and
+// inhibitory receptor ports, signs kept (_kernel/models/iaf_psc_alpha.py
+// ports 'ex' / 'in_'); iaf_alpha_step below splits one summed input by sign.
 template <typename Real>
-__device__ __forceinline__ bool iaf_alpha_step(const PopCoef<Real> &c, Real (&s)[6], int &r,
-                                               Real w_all) {
-    const Real w_ex = w_all > Real(0) ? w_all : Real(0);
-    const Real w_in = w_all < Real(0) ? w_all : Real(0);
+__device__ __forceinline__ bool iaf_alpha_step_ports(const PopCoef<Real> &c, Real (&s)[6], int &r,
+                                                     Real w_ex, Real w_in) {
     Real y3 = s[0] - c.E_L;
     if (r == 0) {
         Real v = c.P30 * (s[5] + c.I_e) + c.P31ex * s[2] + c.P32ex * s[1] + c.P31in * s[4] +
@@ -169,12 +170,18 @@ __device__ __forceinline__ bool iaf_alpha_step(const PopCoef<Real> &c, Real (&s)
     s[5] = Real(0);  // no current injector on this path: y0 <- 0
     return spike;
 }
+template <typename Real>
+__device__ __forceinline__ bool iaf_alpha_step(const PopCoef<Real> &c, Real (&s)[6], int &r,
+                                               Real w_all) {
+    return iaf_alpha_step_ports<Real>(c, s, r, w_all > Real(0) ? w_all : Real(0),
+                                      w_all < Real(0) ? w_all : Real(0));
+}
 
 // iaf_psc_exp, deterministic threshold (_nest_neuron/iaf_psc_exp.py:552-682).
 // s: V, i_syn_ex, i_syn_in, i_0, i_1.
 template <typename Real>
-__device__ __forceinline__ bool iaf_exp_step(const PopCoef<Real> &c, Real (&s)[6], int &r,
-                                             Real w_all) {
+__device__ __forceinline__ bool iaf_exp_step_ports(const PopCoef<Real> &c, Real (&s)[6], int &r,
+                                                   Real w_ex, Real w_in) {
     Real V_rel = s[0] - c.E_L;
     if (r == 0) {
         V_rel = V_rel * c.eP22 + s[1] * c.eP21ex + s[2] * c.eP21in + (c.I_e + s[3]) * c.eP20;
@@ -184,8 +191,6 @@ __device__ __forceinline__ bool iaf_exp_step(const PopCoef<Real> &c, Real (&s)[6
     Real iex = s[1] * c.eP11ex;
     Real iin = s[2] * c.eP11in;
     iex = iex + c.one_m_eP11ex * s[4];
-    const Real w_ex = w_all > Real(0) ? w_all : Real(0);
-    const Real w_in = w_all < Real(0) ? w_all : Real(0);
     iex = iex + w_ex;
     iin = iin + w_in;
     const bool spike = V_rel >= c.theta;
@@ -199,6 +204,12 @@ __device__ __forceinline__ bool iaf_exp_step(const PopCoef<Real> &c, Real (&s)[6
     s[3] = Real(0);
     s[4] = Real(0);
     return spike;
+}
+template <typename Real>
+__device__ __forceinline__ bool iaf_exp_step(const PopCoef<Real> &c, Real (&s)[6], int &r,
+                                             Real w_all) {
+    return iaf_exp_step_ports<Real>(c, s, r, w_all > Real(0) ? w_all : Real(0),
+                                    w_all < Real(0) ? w_all : Real(0));
 }
 
 }  // namespace bspk

@@ -305,14 +305,16 @@ __global__ void __launch_bounds__(128) k_neuron_step(const StepArgs<Real> a, dou
         Real s6[6];
 #pragma unroll
         for (int i = 0; i < 6; ++i) s6[i] = st[i];
-        sp = iaf_alpha_step<Real>(c, s6, r, in[0]);
+        sp = a.ports ? iaf_alpha_step_ports<Real>(c, s6, r, in[0], in[1])
+                     : iaf_alpha_step<Real>(c, s6, r, in[0]);
 #pragma unroll
         for (int i = 0; i < 6; ++i) st[i] = s6[i];
     } else if constexpr (MODEL == 1) {
         Real s6[6];
 #pragma unroll
         for (int i = 0; i < 6; ++i) s6[i] = st[i];
-        sp = iaf_exp_step<Real>(c, s6, r, in[0]);
+        sp = a.ports ? iaf_exp_step_ports<Real>(c, s6, r, in[0], in[1])
+                     : iaf_exp_step<Real>(c, s6, r, in[0]);
 #pragma unroll
         for (int i = 0; i < 6; ++i) st[i] = s6[i];
     } else if constexpr (MODEL == 5) {
@@ -475,7 +477,8 @@ StepArgs<Real> step_args(bspk_plan *p, int64_t *step_ptr) {
     a.nproj = static_cast<int>(p->projs.size());
     a.ndrive = static_cast<int>(p->drives.size());
     a.model = p->cfg.model;
-    a.R = model_n_receptors(p->cfg.model);
+    a.ports = p->ports_sep;
+    a.R = plan_n_receptors(p);
     a.L = p->L;
     a.coef = static_cast<const PopCoef<Real> *>(p->d_coef);
     for (int i = 0; i < 8; ++i) a.s[i] = static_cast<Real *>(p->d_s[i]);

@@ -320,6 +320,10 @@ namespace {
 // for iaf_psc_exp_multisynapse.
 int check_receptor(const bspk_plan *p, int post_pop, int receptor) {
     const int model = p->cfg.model;
+    if (p->ports_sep) {
+        if (receptor < 0 || receptor > 1) return fail(BSPK_ERR_ARG, "receptor must be 0 ('ex') or 1 ('in_')");
+        return BSPK_OK;
+    }
     if (model == BSPK_IAF_PSC_EXP_MULTISYNAPSE) {
         const int n = p->pops[post_pop].c.nrec;
         if (receptor < 0 || receptor >= n)
@@ -557,6 +561,72 @@ int bspk_stdp_triplet_attach(bspk_plan *p, int proj_id, const bspk_stdp_triplet_
     J.homogeneous = false;
     J.rule = 1;
     J.trip = *tp;
+    return BSPK_OK;
+}
+
+int bspk_kernel_fixed_indegree(uint32_t seed, uint32_t proj_hi, uint32_t proj_lo, int n_parts,
+                               const uint32_t *part_hi, const uint32_t *part_lo,
+                               const int64_t *part_len, const int64_t *post_local,
+                               const int64_t *self_pos, int64_t n_pre, int K, int32_t *src_pos) {
+    if (n_parts < 0 || K < 0 || n_pre < 0 || (n_parts > 0 && (!part_hi || !part_lo || !part_len)))
+        return fail(BSPK_ERR_ARG, "bad arguments");
+    int64_t n_post = 0;
+    for (int q = 0; q < n_parts; ++q) {
+        if (part_len[q] < 0) return fail(BSPK_ERR_ARG, "negative part length");
+        n_post += part_len[q];
+    }
+    if (n_post == 0 || K == 0) return BSPK_OK;
+    if (!post_local || !src_pos) return fail(BSPK_ERR_ARG, "null arrays");
+    for (int64_t j = 0; j < n_post; ++j) {
+        if (post_local[j] < 0 || (post_local[j] >> 10) > 0xFFFFFFFFll)
+            return fail(BSPK_ERR_ARG, "post ids must be non-negative and their blocks < 2^32");
+        const int64_t sp = self_pos ? self_pos[j] : -1;
+        if (sp >= n_pre) return fail(BSPK_ERR_ARG, "self position outside the pre view");
+        if (n_pre - (sp >= 0 ? 1 : 0) <= 0)
+            return fail(BSPK_ERR_ARG, "fixed_indegree: a target has no available source");
+    }
+    // object key: fold_in(fold_in(PRNGKey(seed), hi), lo) of the projection name
+    const JaxKey obj = jax_fold(jax_fold(jax_key(static_cast<int64_t>(seed)), proj_hi), proj_lo);
+    std::vector<int64_t> first(n_parts + 1, 0);
+    for (int q = 0; q < n_parts; ++q) first[q + 1] = first[q] + part_len[q];
+    unsigned nth = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    if (n_post * K < 200000) nth = 1;
+    std::vector<std::thread> ts;
+    for (unsigned t = 0; t < nth; ++t) {
+        ts.emplace_back([=, &first]() {
+            std::vector<int64_t> idx(K);
+            for (int q = 0; q < n_parts; ++q) {
+                const JaxKey pk = jax_fold(jax_fold(obj, part_hi[q]), part_lo[q]);
+                for (int64_t j = first[q] + t; j < first[q + 1]; j += nth) {
+                    const uint64_t l = static_cast<uint64_t>(post_local[j]);
+                    const JaxKey kj = jax_fold(jax_fold(jax_fold(pk, static_cast<uint32_t>(l >> 10)),
+                                                        0xFFFFFFFFu),
+                                               static_cast<uint32_t>(l & 1023u));
+                    const int64_t sp = self_pos ? self_pos[j] : -1;
+                    const uint64_t avail = static_cast<uint64_t>(n_pre - (sp >= 0 ? 1 : 0));
+                    jax_randint_span(kj, K, avail, 32, idx.data());
+                    for (int k = 0; k < K; ++k) {
+                        int64_t c = idx[k];
+                        if (sp >= 0 && c >= sp) c += 1;  // skip the post neuron itself
+                        src_pos[j * K + k] = static_cast<int32_t>(c);
+                    }
+                }
+            }
+        });
+    }
+    for (auto &th : ts) th.join();
+    return BSPK_OK;
+}
+
+int bspk_plan_set_ports(bspk_plan *p, int separate) {
+    if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    if (p->uploaded || !p->input_kind.empty())
+        return fail(BSPK_ERR_STATE, "set the ports before adding inputs");
+    if (separate && p->cfg.model != BSPK_IAF_PSC_ALPHA && p->cfg.model != BSPK_IAF_PSC_EXP)
+        return fail(BSPK_ERR_UNSUPPORTED, "separate ports are for the iaf_psc models");
+    if (separate && p->cfg.deterministic)
+        return fail(BSPK_ERR_UNSUPPORTED, "separate ports are not available in deterministic mode");
+    p->ports_sep = separate ? 1 : 0;
     return BSPK_OK;
 }
 
@@ -824,7 +894,7 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
     p->sm_count = prop.multiProcessorCount;
     const bool dbl = p->cfg.precision == 64;
     const bool exact = p->cfg.deterministic != 0;
-    const bool aeif = model_per_step(p->cfg.model);  // per-step engine (RKF45, multisynapse)
+    const bool aeif = plan_per_step(p);  // per-step engine (RKF45, multisynapse, ports)
     bool plastic = false;
     for (auto &J : p->projs) plastic |= J.plastic;
 
@@ -879,7 +949,7 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
         }
     }
     // ring: [L][R][N], R = 2 for conductance models
-    const int R = model_n_receptors(p->cfg.model);
+    const int R = plan_n_receptors(p);
     const size_t ring_bytes = static_cast<size_t>(p->elt) * p->L * R * p->N;
     rc = dalloc_bytes(p, &p->d_ring, ring_bytes);
     if (rc) return rc;
@@ -1136,7 +1206,7 @@ extern "C" int bspk_run(bspk_plan *p, int64_t n_steps, void *stream) {
     BSPK_CUDA(cudaMemsetAsync(p->d_barrier, 0, sizeof(unsigned int), st));
     BSPK_CUDA(cudaEventRecord(p->ev0, st));
     cudaError_t e = cudaSuccess;
-    bool per_step = model_per_step(p->cfg.model);
+    bool per_step = plan_per_step(p);
     for (auto &J : p->projs) per_step |= J.plastic;
     if (p->tiled) BSPK_CUDA(cudaMemsetAsync(p->d_trec, 0, sizeof(long long) * p->grid, st));
     if (per_step) {

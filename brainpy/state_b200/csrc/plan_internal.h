@@ -129,6 +129,9 @@ struct bspk_plan {
     int list_cap = 0;
     bool smem_ptr = false;
     int hold_cta = -1, hold_win = -1;  // test hook of the next run (tiled path)
+    // iaf models with receptor ports kept apart (0 = 'ex', 1 = 'in_', signs
+    // kept), stepped by the per-step engine; 0 = one summed input split by sign
+    int ports_sep = 0;
     int tW = 1;                    // tiled window (half the smallest lag when pipelined)
     int tpipe = 0;                 // 1: window j - 1 is delivered after window j's update
     void *d_tdrive = nullptr;      // Poisson drive of one launch, [steps][N]
@@ -147,4 +150,12 @@ int dalloc_bytes(bspk_plan *p, void **ptr, size_t bytes);
 int host_make_coef(int model, const std::vector<double> &params, double h, PopCoef<double> *c);
 std::vector<uint64_t> host_poisson_thresholds(double lam);
 int sync_and_check(bspk_plan *p);
+// Input channels of the plan's ring (receptor ports) and whether the
+// per-step engine steps it.
+inline int plan_n_receptors(const bspk_plan *p) {
+    return p->ports_sep ? 2 : model_n_receptors(p->cfg.model);
+}
+inline bool plan_per_step(const bspk_plan *p) {
+    return model_per_step(p->cfg.model) || p->ports_sep != 0;
+}
 }  // namespace bspk

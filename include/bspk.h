@@ -153,6 +153,30 @@ int bspk_stdp_attach(bspk_plan *plan, int proj_id, const bspk_stdp_params *p);
  * of bspk_stdp_attach under another name. */
 int bspk_stdp_triplet_attach(bspk_plan *plan, int proj_id, const bspk_stdp_triplet_params *p);
 
+/* fixed_indegree with multapses as the kernel front end draws it
+ * (_kernel/connectivity/rules.py:226-265, keys of _kernel/rng.py:106-300):
+ * for post neuron j of part q of the post view (population name id
+ * (part_hi[q], part_lo[q]), local id l = post_local[j]),
+ *   key_j = fold(fold(fold(fold(fold(obj, hi_q), lo_q), l / 1024), 2^32 - 1), l % 1024),
+ *   obj   = fold(fold(PRNGKey(seed), proj_hi), proj_lo)  (the projection name's id),
+ * and its K sources are randint(key_j, (K,), 0, n_pre - has_self) with 32-bit
+ * draws, shifted past self_pos[j] (its own position in the pre view, -1 or
+ * NULL for none, which excludes autapses).  src_pos[j * K + k] are positions
+ * in the pre view.  Host code, no GPU. */
+int bspk_kernel_fixed_indegree(uint32_t seed, uint32_t proj_hi, uint32_t proj_lo, int n_parts,
+                               const uint32_t *part_hi, const uint32_t *part_lo,
+                               const int64_t *part_len, const int64_t *post_local,
+                               const int64_t *self_pos, int64_t n_pre, int K, int32_t *src_pos);
+
+/* Receptor ports of the iaf_psc models.  0 (default): every input is summed
+ * and the sum split by sign into the excitatory and inhibitory currents, as
+ * the Simulator does (_base.py:312-382, iaf_psc_alpha.py:617-619).
+ * 1: port 0 ('ex') and port 1 ('in_') stay apart and keep their weights'
+ * signs, as the kernel models' receptor ports do
+ * (_kernel/models/iaf_psc_alpha.py, iaf_psc_exp.py inputs); such plans run on
+ * the per-step engine.  Call before adding projections or drives. */
+int bspk_plan_set_ports(bspk_plan *plan, int separate);
+
 /* Test hook for failure detection (no counterpart in the reference): in the
  * next bspk_run of a plan on the tiled path, CTA `cta` does not publish the
  * header of its spike record of window `window` (windows of the run's first

@@ -257,6 +257,7 @@ typedef struct {
 struct bo_sim {
     double dt;
     int sem, model;
+    int ports; /* iaf models: 1 = ports 0 ('ex') / 1 ('in_') apart, signs kept */
     int npop, nin, ntot;
     pop_t pops[64];
     input_t ins[256];
@@ -581,6 +582,10 @@ int64_t bo_rk_substeps(bo_sim *s) { return s->rk_substeps; }
  * results do not depend on the thread count. */
 void bo_set_threads(bo_sim *s, int n) { s->threads = n > 0 ? n : 1; }
 
+/* Receptor ports of the iaf models: 0 = one summed input split by sign
+ * (Simulator), 1 = ports 0 / 1 apart with signs kept (kernel models). */
+void bo_set_ports(bo_sim *s, int separate) { s->ports = separate ? 1 : 0; }
+
 static void alloc_buffers(bo_sim *s) {
     if (s->hist) return;
     int maxd = 0;
@@ -679,13 +684,15 @@ static void legacy_input(bo_sim *s, input_t *in, int64_t n, double *y) {
 }
 
 /* _nest_neuron/iaf_psc_alpha.py:558-684 */
-static int step_iaf_alpha(bo_sim *s, pop_t *P, int g, double w_all, double x_next) {
+/* w_ex / w_in: this step's jumps into the excitatory and inhibitory ports;
+ * the summed-input form below splits one input by sign (iaf_psc_alpha.py:617-619),
+ * the kernel models' ports keep them apart (_kernel/models/iaf_psc_alpha.py) */
+static int step_iaf_alpha_ports(bo_sim *s, pop_t *P, int g, double w_ex, double w_in,
+                                double x_next) {
     double V = s->st[0][g], Iex = s->st[1][g], dIex = s->st[2][g], Iin = s->st[3][g],
            dIin = s->st[4][g], y0 = s->st[5][g];
     int r = s->ref[g];
     double E_L = P->p[0], I_e = P->p[8], V_min = P->p[9];
-    double w_ex = w_all > 0.0 ? w_all : 0.0;
-    double w_in = w_all < 0.0 ? w_all : 0.0;
     double y3 = V - E_L;
     double theta = P->p[4] - E_L;
     double v_reset = P->p[5] - E_L;
@@ -720,7 +727,8 @@ static int step_iaf_alpha(bo_sim *s, pop_t *P, int g, double w_all, double x_nex
 }
 
 /* _nest_neuron/iaf_psc_exp.py:552-682 (deterministic threshold branch) */
-static int step_iaf_exp(bo_sim *s, pop_t *P, int g, double w_all, double x_next) {
+static int step_iaf_exp_ports(bo_sim *s, pop_t *P, int g, double w_ex, double w_in,
+                              double x_next) {
     double V = s->st[0][g], iex = s->st[1][g], iin = s->st[2][g], i0 = s->st[3][g],
            i1 = s->st[4][g];
     int r = s->ref[g];
@@ -736,8 +744,6 @@ static int step_iaf_exp(bo_sim *s, pop_t *P, int g, double w_all, double x_next)
     iex = iex * P->eP11ex;
     iin = iin * P->eP11in;
     iex = iex + (1.0 - P->eP11ex) * i1;
-    double w_ex = w_all > 0.0 ? w_all : 0.0;
-    double w_in = w_all < 0.0 ? w_all : 0.0;
     iex = iex + w_ex;
     iin = iin + w_in;
     int spike = V_rel >= theta;
@@ -752,6 +758,15 @@ static int step_iaf_exp(bo_sim *s, pop_t *P, int g, double w_all, double x_next)
     s->st[4][g] = 0.0;
     s->ref[g] = r;
     return spike;
+}
+
+static int step_iaf_alpha(bo_sim *s, pop_t *P, int g, double w_all, double x_next) {
+    return step_iaf_alpha_ports(s, P, g, w_all > 0.0 ? w_all : 0.0, w_all < 0.0 ? w_all : 0.0,
+                                x_next);
+}
+static int step_iaf_exp(bo_sim *s, pop_t *P, int g, double w_all, double x_next) {
+    return step_iaf_exp_ports(s, P, g, w_all > 0.0 ? w_all : 0.0, w_all < 0.0 ? w_all : 0.0,
+                              x_next);
 }
 
 /* _nest_neuron/iaf_psc_exp_multisynapse.py:716-790: exact membrane step with
@@ -1036,7 +1051,11 @@ int64_t bo_run(bo_sim *s, int64_t n_steps, int64_t *spk_step, int32_t *spk_gid,
 #pragma omp parallel for num_threads(s->threads > 0 ? s->threads : 1) schedule(static) reduction(| : uns)
             for (int k = 0; k < P->n; ++k) {
                 int g = P->off + k, sp;
-                if (s->model == BO_IAF_PSC_ALPHA) sp = step_iaf_alpha(s, P, g, acc0[g], 0.0);
+                if (s->model == BO_IAF_PSC_ALPHA && s->ports)
+                    sp = step_iaf_alpha_ports(s, P, g, acc0[g], acc1[g], 0.0);
+                else if (s->model == BO_IAF_PSC_EXP && s->ports)
+                    sp = step_iaf_exp_ports(s, P, g, acc0[g], acc1[g], 0.0);
+                else if (s->model == BO_IAF_PSC_ALPHA) sp = step_iaf_alpha(s, P, g, acc0[g], 0.0);
                 else if (s->model == BO_IAF_PSC_EXP) sp = step_iaf_exp(s, P, g, acc0[g], 0.0);
                 else if (s->model == BO_IAF_PSC_EXP_MULTISYNAPSE) {
                     double w[RCH];

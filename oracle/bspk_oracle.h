@@ -107,6 +107,7 @@ int64_t bo_step_count(bo_sim *s);
 int bo_n_total(bo_sim *s);
 int64_t bo_rk_substeps(bo_sim *s);
 void bo_set_threads(bo_sim *s, int n);
+void bo_set_ports(bo_sim *s, int separate);
 
 /* Surrogate-gradient BPTT through a recurrent iaf_psc_exp network
  * (bspk_oracle_bptt.c).  W is given row-major over post neurons:

@@ -74,6 +74,7 @@ def lib():
         L.bo_run.argtypes = [vp, i64, vp, vp, i64, vp]
         L.bo_step_neuron.argtypes = [vp, C.c_int, dbl, dbl, dbl]
         L.bo_step_neuron_ms.argtypes = [vp, C.c_int, vp, dbl]
+        L.bo_set_ports.argtypes = [vp, C.c_int]
         L.bo_step_count.restype = i64
         L.bo_step_count.argtypes = [vp]
         L.bo_n_total.argtypes = [vp]
@@ -139,6 +140,41 @@ def jax_randint(key, n, minval, maxval, nbits=32):
     out = np.zeros(n, np.int64)
     lib().bo_jax_randint(_p(k), int(n), int(minval), int(maxval), int(nbits), _p(out))
     return out
+
+
+def name_id(name):
+    """(hi, lo) words of the first 8 bytes of blake2b(name) (_kernel/rng.py:122-150)."""
+    import hashlib
+    d = hashlib.blake2b(name.encode("utf-8"), digest_size=8).digest()
+    return int.from_bytes(d[:4], "big"), int.from_bytes(d[4:], "big")
+
+
+def kernel_fixed_indegree(seed, proj_name, parts, n_pre, self_pos, K):
+    """Kernel-front-end fixed_indegree with multapses, one key per post neuron:
+    object key fold(fold(PRNGKey(seed), hi), lo) of the projection name
+    (_kernel/rng.py:152-175), then per part (population name, local ids)
+    fold(fold(obj, hi_q), lo_q) and per local id l
+    fold(fold(fold(., l // 1024), 0xFFFFFFFF), l % 1024) (rng.py:237-300);
+    sources randint(key, (K,), 0, n_pre - has_self) shifted past the post's own
+    position (_kernel/connectivity/rules.py:226-265).  Returns positions in the
+    pre view, shape (n_post, K)."""
+    hi, lo = name_id(proj_name)
+    obj = jax_fold_in(jax_fold_in(jax_key(seed), hi), lo)
+    rows = []
+    j = 0
+    for pop_name, local in parts:
+        qh, ql = name_id(pop_name)
+        pk = jax_fold_in(jax_fold_in(obj, qh), ql)
+        for l in np.asarray(local, np.int64):
+            kj = jax_fold_in(jax_fold_in(jax_fold_in(pk, int(l) // 1024), 0xFFFFFFFF),
+                             int(l) % 1024)
+            sp = int(self_pos[j]) if self_pos is not None else -1
+            idx = jax_randint(kj, K, 0, n_pre - (1 if sp >= 0 else 0))
+            if sp >= 0:
+                idx = idx + (idx >= sp)
+            rows.append(idx)
+            j += 1
+    return np.array(rows, np.int64).reshape(-1, K)
 
 
 def fixed_indegree(seed, n_pre, n_post, K, pre_is_post=False, allow_autapses=True, nbits=32):
@@ -276,6 +312,10 @@ class OracleSim:
         if n > cap:
             raise OverflowError("spike buffer too small")
         return st[:n], gid[:n], v
+
+    def set_ports(self, separate):
+        """iaf models: receptor ports 0 / 1 kept apart (signs kept)."""
+        self._L.bo_set_ports(self._h, int(bool(separate)))
 
     def step_neuron_ms(self, gid, w, x_next=0.0):
         """One iaf_psc_exp_multisynapse update with weight w[k] into receptor k."""
