@@ -239,6 +239,7 @@ typedef struct {
     int32_t *post, *delay;
     double *w;
     int max_delay;
+    int hdelay; /* the one delay of every edge, or -1 when they differ */
     /* drive */
     double rate, weight, lam, enl;
     int ddelay;
@@ -455,6 +456,7 @@ int bo_add_proj(bo_sim *s, int pre_pop, int post_pop, int64_t n_edges,
     in->delay = (int32_t *)malloc(sizeof(int32_t) * ne);
     in->w = (double *)malloc(sizeof(double) * ne);
     int maxd = 0;
+    in->hdelay = n_edges > 0 ? delay_steps[0] : -1;
     for (int64_t e = 0; e < n_edges; ++e) {
         if (post_local[e] < 0 || post_local[e] >= s->pops[post_pop].n) return -2;
         if (delay_steps[e] < (s->sem == BO_RING ? 1 : 0)) return -3;
@@ -462,6 +464,7 @@ int bo_add_proj(bo_sim *s, int pre_pop, int post_pop, int64_t n_edges,
         in->delay[e] = delay_steps[e];
         in->w[e] = w[e];
         if (delay_steps[e] > maxd) maxd = delay_steps[e];
+        if (delay_steps[e] != in->hdelay) in->hdelay = -1;
     }
     in->max_delay = maxd;
     return s->nin++;
@@ -644,6 +647,15 @@ static void legacy_input(bo_sim *s, input_t *in, int64_t n, double *y) {
     }
     pop_t *P = &s->pops[in->pre_pop];
     if (!in->plastic) {
+        if (in->hdelay >= 0) {
+            /* one delay: test each row once (the same sums in the same order) */
+            for (int i = 0; i < P->n; ++i) {
+                if (!fired(s, n - (in->hdelay + 1), P->off + i)) continue;
+                for (int64_t e = in->indptr[i]; e < in->indptr[i + 1]; ++e)
+                    y[in->post[e]] += in->w[e];
+            }
+            return;
+        }
         for (int i = 0; i < P->n; ++i)
             for (int64_t e = in->indptr[i]; e < in->indptr[i + 1]; ++e)
                 if (fired(s, n - (in->delay[e] + 1), P->off + i)) y[in->post[e]] += in->w[e];

@@ -214,3 +214,35 @@ def test_tiled_split_delivery_across_calls(oracle):
     assert len(st) > 0
     assert _raster(st, g) == _raster(ost, og)
     np.testing.assert_allclose(np.concatenate(vs), ov, rtol=0, atol=1e-9)
+
+
+def test_config0_deterministic_fp64_reproduces_oracle_bitwise(oracle):
+    """The first configuration at full size: Brunel order 500 (2000 E + 500 I,
+    CE = 200, CI = 50, 625 k edges), homogeneous 1.5 ms delay with the
+    Simulator's timing, 500 ms = 5000 steps, deterministic FP64 pull
+    delivery.  Spike trains and V_m traces must equal the float64 oracle's
+    bit for bit."""
+    from brainpy.state_b200 import _lib, brunel
+    seed = 1234
+    pl, p = brunel.build_plan(order=500, precision=64, delay_steps=15, noise_delay=15,
+                              seed=seed, semantics=_lib.LEGACY, deterministic=True, rec_v=25)
+    NE, NI = p["NE"], p["NI"]
+    o = oracle.OracleSim(0.1, "iaf_psc_alpha", semantics=oracle.LEGACY)
+    o.add_pop(NE, p["neuron"])
+    o.add_pop(NI, p["neuron"])
+    o.add_drive(0, p["rate"], p["J_ex"], 15, brunel.derive_seed(seed, 0))
+    o.add_drive(1, p["rate"], p["J_ex"], 15, brunel.derive_seed(seed, 1))
+    for j in range(4):
+        indptr, post, d, w = pl.csr(j)
+        o.add_proj(0 if j < 2 else 1, j % 2, indptr, post, w, d)
+    vr = np.random.default_rng(seed + 7)
+    o.set_state(0, "V_m", vr.uniform(0.0, 20.0, NE))
+    o.set_state(1, "V_m", vr.uniform(0.0, 20.0, NI))
+    o.record_v(np.linspace(0, NE + NI - 1, 25).astype(np.int32))
+    pl.run(5000)
+    st, g = pl.spikes()
+    ost, og, ov = o.run(5000)
+    rate = len(ost) / (NE + NI) / 0.5
+    assert 5.0 < rate < 100.0
+    assert _raster(st, g) == _raster(ost, og)
+    np.testing.assert_array_equal(pl.v_trace(), ov)
