@@ -122,6 +122,24 @@ def time_runs(pl, n_runs, stream, flush):
     return times, spikes, events
 
 
+def _cv_isi(steps, gids, min_spikes=3):
+    """Mean over neurons with at least min_spikes spikes of the coefficient of
+    variation of their inter-spike intervals (_kernel/validation/stats.py:44-59)."""
+    import numpy as np
+    if steps.size == 0:
+        return None
+    order = np.lexsort((steps, gids))
+    s, g = steps[order], gids[order]
+    cuts = np.nonzero(np.diff(g))[0] + 1
+    cvs = []
+    for a, b in zip(np.concatenate([[0], cuts]), np.concatenate([cuts, [g.size]])):
+        if b - a >= min_spikes:
+            isi = np.diff(s[a:b]).astype(np.float64)
+            if isi.mean() > 0:
+                cvs.append(isi.std() / isi.mean())
+    return round(float(np.mean(cvs)), 4) if cvs else None
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -157,6 +175,7 @@ def run_ours(args):
     rate_hz = nspk / args.steps / N
     drive_ev_s = world * N * p["rate"] * (sim_ms / 1000.0) / (ms_step / 1000.0)
     kms, launches = pl.kernel_time()
+    cv_isi = _cv_isi(*pl.spikes())  # the last timed launch's spikes (outside the timed region)
 
     # roofline of the persistent kernel: algorithmic bytes per launch
     # (64 B/neuron/time step: 7 FP32 state words read+written and the ring
@@ -189,6 +208,7 @@ def run_ours(args):
                    "parallelism": f"replicas{world}"},
         "syn_events_per_s": round(syn_ev_s, 1), "drive_events_per_s": round(drive_ev_s, 1),
         "rate_hz": round(rate_hz / (sim_ms / 1000.0), 3),
+        "cv_isi": cv_isi,
         "ms_per_time_step": round(ms_step / STEPS_PER_BENCH_STEP, 6),
         "wall_s_timed": round(wall, 4),
         "gpu_launches": int(args.steps) * int(launches),
@@ -207,6 +227,7 @@ def run_ours(args):
         if not args.no_extras:
             result["sweep_batch"] = sweep_numbers(args)
             result["bptt"] = bptt_numbers(args)
+            result["adex_stdp"] = adex_numbers(args)
     if world > 1 and not args.quick and not args.no_extras:
         # every rank takes part (same collectives in the same order on all ranks)
         sw = sweep_sharded(rank, world)
@@ -349,6 +370,28 @@ def sweep_sharded(rank, world):
             "ms_per_simulated_s": round(ms_max, 3),
             "neuron_updates_per_s": round(n_all * steps / (ms_max / 1000.0), 1),
             "scaling": "strong", "collectives": "timing reductions only"}
+
+
+def adex_numbers(args):
+    """The AdEx conductance network with plasticity (16 000 E + 4 000 I
+    aeif_cond_alpha, RKF45 tolerance 1e-6, 40 M lognormal conductance edges of
+    which 25.6 M are plastic E->E stdp_synapse, 5 kHz drive), 2000 ms in FP32
+    through Simulator.simulate, timed on the device (all kernels of the run)."""
+    from brainpy.state_b200 import adex_net
+    from brainpy.state_b200.units import ms
+    t0 = time.perf_counter()
+    sim, h = adex_net.build(scale=1.0, precision=32, n_record=200)
+    res = sim.simulate(2000.0 * ms)
+    wall = time.perf_counter() - t0
+    kms, launches = sim._plan.kernel_time()
+    spk = res.spikes(h["rec"])
+    return {"workload": "16000E+4000I aeif_cond_alpha, in-degree 1600 E + 400 I, lognormal "
+                        "weights (ln 1 nS, 0.5), E->E stdp_synapse (25.6 M edges), 5 kHz drive "
+                        "of 6 nS, RKF45 tol 1e-6, 2000 ms, FP32 stages / FP64 error control",
+            "ms_per_simulated_s": round(kms / 2.0, 2),
+            "rtf": round(2000.0 / kms, 4),
+            "rate_hz_sampled": round(float(spk.sum()) / spk.shape[1] / 2.0, 3),
+            "build_and_run_wall_s": round(wall, 2)}
 
 
 def bptt_numbers(args):

@@ -80,6 +80,7 @@ def lib():
             "bspk_record_v": (C.c_int, [vp, C.c_int, vp]),
             "bspk_debug_withhold_record": (C.c_int, [vp, C.c_int, C.c_int]),
             "bspk_plan_set_ports": (C.c_int, [vp, C.c_int]),
+            "bspk_proj_set_weights": (C.c_int, [vp, C.c_int, C.c_int64, vp]),
             "bspk_kernel_fixed_indegree": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
                                                      vp, vp, vp, vp, vp, C.c_int64, C.c_int, vp]),
             "bspk_record_spikes_of": (C.c_int, [vp, C.c_int, vp]),
@@ -262,6 +263,11 @@ class Plan:
         tp = StdpTripletParams(tau_plus, tau_plus_triplet, tau_minus, tau_minus_triplet, Aplus,
                                Aplus_triplet, Aminus, Aminus_triplet, Wmax)
         check(self._L.bspk_stdp_triplet_attach(self._h, proj, C.byref(tp)))
+
+    def set_weights(self, proj, w):
+        """Per-edge weights of projection `proj` in its CSR order (before upload)."""
+        w = np.ascontiguousarray(w, np.float64)
+        check(self._L.bspk_proj_set_weights(self._h, int(proj), int(w.size), ptr(w)))
 
     def set_ports(self, separate):
         """iaf models: keep receptor ports 0 ('ex') and 1 ('in_') apart, signs

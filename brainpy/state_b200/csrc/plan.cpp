@@ -530,6 +530,19 @@ int plastic_checks(bspk_plan *p, int proj_id) {
 
 extern "C" {
 
+int bspk_proj_set_weights(bspk_plan *p, int proj_id, int64_t n_edges, const double *w) {
+    if (!p || !w) return fail(BSPK_ERR_ARG, "null argument");
+    if (p->uploaded) return fail(BSPK_ERR_STATE, "plan already uploaded");
+    if (proj_id < 0 || proj_id >= static_cast<int>(p->projs.size())) return fail(BSPK_ERR_ARG, "bad projection");
+    Proj &J = p->projs[proj_id];
+    if (n_edges != static_cast<int64_t>(J.post_local.size()))
+        return fail(BSPK_ERR_ARG, "weights must cover every edge of the projection");
+    if (J.plastic) return fail(BSPK_ERR_STATE, "set the weights before making the projection plastic");
+    J.w.assign(w, w + n_edges);
+    J.homogeneous = false;
+    return BSPK_OK;
+}
+
 int bspk_stdp_attach(bspk_plan *p, int proj_id, const bspk_stdp_params *sp) {
     if (!p || !sp) return fail(BSPK_ERR_ARG, "null argument");
     if (!(sp->tau_plus > 0)) return fail(BSPK_ERR_ARG, "'tau_plus' must be > 0.");

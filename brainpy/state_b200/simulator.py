@@ -422,7 +422,7 @@ class Simulator:
         self._model = None
         self._proj_counter = itertools.count()
         self._ops = []            # deferred plan operations in creation order
-        self._spike_taps = {}     # id(recorder) -> (population, indices)
+        self._spike_taps = {}     # id(recorder) -> [(population, indices)], view order
         self._analog_taps = {}    # id(recorder) -> (population, indices, names)
         self._weight_taps = {}
         self._plan = None
@@ -480,8 +480,8 @@ class Simulator:
             return None
         if len(post.segments) == 1 and isinstance(post.segments[0].population, _Device) and \
                 post.segments[0].population.spec.kind == "spike_recorder":
-            seg = pre.segments[0]
-            self._spike_taps[id(post.segments[0].population)] = (seg.population, seg.indices)
+            self._spike_taps[id(post.segments[0].population)] = [(sg.population, sg.indices)
+                                                                 for sg in pre.segments]
             self._plan = None
             return None
         if not allow_multapses:
@@ -539,11 +539,15 @@ class Simulator:
         pseed = self._derive_seed(seed, ordinal)
         rng = np.random.default_rng(pseed)
         receptor = self._receptor(receptor_type)
-        if isinstance(rule, _FixedIndegree) and full_pre and full_post and \
-                not isinstance(weight, (Uniform, Normal, LogNormal)):
+        if isinstance(rule, _FixedIndegree) and full_pre and full_post:
             E = rule.K * dst.n
             dl = self._delays(delay, E, rng)
-            wv = float(mantissa(weight if weight is not None else 1.0, w_unit))
+            if isinstance(weight, (Uniform, Normal, LogNormal)):
+                # edges from the library's sampler, weights drawn per edge in
+                # CSR order from this projection's seeded stream
+                wv = np.asarray(weight.sample(E, rng, w_unit), dtype=np.float64)
+            else:
+                wv = float(mantissa(weight if weight is not None else 1.0, w_unit))
             op = ("fixed_indegree", src.pop_id, dst.pop_id, rule.K, pseed, allow_autapses, wv,
                   dl, receptor, synapse)
             self._ops.append(op)
@@ -615,8 +619,11 @@ class Simulator:
             elif op[0] == "fixed_indegree":
                 _, a, b, K, seed, auto, w, dl, rec, syn = op
                 nbits = 64 if self.precision == 64 else 32
-                j = pl.add_fixed_indegree(a, b, K, seed, w, delay_steps=dl, allow_autapses=auto,
-                                          nbits=nbits, receptor=rec)
+                per_edge = isinstance(w, np.ndarray)
+                j = pl.add_fixed_indegree(a, b, K, seed, 1.0 if per_edge else w, delay_steps=dl,
+                                          allow_autapses=auto, nbits=nbits, receptor=rec)
+                if per_edge:
+                    pl.set_weights(j, w)
                 self._attach(pl, j, syn)
             else:
                 _, a, b, indptr, post, w, dl, rec, syn = op
@@ -633,7 +640,8 @@ class Simulator:
         if gids:
             pl.record_v(np.asarray(gids, np.int32))
         offs = np.cumsum([0] + [q.n for q in self._pops])
-        tapped = [offs[pop.pop_id] + idx for pop, idx in self._spike_taps.values()]
+        tapped = [offs[pop.pop_id] + idx for segs in self._spike_taps.values()
+                  for pop, idx in segs]
         pl.record_spikes_of(np.unique(np.concatenate(tapped)).astype(np.int32) if tapped
                             else np.zeros(0, np.int32))
         pl.upload()
@@ -700,15 +708,15 @@ class Simulator:
         st, gid = pl.spikes()
         spikes, events = {}, {}
         offs = np.cumsum([0] + [p.n for p in self._pops])
-        for rid, (pop, idx) in self._spike_taps.items():
-            lo = offs[pop.pop_id]
-            mat = np.zeros((n, idx.size), np.float32 if self.precision == 32 else np.float64)
-            pos = np.full(pop.n, -1, np.int64)
-            pos[idx] = np.arange(idx.size)
-            sel = (gid >= lo) & (gid < lo + pop.n)
-            col = pos[gid[sel] - lo]
+        for rid, segs in self._spike_taps.items():
+            # columns in view order, across the view's populations
+            cols = np.concatenate([offs[pop.pop_id] + idx for pop, idx in segs])
+            mat = np.zeros((n, cols.size), np.float32 if self.precision == 32 else np.float64)
+            pos = np.full(int(offs[-1]), -1, np.int64)
+            pos[cols] = np.arange(cols.size)
+            col = pos[gid] if gid.size else np.zeros(0, np.int64)
             ok = col >= 0
-            rows = st[sel][ok] - step0
+            rows = st[ok] - step0
             mat[rows, col[ok]] = 1.0
             spikes[rid] = mat
             events[rid] = (rows, col[ok])

@@ -141,6 +141,11 @@ int bspk_drive_add_poisson(bspk_plan *plan, int post_pop, double rate_hz, double
 int bspk_proj_csr_get(bspk_plan *plan, int proj_id, int64_t *indptr, int32_t *post_local,
                       int32_t *delay_steps, double *w);
 
+/* Per-edge weights of a projection, in its CSR order (bspk_proj_csr_get),
+ * before upload: distributed weights on connectivity drawn by the library
+ * (the reference's connect(weight=<Distribution>), connectivity.py:385-405). */
+int bspk_proj_set_weights(bspk_plan *plan, int proj_id, int64_t n_edges, const double *w);
+
 /* Make a CSR projection plastic with the pair STDP rule of
  * _nest_plasticity/stdp_synapse.py:163-179 driven by the eager substrate of
  * _nest_network/event_plastic.py:390-518 (weights kept in FP64). */
