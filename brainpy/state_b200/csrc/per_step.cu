@@ -45,7 +45,7 @@ __device__ __forceinline__ bool fired(const uint64_t *hist, int gid, int64_t m) 
 // ------------------------------------------------ aeif_cond_alpha + RKF45
 
 // RKF45 tableau (_nest_base/utils.py:266-279); b_err = b - b_hat.
-__constant__ double kA[6][5] = {
+__device__ constexpr double kA[6][5] = {
     {0, 0, 0, 0, 0},
     {1.0 / 4, 0, 0, 0, 0},
     {3.0 / 32, 9.0 / 32, 0, 0, 0},
@@ -53,8 +53,8 @@ __constant__ double kA[6][5] = {
     {439.0 / 216, -8.0, 3680.0 / 513, -845.0 / 4104, 0},
     {-8.0 / 27, 2.0, -3544.0 / 2565, 1859.0 / 4104, -11.0 / 40},
 };
-__constant__ double kB[6] = {16.0 / 135, 0.0, 6656.0 / 12825, 28561.0 / 56430, -9.0 / 50, 2.0 / 55};
-__constant__ double kBhat[6] = {25.0 / 216, 0.0, 1408.0 / 2565, 2197.0 / 4104, -1.0 / 5, 0.0};
+__device__ constexpr double kB[6] = {16.0 / 135, 0.0, 6656.0 / 12825, 28561.0 / 56430, -9.0 / 50, 2.0 / 55};
+__device__ constexpr double kBhat[6] = {25.0 / 216, 0.0, 1408.0 / 2565, 2197.0 / 4104, -1.0 / 5, 0.0};
 
 // Vector field (_nest_neuron/aeif_cond_alpha.py:554-592); the exponential
 // spike current is evaluated in FP64 whatever the state precision.
@@ -137,6 +137,7 @@ __device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
         const double hh = h < dt - t_loc ? h : dt - t_loc;
         h = hh > min_h ? hh : min_h;
         const Real hR = static_cast<Real>(h);
+#pragma unroll
         for (int st = 0; st < 6; ++st) {
             Real yi[NS];
             if (st == 0) {
@@ -147,6 +148,7 @@ __device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
                 for (int i = 0; i < NS; ++i) {
                     Real acc = Real(0);
                     bool first = true;
+#pragma unroll
                     for (int j = 0; j < st; ++j) {
                         const double aij = kA[st][j];
                         if (aij == 0.0) continue;
@@ -398,12 +400,18 @@ __global__ void k_stdp_traces(StdpDev s, const uint64_t *hist, const int64_t *st
     }
 }
 
+// x^mu of the soft-bound terms: no pow for the additive rule (mu = 0, the
+// reference kernel's fast path, _kernel/plasticity.py:548-556) or the
+// multiplicative one (mu = 1, where x^1 is x)
+__device__ __forceinline__ double stdp_pow(double x, double mu) {
+    return mu == 1.0 ? x : (mu == 0.0 ? 1.0 : pow(x, mu));
+}
 __device__ __forceinline__ double stdp_facilitate(const StdpDev &s, double w, double kplus) {
-    const double nw = w / s.Wmax + s.lambda_ * pow(1.0 - w / s.Wmax, s.mu_plus) * kplus;
+    const double nw = w / s.Wmax + s.lambda_ * stdp_pow(1.0 - w / s.Wmax, s.mu_plus) * kplus;
     return nw < 1.0 ? nw * s.Wmax : s.Wmax;
 }
 __device__ __forceinline__ double stdp_depress(const StdpDev &s, double w, double kminus) {
-    const double nw = w / s.Wmax - s.alpha * s.lambda_ * pow(w / s.Wmax, s.mu_minus) * kminus;
+    const double nw = w / s.Wmax - s.alpha * s.lambda_ * stdp_pow(w / s.Wmax, s.mu_minus) * kminus;
     return nw > 0.0 ? nw * s.Wmax : 0.0;
 }
 // stdp_triplet_synapse.py:179-197: potentiation reads the fast pre trace r1
