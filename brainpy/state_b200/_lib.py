@@ -88,6 +88,7 @@ def lib():
             "bspk_run": (C.c_int, [vp, i64, vp]),
             "bspk_spikes_get": (C.c_int, [vp, i64, vp, vp, C.POINTER(i64)]),
             "bspk_v_get": (C.c_int, [vp, vp]),
+            "bspk_v_get_f32": (C.c_int, [vp, vp]),
             "bspk_weights_get": (C.c_int, [vp, C.c_int, vp]),
             "bspk_state_get": (C.c_int, [vp, C.c_int, C.c_char_p, vp]),
             "bspk_state_set": (C.c_int, [vp, C.c_int, C.c_char_p, vp]),
@@ -311,9 +312,14 @@ class Plan:
         order = np.lexsort((g[:m], st[:m]))
         return st[:m][order], g[:m][order]
 
-    def v_trace(self):
-        out = np.zeros((self._last_steps, self.n_rec_v), np.float64)
-        check(self._L.bspk_v_get(self._h, ptr(out)))
+    def v_trace(self, dtype=np.float64):
+        """(steps, n_rec) V_m of the last run, float64 or float32."""
+        if np.dtype(dtype) == np.float32:
+            out = np.empty((self._last_steps, self.n_rec_v), np.float32)
+            check(self._L.bspk_v_get_f32(self._h, ptr(out)))
+        else:
+            out = np.empty((self._last_steps, self.n_rec_v), np.float64)
+            check(self._L.bspk_v_get(self._h, ptr(out)))
         return out
 
     def weights(self, proj):

@@ -84,9 +84,16 @@ int bspk_checkpoint_restore(bspk_plan *p, const void *host_buf, int64_t bytes) {
     BSPK_CUDA(cudaSetDevice(p->cfg.device));
     BSPK_CUDA(cudaDeviceSynchronize());
     b += sizeof(hdr);
+    // through the plan's pinned staging buffer: one host copy, then
+    // host-to-device copies at link speed
+    const size_t body = static_cast<size_t>(need) - sizeof(hdr);
+    rc = plan_stage(p, body);
+    if (rc) return rc;
+    memcpy(p->h_stage, b, body);
+    const char *st = static_cast<const char *>(p->h_stage);
     for (auto &s : sections(p)) {
-        BSPK_CUDA(cudaMemcpy(s.ptr, b, s.bytes, cudaMemcpyHostToDevice));
-        b += s.bytes;
+        BSPK_CUDA(cudaMemcpy(s.ptr, st, s.bytes, cudaMemcpyHostToDevice));
+        st += s.bytes;
     }
     p->step = hdr[1];
     return BSPK_OK;

@@ -369,6 +369,7 @@ int bspk_plan_destroy(bspk_plan *p) {
     cudaGetDevice(&dev);
     if (p->uploaded) cudaSetDevice(p->cfg.device);
     for (void *a : p->allocs) cudaFree(a);
+    if (p->h_stage) cudaFreeHost(p->h_stage);
     if (p->ev0) cudaEventDestroy(p->ev0);
     if (p->ev1) cudaEventDestroy(p->ev1);
     cudaSetDevice(dev);
@@ -1247,6 +1248,16 @@ extern "C" int bspk_run(bspk_plan *p, int64_t n_steps, void *stream) {
     return BSPK_OK;
 }
 
+int bspk::plan_stage(bspk_plan *p, size_t bytes) {
+    if (p->h_stage_bytes >= bytes) return BSPK_OK;
+    if (p->h_stage) cudaFreeHost(p->h_stage);
+    p->h_stage = nullptr;
+    p->h_stage_bytes = 0;
+    BSPK_CUDA(cudaMallocHost(&p->h_stage, bytes));
+    p->h_stage_bytes = bytes;
+    return BSPK_OK;
+}
+
 int bspk::sync_and_check(bspk_plan *p) {
     BSPK_CUDA(cudaSetDevice(p->cfg.device));
     BSPK_CUDA(cudaDeviceSynchronize());
@@ -1340,13 +1351,37 @@ int bspk_v_get(bspk_plan *p, double *out) {
     if (rc) return rc;
     const size_t n = static_cast<size_t>(p->last_run_steps) * p->rec_v.size();
     if (n == 0) return BSPK_OK;
+    // the traces come through a pinned staging buffer kept by the plan: a
+    // device-to-pinned copy runs at link speed, a copy into pageable memory
+    // is staged by the driver in small pieces
+    const size_t bytes = static_cast<size_t>(p->elt) * n;
+    rc = plan_stage(p, bytes);
+    if (rc) return rc;
+    BSPK_CUDA(cudaMemcpy(p->h_stage, p->d_v, bytes, cudaMemcpyDeviceToHost));
     if (p->elt == 8) {
-        BSPK_CUDA(cudaMemcpy(out, p->d_v, 8 * n, cudaMemcpyDeviceToHost));
+        memcpy(out, p->h_stage, bytes);
     } else {
-        std::vector<float> f(n);
-        BSPK_CUDA(cudaMemcpy(f.data(), p->d_v, 4 * n, cudaMemcpyDeviceToHost));
+        const float *f = static_cast<const float *>(p->h_stage);
         for (size_t i = 0; i < n; ++i) out[i] = f[i];
     }
+    return BSPK_OK;
+}
+
+int bspk_v_get_f32(bspk_plan *p, float *out) {
+    if (!p || !p->uploaded || !out) return fail(BSPK_ERR_ARG, "bad arguments");
+    int rc = sync_and_check(p);
+    if (rc) return rc;
+    const size_t n = static_cast<size_t>(p->last_run_steps) * p->rec_v.size();
+    if (n == 0) return BSPK_OK;
+    if (p->elt == 4) {  // the traces are float32 on the device: one copy
+        BSPK_CUDA(cudaMemcpy(out, p->d_v, 4 * n, cudaMemcpyDeviceToHost));
+        return BSPK_OK;
+    }
+    rc = plan_stage(p, 8 * n);
+    if (rc) return rc;
+    BSPK_CUDA(cudaMemcpy(p->h_stage, p->d_v, 8 * n, cudaMemcpyDeviceToHost));
+    const double *d = static_cast<const double *>(p->h_stage);
+    for (size_t i = 0; i < n; ++i) out[i] = static_cast<float>(d[i]);
     return BSPK_OK;
 }
 

@@ -129,6 +129,8 @@ struct bspk_plan {
     int list_cap = 0;
     bool smem_ptr = false;
     int hold_cta = -1, hold_win = -1;  // test hook of the next run (tiled path)
+    void *h_stage = nullptr;  // pinned host staging of read-backs (V_m traces), grown on demand
+    size_t h_stage_bytes = 0;
     // iaf models with receptor ports kept apart (0 = 'ex', 1 = 'in_', signs
     // kept), stepped by the per-step engine; 0 = one summed input split by sign
     int ports_sep = 0;
@@ -150,6 +152,8 @@ int dalloc_bytes(bspk_plan *p, void **ptr, size_t bytes);
 int host_make_coef(int model, const std::vector<double> &params, double h, PopCoef<double> *c);
 std::vector<uint64_t> host_poisson_thresholds(double lam);
 int sync_and_check(bspk_plan *p);
+// Grow the plan's pinned staging buffer to at least `bytes`.
+int plan_stage(bspk_plan *p, size_t bytes);
 // Input channels of the plan's ring (receptor ports) and whether the
 // per-step engine steps it.
 inline int plan_n_receptors(const bspk_plan *p) {

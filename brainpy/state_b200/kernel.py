@@ -31,7 +31,6 @@ trials, plasticity or learners.
 from __future__ import annotations
 
 import hashlib
-import math
 
 import numpy as np
 
@@ -317,6 +316,8 @@ class Network:
                 raise NotImplementedError(f"recordable {r!r}: only 'spike' and 'V_m'")
         if any(p.is_device for p in view.populations):
             raise NotImplementedError("recording a device")
+        if np.unique(view.gids).size != view.size:
+            raise ValueError("an observer's view lists a neuron twice")
         k = 1 if interval is None else _steps(interval, self.dt, "interval")
         if k < 1:
             raise ValueError("interval must be >= dt")
@@ -519,12 +520,11 @@ class Runner:
             rec = Recording()
             if "spike" in o.recordables:
                 counts = np.zeros((ns, cols.size), np.float64)
-                col_of = {int(c): [] for c in cols}
-                for i, c in enumerate(cols):
-                    col_of[int(c)].append(i)
-                for s, gg in zip(st.tolist(), g.tolist()):
-                    for i in col_of.get(gg, ()):
-                        counts[(s - self.n) // k, i] += 1.0
+                pos = np.full(prog.n_lib, -1, np.int64)
+                pos[cols] = np.arange(cols.size)
+                col = pos[g] if g.size else np.zeros(0, np.int64)
+                ok = col >= 0
+                np.add.at(counts, ((st[ok] - self.n) // k, col[ok]), 1.0)
                 rec["spike"] = counts
             if "V_m" in o.recordables:
                 at = np.searchsorted(prog.rec_v, cols)

@@ -722,7 +722,8 @@ class Simulator:
             events[rid] = (rows, col[ok])
         traces = {}
         if self._analog_taps:
-            v = pl.v_trace()
+            # traces in the run's precision, like the spike matrices
+            v = pl.v_trace(np.float32 if self.precision == 32 else np.float64)
             for rid, sl in self._v_slices.items():
                 traces[(rid, "V_m")] = v[:, sl]
         weights = {k: pl.weights(h.proj_id)[None, :] for k, h in self._weight_taps.items()}

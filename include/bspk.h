@@ -210,6 +210,9 @@ int bspk_spikes_get(bspk_plan *plan, int64_t cap, int64_t *steps, int32_t *gids,
                     int64_t *n_out);
 /* V_m trace of the last run: [n_steps][n_rec] as double. */
 int bspk_v_get(bspk_plan *plan, double *out);
+/* The same V_m traces in float32 (the device's own values for a precision-32
+ * plan, rounded for a precision-64 one). */
+int bspk_v_get_f32(bspk_plan *plan, float *out);
 int bspk_weights_get(bspk_plan *plan, int proj_id, double *w_csr_order);
 int bspk_state_get(bspk_plan *plan, int pop, const char *name, double *values);
 int bspk_state_set(bspk_plan *plan, int pop, const char *name, const double *values);
