@@ -111,3 +111,23 @@ def test_poisson_cdf_counts_match_oracle(oracle):
                 F.append(F[-1] + p)
             ref = next((j for j, f in enumerate(F) if u <= f), len(F))
             assert k == ref, (lam, u)
+
+
+def test_set_weights_on_library_drawn_connectivity():
+    """Distributed weights on library-drawn fixed_indegree edges: the weights
+    land in CSR order, the edges stay those of the sampler (host only)."""
+    pl = _lib.Plan(0.1)
+    a = pl.add_pop(50, ALPHA)
+    j = pl.add_fixed_indegree(a, a, 7, 123, 1.0, delay_const=5)
+    indptr, post, d, w = pl.csr(j)
+    assert w.size == 350 and np.all(w == 1.0)
+    new = np.linspace(0.5, 2.0, 350)
+    pl.set_weights(j, new)
+    indptr2, post2, d2, w2 = pl.csr(j)
+    np.testing.assert_array_equal(w2, new)
+    np.testing.assert_array_equal(post2, post)
+    with pytest.raises(ValueError, match="every edge"):
+        pl.set_weights(j, new[:10])
+    pl.attach_stdp(j, Wmax=5.0)
+    with pytest.raises(RuntimeError, match="before making the projection plastic"):
+        pl.set_weights(j, new)
