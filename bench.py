@@ -469,7 +469,8 @@ def _oracle_network(pl_builder_seed=1234, precision=32):
     """The bench network rebuilt in the float64 oracle (same CSR, drives)."""
     from oracle import oracle as O
     from brainpy.state_b200 import brunel
-    pl, p = brunel.build_plan(order=2500, precision=precision, seed=pl_builder_seed, rec_v=0)
+    pl, p = brunel.build_plan(order=2500, precision=precision, seed=pl_builder_seed, rec_v=0,
+                              upload=False)  # the structure only: no device needed
     sim = O.OracleSim(0.1, "iaf_psc_alpha", semantics=O.RING)
     e = sim.add_pop(p["NE"], p["neuron"])
     i = sim.add_pop(p["NI"], p["neuron"])
@@ -478,8 +479,9 @@ def _oracle_network(pl_builder_seed=1234, precision=32):
     for j, (pre, post) in enumerate(((0, 0), (0, 1), (1, 0), (1, 1))):
         indptr, post_l, d, w = pl.csr(j)
         sim.add_proj(pre, post, indptr, post_l, w, d)
-    sim.set_state(e, "V_m", pl.get_state(0, "V_m"))
-    sim.set_state(i, "V_m", pl.get_state(1, "V_m"))
+    ve, vi = brunel.initial_v(pl_builder_seed, p["NE"], p["NI"])
+    sim.set_state(e, "V_m", ve)
+    sim.set_state(i, "V_m", vi)
     del pl
     return sim, p
 

@@ -43,11 +43,19 @@ def derive_seed(base, ordinal):
     return ((0 if base is None else int(base)) * 1_000_003 + ordinal + 1) & 0x7FFFFFFF
 
 
+def initial_v(seed, NE, NI, v_init=(0.0, 20.0)):
+    """Initial V_m of build_plan's E and I populations (uniform, seeded)."""
+    vr = np.random.default_rng(seed + 7)
+    return vr.uniform(v_init[0], v_init[1], NE), vr.uniform(v_init[0], v_init[1], NI)
+
+
 def build_plan(order=2500, precision=32, delay_steps=(10, 30), noise_delay=15, seed=1234,
                semantics=_lib.RING, deterministic=False, rec_v=100, spike_capacity=1 << 23,
-               v_init=(0.0, 20.0), g=5.0, eta=2.0):
+               v_init=(0.0, 20.0), g=5.0, eta=2.0, upload=True):
     """Brunel network in one plan.  ``delay_steps``: an int (homogeneous) or a
-    (lo, hi) pair of per-edge delays drawn uniformly on the step grid."""
+    (lo, hi) pair of per-edge delays drawn uniformly on the step grid.
+    ``upload=False`` stops before the device (the host copy of the structure
+    stays readable through ``csr``)."""
     p = brunel_params(order, g=g, eta=eta)
     pl = _lib.Plan(0.1, "iaf_psc_alpha", precision=precision, semantics=semantics,
                    deterministic=deterministic, spike_capacity=spike_capacity)
@@ -74,10 +82,12 @@ def build_plan(order=2500, precision=32, delay_steps=(10, 30), noise_delay=15, s
     N = p["NE"] + p["NI"]
     if rec_v:
         pl.record_v(np.linspace(0, N - 1, rec_v).astype(np.int32))
+    if not upload:
+        return pl, p
     pl.upload()
-    vr = np.random.default_rng(seed + 7)
-    pl.set_state(e, "V_m", vr.uniform(v_init[0], v_init[1], p["NE"]))
-    pl.set_state(i, "V_m", vr.uniform(v_init[0], v_init[1], p["NI"]))
+    ve, vi = initial_v(seed, p["NE"], p["NI"], v_init)
+    pl.set_state(e, "V_m", ve)
+    pl.set_state(i, "V_m", vi)
     return pl, p
 
 
