@@ -1353,7 +1353,7 @@ int bspk_v_get(bspk_plan *p, double *out) {
     if (n == 0) return BSPK_OK;
     // the traces come through a pinned staging buffer kept by the plan: a
     // device-to-pinned copy runs at link speed, a copy into pageable memory
-    // is staged by the driver in small pieces
+    // is staged by the CUDA driver in small pieces
     const size_t bytes = static_cast<size_t>(p->elt) * n;
     rc = plan_stage(p, bytes);
     if (rc) return rc;
