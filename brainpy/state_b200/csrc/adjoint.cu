@@ -361,20 +361,35 @@ __global__ void __launch_bounds__(1024) k_adj_backward(const AdjArgs<Real> a) {
                             const int k = k0 + u;
                             col[u] = k < d ? __ldg(a.in_col + static_cast<size_t>(k) * N + i) : -1;
                         }
+                        // the read-modify-writes of one batch: all loads
+                        // first, then all stores (one L2 round trip, not one
+                        // per spiking pre); each edge still accumulates in
+                        // time order
+                        Real spre[kAdjUnroll], old[kAdjUnroll];
 #pragma unroll
-                        for (int u = 0; u < kAdjUnroll; ++u) {
-                            if (col[u] < 0) continue;
-                            const Real sv_pre = s.sp[col[u]];
-                            if (sv_pre != Real(0)) {
-                                const size_t o = static_cast<size_t>(k0 + u) * N + i;
-                                dwb[o] = dwb[o] + lx * sv_pre;
-                            }
-                        }
+                        for (int u = 0; u < kAdjUnroll; ++u)
+                            spre[u] = col[u] >= 0 ? s.sp[col[u]] : Real(0);
+#pragma unroll
+                        for (int u = 0; u < kAdjUnroll; ++u)
+                            old[u] = spre[u] != Real(0) ? dwb[static_cast<size_t>(k0 + u) * N + i]
+                                                        : Real(0);
+#pragma unroll
+                        for (int u = 0; u < kAdjUnroll; ++u)
+                            if (spre[u] != Real(0))
+                                dwb[static_cast<size_t>(k0 + u) * N + i] = old[u] + lx * spre[u];
                     }
                 }
-                for (int q = 0; q < nact; ++q) {
-                    const size_t o = static_cast<size_t>(s.act[q]) * N + i;
-                    dwib[o] = dwib[o] + lx * static_cast<Real>(s.u[q]);
+                for (int q0 = 0; q0 < nact; q0 += kAdjUnroll) {
+                    Real old[kAdjUnroll];
+#pragma unroll
+                    for (int u = 0; u < kAdjUnroll; ++u)
+                        old[u] = q0 + u < nact ? dwib[static_cast<size_t>(s.act[q0 + u]) * N + i]
+                                               : Real(0);
+#pragma unroll
+                    for (int u = 0; u < kAdjUnroll; ++u)
+                        if (q0 + u < nact)
+                            dwib[static_cast<size_t>(s.act[q0 + u]) * N + i] =
+                                old[u] + lx * static_cast<Real>(s.u[q0 + u]);
                 }
             }
             __syncthreads();
