@@ -391,6 +391,8 @@ def adex_numbers(args):
             "ms_per_simulated_s": round(kms / 2.0, 2),
             "rtf": round(2000.0 / kms, 4),
             "rate_hz_sampled": round(float(spk.sum()) / spk.shape[1] / 2.0, 3),
+            "rk_substeps_per_neuron_step": round(
+                sim._plan.rk_substeps() / float((h["NE"] + h["NI"]) * 20000), 3),
             "build_and_run_wall_s": round(wall, 2)}
 
 

@@ -94,6 +94,7 @@ def lib():
             "bspk_state_set": (C.c_int, [vp, C.c_int, C.c_char_p, vp]),
             "bspk_step_count": (i64, [vp]),
             "bspk_last_kernel_time": (C.c_int, [vp, C.POINTER(dbl), C.POINTER(i64)]),
+            "bspk_rk_substeps": (C.c_int, [vp, C.POINTER(i64)]),
             "bspk_checkpoint_size": (C.c_int, [vp, C.POINTER(i64)]),
             "bspk_checkpoint_save": (C.c_int, [vp, vp, i64]),
             "bspk_checkpoint_restore": (C.c_int, [vp, vp, i64]),
@@ -344,6 +345,13 @@ class Plan:
         ms, n = C.c_double(), C.c_int64()
         check(self._L.bspk_last_kernel_time(self._h, C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    def rk_substeps(self):
+        """RKF45 substeps, accepted and rejected, of every conductance-model
+        neuron since upload."""
+        n = C.c_int64()
+        check(self._L.bspk_rk_substeps(self._h, C.byref(n)))
+        return n.value
 
     def checkpoint(self):
         n = C.c_int64()

@@ -42,6 +42,7 @@ struct StepArgs {
     int64_t run_step0;
     unsigned long long *rk_iters;
     int *err;
+    int static_chunks;  // edge work items per row of the widest static projection
 };
 
 // One plastic projection (pair STDP, eager substrate).
@@ -51,6 +52,8 @@ struct StdpDev {
     double tau_plus, tau_minus, lambda_, alpha, mu_plus, mu_minus, Wmax, dec_pre, dec_post;
     int rule;  // 0: pair stdp_synapse, 1: stdp_triplet_synapse
     double a2p, a3p, a2m, a3m, dec_pre2, dec_post2;  // triplet amplitudes, slow-trace decays
+    double inv_Wmax;
+    int out_chunks, in_chunks;  // edge work items per pre row / post column
     const int64_t *indptr;   // CSR over pre
     const uint32_t *edges;   // post_local | lag << 24
     double *w;               // FP64 weights, CSR order

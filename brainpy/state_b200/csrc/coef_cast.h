@@ -13,11 +13,14 @@ PopCoef<Real> cast_coef(const PopCoef<double> &d) {
     C_(ipsc) C_(eP11ex) C_(eP11in) C_(eP22) C_(eP21ex) C_(eP21in) C_(eP20) C_(one_m_eP11ex)
     C_(V_peak) C_(V_reset) C_(g_L) C_(C_m) C_(E_ex) C_(E_in) C_(Delta_T) C_(tau_w) C_(a) C_(b)
     C_(V_th) C_(tau_syn_ex) C_(tau_syn_in) C_(atol) C_(pscon_ex) C_(pscon_in) C_(v_peak_detect)
+    C_(inv_C_m) C_(inv_tau_syn_ex) C_(inv_tau_syn_in) C_(inv_tau_w)
 #undef C_
     for (int k = 0; k < 4; ++k) {
         c.msP11[k] = static_cast<Real>(d.msP11[k]);
         c.msP21[k] = static_cast<Real>(d.msP21[k]);
     }
+    c.inv_Delta_T = d.inv_Delta_T;
+    c.inv_atol = d.inv_atol;
     c.nrec = d.nrec;
     c.ref_count = d.ref_count;
     c.off = d.off;

@@ -57,6 +57,12 @@ struct PopCoef {
     // aeif_cond_alpha
     Real V_peak, V_reset, g_L, C_m, E_ex, E_in, Delta_T, tau_w, a, b, V_th, tau_syn_ex,
         tau_syn_in, atol, pscon_ex, pscon_in, v_peak_detect;
+    // reciprocals taken once on the host in FP64: the RKF45 stages multiply
+    // instead of dividing (a division is a long dependent sequence on the
+    // substep chain); inv_Delta_T and inv_atol stay FP64 for the exponential
+    // term and the error norm
+    Real inv_C_m, inv_tau_syn_ex, inv_tau_syn_in, inv_tau_w;
+    double inv_Delta_T, inv_atol;
     // iaf_psc_exp_multisynapse: per-receptor decay and membrane coupling
     // (eP22 / eP20 hold the membrane propagators)
     Real msP11[4], msP21[4];

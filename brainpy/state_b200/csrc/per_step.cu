@@ -37,6 +37,11 @@ __device__ __forceinline__ int find_pop_t(const PopCoef<Real> *c, int npop, int 
     return p;
 }
 
+// Edge work items of the delivery and STDP kernels: kEdgeU edges per lane,
+// kChunkEdges = 32 kEdgeU per warp-sized item.
+constexpr int kEdgeU = 8;
+constexpr int kChunkEdges = 32 * kEdgeU;
+
 __device__ __forceinline__ bool fired(const uint64_t *hist, int gid, int64_t m) {
     if (m < 0) return false;
     return (hist[gid] >> (m & 63)) & 1ull;
@@ -56,8 +61,11 @@ __device__ constexpr double kA[6][5] = {
 __device__ constexpr double kB[6] = {16.0 / 135, 0.0, 6656.0 / 12825, 28561.0 / 56430, -9.0 / 50, 2.0 / 55};
 __device__ constexpr double kBhat[6] = {25.0 / 216, 0.0, 1408.0 / 2565, 2197.0 / 4104, -1.0 / 5, 0.0};
 
-// Vector field (_nest_neuron/aeif_cond_alpha.py:554-592); the exponential
-// spike current is evaluated in FP64 whatever the state precision.
+// Vector field (_nest_neuron/aeif_cond_alpha.py:554-592).  The exponential
+// spike current is evaluated in FP64 from 2 Delta_T below V_th upward whatever
+// the state precision (the spike-initiation zone, where the term grows without
+// bound); below that, an FP32 state takes it in FP32.
+constexpr double kExpFp64Above = -2.0;
 template <typename Real>
 __device__ __forceinline__ void aeif_vf(const PopCoef<Real> &c, int r, Real i_stim, const Real *y,
                                         Real *dy) {
@@ -66,18 +74,27 @@ __device__ __forceinline__ void aeif_vf(const PopCoef<Real> &c, int r, Real i_st
     const Real v_eff = refr ? c.V_reset : (v < c.V_peak ? v : (v != v ? v : c.V_peak));
     const Real i_ex = y[2] * (v_eff - c.E_ex);
     const Real i_in = y[4] * (v_eff - c.E_in);
-    const double dts = c.Delta_T == Real(0) ? 1.0 : static_cast<double>(c.Delta_T);
-    double arg = static_cast<double>(v_eff - c.V_th) / dts;
-    arg = arg < -500.0 ? -500.0 : (arg > 500.0 ? 500.0 : arg);
-    const Real i_spike =
-        static_cast<Real>(static_cast<double>(c.g_L) * static_cast<double>(c.Delta_T) * exp(arg));
-    const Real dV = (-c.g_L * (v_eff - c.E_L) + i_spike - i_ex - i_in - y[5] + c.I_e + i_stim) / c.C_m;
+    Real i_spike;
+    const Real argR = (v_eff - c.V_th) * static_cast<Real>(c.inv_Delta_T);
+    if (sizeof(Real) == 4 && argR < Real(kExpFp64Above)) {
+        // FP32 state, more than 2 Delta_T below V_th: the term is below
+        // g_L Delta_T e^-2 (8 pA at the NEST defaults) and expf's 2-ulp error
+        // is under the rounding of the FP32 current sum
+        i_spike = c.g_L * c.Delta_T * expf(argR < Real(-500) ? Real(-500) : argR);
+    } else {
+        double arg = static_cast<double>(v_eff - c.V_th) * c.inv_Delta_T;
+        arg = arg < -500.0 ? -500.0 : (arg > 500.0 ? 500.0 : arg);
+        i_spike = static_cast<Real>(static_cast<double>(c.g_L) * static_cast<double>(c.Delta_T) *
+                                    exp(arg));
+    }
+    const Real dV = (-c.g_L * (v_eff - c.E_L) + i_spike - i_ex - i_in - y[5] + c.I_e + i_stim) *
+                    c.inv_C_m;
     dy[0] = refr ? Real(0) : dV;
-    dy[1] = -y[1] / c.tau_syn_ex;
-    dy[2] = y[1] - y[2] / c.tau_syn_ex;
-    dy[3] = -y[3] / c.tau_syn_in;
-    dy[4] = y[3] - y[4] / c.tau_syn_in;
-    dy[5] = (c.a * (v_eff - c.E_L) - y[5]) / c.tau_w;
+    dy[1] = -y[1] * c.inv_tau_syn_ex;
+    dy[2] = y[1] - y[2] * c.inv_tau_syn_ex;
+    dy[3] = -y[3] * c.inv_tau_syn_in;
+    dy[4] = y[3] - y[4] * c.inv_tau_syn_in;
+    dy[5] = (c.a * (v_eff - c.E_L) - y[5]) * c.inv_tau_w;
 }
 
 // Vector fields of the iaf conductance models: iaf_cond_exp
@@ -95,16 +112,16 @@ __device__ __forceinline__ void iaf_cond_vf(const PopCoef<Real> &c, int r, Real 
     const Real i_syn_exc = gex * (v_eff - c.E_ex);
     const Real i_syn_inh = gin * (v_eff - c.E_in);
     const Real i_leak = c.g_L * (v_eff - c.E_L);
-    const Real dV = (-i_leak - i_syn_exc - i_syn_inh + c.I_e + i_stim) / c.C_m;
+    const Real dV = (-i_leak - i_syn_exc - i_syn_inh + c.I_e + i_stim) * c.inv_C_m;
     dy[0] = refr ? Real(0) : dV;
     if constexpr (MODEL == 3) {
-        dy[1] = -y[1] / c.tau_syn_ex;
-        dy[2] = -y[2] / c.tau_syn_in;
+        dy[1] = -y[1] * c.inv_tau_syn_ex;
+        dy[2] = -y[2] * c.inv_tau_syn_in;
     } else {
-        dy[1] = -y[1] / c.tau_syn_ex;
-        dy[2] = y[1] - y[2] / c.tau_syn_ex;
-        dy[3] = -y[3] / c.tau_syn_in;
-        dy[4] = y[3] - y[4] / c.tau_syn_in;
+        dy[1] = -y[1] * c.inv_tau_syn_ex;
+        dy[2] = y[1] - y[2] * c.inv_tau_syn_ex;
+        dy[3] = -y[3] * c.inv_tau_syn_in;
+        dy[4] = y[3] - y[4] * c.inv_tau_syn_in;
     }
 }
 
@@ -127,7 +144,7 @@ __device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
     for (int i = 0; i < NS; ++i) y[i] = s[i];
     double h = static_cast<double>(s[NS]);
     const Real i_stim = s[NS + 1];
-    const double atol = static_cast<double>(c.atol);
+    const double inv_atol = c.inv_atol;
     bool spiked = false, unstable = false;
     double t_loc = 0.0;
     if (h < min_h) h = min_h;
@@ -187,7 +204,9 @@ __device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
             const double ay = fabs(static_cast<double>(y[i])) > fabs(static_cast<double>(yh[i]))
                                   ? fabs(static_cast<double>(y[i]))
                                   : fabs(static_cast<double>(yh[i]));
-            const double e = fabs(static_cast<double>(ye)) / (atol + 0.0 * ay);
+            // |err| / atol (rtol = 0); the 0 * |y| term carries a NaN or an
+            // infinite state into the norm as the reference's scale does
+            const double e = fabs(static_cast<double>(ye)) * inv_atol + 0.0 * ay;
             err = i == 0 ? e : ((err != err || e != e) ? NAN : (err > e ? err : e));
         }
         if (err != err) err = INFINITY;
@@ -210,13 +229,14 @@ __device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
             }
         }
         const double err_sg = err > 1e-30 ? err : 1e-30;
-        const double inv_err = 1.0 / err_sg;
         double fac;
         if (accept) {
-            fac = err_sg <= 1e-30 ? 5.0 : 0.9 * pow(inv_err, 1.0 / 5.0);
+            // 0.9 (1 / err)^(1/5), taken as exp(-log(err) / 5): no division
+            // and a shorter chain than pow on the substep's critical path
+            fac = err_sg <= 1e-30 ? 5.0 : 0.9 * exp(-0.2 * log(err_sg));
             if (!(err_sg <= 1e-30)) fac = fac < 0.2 ? 0.2 : (fac > 5.0 ? 5.0 : fac);
         } else {
-            fac = 0.9 * pow(inv_err, 1.0 / 4.0);
+            fac = 0.9 * exp(-0.25 * log(err_sg));
             fac = fac < 0.2 ? 0.2 : (fac > 1.0 ? 1.0 : fac);
         }
         const double hn = h * fac;
@@ -225,7 +245,13 @@ __device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
     }
     if (iters >= kMaxIters && t_loc < dt) atomicExch(err, BSPK_DEV_ERR_RKCAP);
     if (unstable) atomicExch(err, BSPK_DEV_ERR_UNSTABLE);
-    atomicAdd(rk_iters, static_cast<unsigned long long>(iters));
+    {
+        // one atomic per group of converged lanes, not one per neuron
+        const unsigned m = __activemask();
+        const unsigned sum = __reduce_add_sync(m, static_cast<unsigned>(iters));
+        if ((threadIdx.x & 31) == __ffs(m) - 1)
+            atomicAdd(rk_iters, static_cast<unsigned long long>(sum));
+    }
     if (r > 0) r = r - 1;
     if constexpr (MODEL == 3) {
         y[1] = y[1] + w_ex;
@@ -347,7 +373,11 @@ __global__ void __launch_bounds__(128) k_neuron_step(const StepArgs<Real> a, dou
     }
 }
 
-// Static delivery of this step's spikes: one warp per (spike, projection).
+// Static delivery of this step's spikes.  A work item is one chunk of
+// kChunkEdges out-edges of one (spike, projection) pair, so a long row is
+// spread over several warps; each lane loads its kEdgeU edge words and
+// weights before the first atomic, which keeps kEdgeU loads in flight instead
+// of one round trip per edge.
 template <typename Real>
 __global__ void __launch_bounds__(256) k_deliver_static(const StepArgs<Real> a) {
     const int64_t n = *a.step_ptr;
@@ -356,23 +386,36 @@ __global__ void __launch_bounds__(256) k_deliver_static(const StepArgs<Real> a) 
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     const int slot_n = static_cast<int>(n % a.L);
-    for (int item = warp; item < nspk * a.nproj; item += nwarps) {
-        const int i = item / a.nproj, q = item % a.nproj;
+    const int C = a.static_chunks;
+    const int64_t per_spike = static_cast<int64_t>(a.nproj) * C;
+    for (int64_t item = warp; item < nspk * per_spike; item += nwarps) {
+        const int i = static_cast<int>(item / per_spike);
+        const int rem = static_cast<int>(item % per_spike);
+        const int q = rem / C, chunk = rem % C;
         if (a.proj_plastic[q]) continue;
-        const ProjDev<Real> P = a.projs[q];
+        const ProjDev<Real> &P = a.projs[q];
         const int g = static_cast<int>(a.step_spk[i]);
         const int pre_off = a.coef[P.pre_pop].off;
         if (g < pre_off || g >= pre_off + a.coef[P.pre_pop].n) continue;
         const int gl = g - pre_off;
-        const int64_t beg = P.indptr[gl], end = P.indptr[gl + 1];
-        for (int64_t e = beg + lane; e < end; e += 32) {
-            const uint32_t ed = __ldg(P.edges + e);
-            int slot = slot_n + static_cast<int>(ed >> kEdgeDelayShift);
-            slot %= a.L;
-            const Real w = P.homogeneous ? P.w0 : __ldg(P.w + e);
+        const int64_t beg = P.indptr[gl] + static_cast<int64_t>(chunk) * kChunkEdges;
+        const int64_t end = P.indptr[gl + 1];
+        if (beg >= end) continue;
+        uint32_t ed[kEdgeU];
+        Real w[kEdgeU];
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            const int64_t e = beg + u * 32 + lane;
+            ed[u] = e < end ? __ldg(P.edges + e) : 0xFFFFFFFFu;
+            w[u] = (e < end && !P.homogeneous) ? __ldg(P.w + e) : P.w0;
+        }
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            if (ed[u] == 0xFFFFFFFFu) continue;
+            const int slot = (slot_n + static_cast<int>(ed[u] >> kEdgeDelayShift)) % a.L;
             atomicAdd(a.ring + (static_cast<size_t>(slot) * a.R + P.receptor) * a.N + P.post_off +
-                          (ed & kEdgePostMask),
-                      w);
+                          (ed[u] & kEdgePostMask),
+                      w[u]);
         }
     }
 }
@@ -406,12 +449,16 @@ __global__ void k_stdp_traces(StdpDev s, const uint64_t *hist, const int64_t *st
 __device__ __forceinline__ double stdp_pow(double x, double mu) {
     return mu == 1.0 ? x : (mu == 0.0 ? 1.0 : pow(x, mu));
 }
+// the normalised weight w / Wmax is taken as w * (1 / Wmax), the reciprocal
+// formed once on the host in FP64
 __device__ __forceinline__ double stdp_facilitate(const StdpDev &s, double w, double kplus) {
-    const double nw = w / s.Wmax + s.lambda_ * stdp_pow(1.0 - w / s.Wmax, s.mu_plus) * kplus;
+    const double wn = w * s.inv_Wmax;
+    const double nw = wn + s.lambda_ * stdp_pow(1.0 - wn, s.mu_plus) * kplus;
     return nw < 1.0 ? nw * s.Wmax : s.Wmax;
 }
 __device__ __forceinline__ double stdp_depress(const StdpDev &s, double w, double kminus) {
-    const double nw = w / s.Wmax - s.alpha * s.lambda_ * stdp_pow(w / s.Wmax, s.mu_minus) * kminus;
+    const double wn = w * s.inv_Wmax;
+    const double nw = wn - s.alpha * s.lambda_ * stdp_pow(wn, s.mu_minus) * kminus;
     return nw > 0.0 ? nw * s.Wmax : 0.0;
 }
 // stdp_triplet_synapse.py:179-197: potentiation reads the fast pre trace r1
@@ -429,52 +476,101 @@ __device__ __forceinline__ double triplet_depress(const StdpDev &s, double w, do
 }
 
 // STDP 2: facilitation on the in-edges of posts that fired at n - 1
-// (_nest_plasticity/stdp_synapse.py:163-165), warp per post.
-__global__ void k_stdp_facilitate(StdpDev s, const uint64_t *hist, const int64_t *step_ptr) {
+// (_nest_plasticity/stdp_synapse.py:163-165).  A work item is one chunk of
+// kChunkEdges in-edges of one post; every lane gathers its kEdgeU pre ids,
+// edge ids, pre traces and weights before the first store.  Each in-edge
+// belongs to one post and each post is listed once, so no two lanes touch
+// one weight.
+__global__ void __launch_bounds__(256) k_stdp_facilitate(StdpDev s, const uint64_t *hist,
+                                                         const int64_t *step_ptr) {
     const int64_t n = *step_ptr;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    const int npost = s.counts[1];
-    for (int it = warp; it < npost; it += nwarps) {
-        const int j = s.post_list[it];
-        for (int64_t e = s.cindptr[j] + lane; e < s.cindptr[j + 1]; e += 32) {
-            const int pre = static_cast<int>(s.cedges[e] & kEdgePostMask);
-            const double x = fired(hist, s.pre_off + pre, n - s.lag) ? 1.0 : 0.0;
-            const double kplus = s.pre_trace[pre] - x;
-            const int64_t eid = s.cperm[e];
-            // the post fired at n - 1, so its own spike is 1 in every post trace
-            s.w[eid] = s.rule == 1 ? triplet_facilitate(s, s.w[eid], kplus, s.post_trace2[j] - 1.0)
-                                   : stdp_facilitate(s, s.w[eid], kplus);
+    const int C = s.in_chunks;
+    const int64_t nitems = static_cast<int64_t>(s.counts[1]) * C;
+    for (int64_t it = warp; it < nitems; it += nwarps) {
+        const int j = s.post_list[it / C];
+        const int64_t beg = s.cindptr[j] + (it % C) * kChunkEdges, end = s.cindptr[j + 1];
+        if (beg >= end) continue;
+        // the post fired at n - 1, so its own spike is 1 in every post trace
+        const double o2 = s.rule == 1 ? s.post_trace2[j] - 1.0 : 0.0;
+        int pre[kEdgeU];
+        int64_t eid[kEdgeU];
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            const int64_t e = beg + u * 32 + lane;
+            pre[u] = e < end ? static_cast<int>(s.cedges[e] & kEdgePostMask) : -1;
+            eid[u] = e < end ? s.cperm[e] : 0;
+        }
+        double kplus[kEdgeU], w[kEdgeU];
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            if (pre[u] < 0) continue;
+            const double x = fired(hist, s.pre_off + pre[u], n - s.lag) ? 1.0 : 0.0;
+            kplus[u] = s.pre_trace[pre[u]] - x;
+            w[u] = s.w[eid[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            if (pre[u] < 0) continue;
+            s.w[eid[u]] = s.rule == 1 ? triplet_facilitate(s, w[u], kplus[u], o2)
+                                      : stdp_facilitate(s, w[u], kplus[u]);
         }
     }
 }
 
 // STDP 3: depression on the out-edges of pres whose delayed spike arrives
 // now (stdp_synapse.py:167-169), then delivery of the updated weight into
-// this step's ring slot (event_plastic.py:497-518), warp per pre.
+// this step's ring slot (event_plastic.py:497-518).  Work items are chunks
+// of kChunkEdges out-edges of one pre, with the loads of a lane's kEdgeU
+// edges issued before its stores and atomics.
 template <typename Real>
-__global__ void k_stdp_depress(StdpDev s, const StepArgs<Real> a) {
+__global__ void __launch_bounds__(256) k_stdp_depress(StdpDev s, const StepArgs<Real> a) {
     const int64_t n = *a.step_ptr;
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
-    const int npre = s.counts[0];
+    const int C = s.out_chunks;
+    const int64_t nitems = static_cast<int64_t>(s.counts[0]) * C;
     const int slot_n = static_cast<int>(n % a.L);
-    for (int it = warp; it < npre; it += nwarps) {
-        const int i = s.pre_list[it];
-        for (int64_t e = s.indptr[i] + lane; e < s.indptr[i + 1]; e += 32) {
-            const int j = static_cast<int>(s.edges[e] & kEdgePostMask);
-            const double y = fired(a.hist, s.post_off + j, n - 1) ? 1.0 : 0.0;
-            const double kminus = s.post_trace[j] - y;
-            // the pre's delayed spike arrives now: 1 in every pre trace
-            const double w = s.rule == 1 ? triplet_depress(s, s.w[e], kminus, s.pre_trace2[i] - 1.0)
-                                         : stdp_depress(s, s.w[e], kminus);
-            s.w[e] = w;
-            atomicAdd(a.ring + (static_cast<size_t>(slot_n) * a.R + s.receptor) * a.N + s.post_off + j,
-                      static_cast<Real>(w));
+    Real *ring = a.ring + (static_cast<size_t>(slot_n) * a.R + s.receptor) * a.N + s.post_off;
+    for (int64_t it = warp; it < nitems; it += nwarps) {
+        const int i = s.pre_list[it / C];
+        const int64_t beg = s.indptr[i] + (it % C) * kChunkEdges, end = s.indptr[i + 1];
+        if (beg >= end) continue;
+        // the pre's delayed spike arrives now: 1 in every pre trace
+        const double r2 = s.rule == 1 ? s.pre_trace2[i] - 1.0 : 0.0;
+        int post[kEdgeU];
+        double w[kEdgeU];
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            const int64_t e = beg + u * 32 + lane;
+            post[u] = e < end ? static_cast<int>(s.edges[e] & kEdgePostMask) : -1;
+            w[u] = e < end ? s.w[e] : 0.0;
+        }
+        double kminus[kEdgeU];
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            if (post[u] < 0) continue;
+            const double y = fired(a.hist, s.post_off + post[u], n - 1) ? 1.0 : 0.0;
+            kminus[u] = s.post_trace[post[u]] - y;
+        }
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            if (post[u] < 0) continue;
+            const double nw = s.rule == 1 ? triplet_depress(s, w[u], kminus[u], r2)
+                                          : stdp_depress(s, w[u], kminus[u]);
+            s.w[beg + u * 32 + lane] = nw;
+            atomicAdd(ring + post[u], static_cast<Real>(nw));
         }
     }
+}
+
+// work items per row for rows of at most max_deg edges (at least one)
+int chunks_of(int64_t max_deg) {
+    const int64_t c = (max_deg + kChunkEdges - 1) / kChunkEdges;
+    return c > 0 ? static_cast<int>(c) : 1;
 }
 
 template <typename Real>
@@ -513,6 +609,10 @@ StepArgs<Real> step_args(bspk_plan *p, int64_t *step_ptr) {
     a.run_step0 = p->step;
     a.rk_iters = p->d_rk_iters;
     a.err = p->d_err;
+    int64_t max_out = 0;
+    for (const Proj &J : p->projs)
+        if (!J.plastic && J.max_out > max_out) max_out = J.max_out;
+    a.static_chunks = chunks_of(max_out);
     return a;
 }
 
@@ -538,6 +638,8 @@ std::vector<StdpDev> stdp_descs(bspk_plan *p) {
         s.dec_pre = std::exp(-p->cfg.dt / J.stdp.tau_plus);
         s.dec_post = std::exp(-p->cfg.dt / J.stdp.tau_minus);
         s.rule = J.rule;
+        s.out_chunks = chunks_of(J.max_out);
+        s.in_chunks = chunks_of(J.max_in);
         if (J.rule == 1) {
             const bspk_stdp_triplet_params &t = J.trip;
             s.Wmax = t.Wmax;
@@ -550,6 +652,7 @@ std::vector<StdpDev> stdp_descs(bspk_plan *p) {
             s.dec_pre2 = std::exp(-p->cfg.dt / t.tau_plus_triplet);
             s.dec_post2 = std::exp(-p->cfg.dt / t.tau_minus_triplet);
         }
+        s.inv_Wmax = 1.0 / s.Wmax;
         s.indptr = J.d_indptr;
         s.edges = J.d_edges;
         s.w = J.d_wplastic;

@@ -126,6 +126,18 @@ double propagator_exp(double tau_syn, double tau_m, double c_m, double h) {
 
 constexpr double kE = 2.718281828459045;
 
+// Reciprocals of the conductance models' divisors, in FP64, for the RKF45
+// stages.  A zero Delta_T leaves the exponential term at zero whatever its
+// argument, so its scale is then 1.
+void set_cond_reciprocals(PopCoef<double> *c) {
+    c->inv_C_m = 1.0 / c->C_m;
+    c->inv_tau_syn_ex = 1.0 / c->tau_syn_ex;
+    c->inv_tau_syn_in = 1.0 / c->tau_syn_in;
+    c->inv_tau_w = c->tau_w > 0.0 ? 1.0 / c->tau_w : 0.0;
+    c->inv_Delta_T = c->Delta_T == 0.0 ? 1.0 : 1.0 / c->Delta_T;
+    c->inv_atol = 1.0 / c->atol;
+}
+
 int make_coef(int model, const std::vector<double> &p, double h, PopCoef<double> *c) {
     memset(c, 0, sizeof(*c));
     if (model == BSPK_IAF_PSC_ALPHA || model == BSPK_IAF_PSC_EXP) {
@@ -204,6 +216,7 @@ int make_coef(int model, const std::vector<double> &p, double h, PopCoef<double>
         c->pscon_ex = kE / c->tau_syn_ex;
         c->pscon_in = kE / c->tau_syn_in;
         c->v_peak_detect = c->Delta_T > 0.0 ? c->V_peak : c->V_th;
+        set_cond_reciprocals(c);
         return BSPK_OK;
     }
     if (model == BSPK_IAF_COND_EXP || model == BSPK_IAF_COND_ALPHA) {
@@ -236,6 +249,7 @@ int make_coef(int model, const std::vector<double> &p, double h, PopCoef<double>
         c->pscon_in = model == BSPK_IAF_COND_ALPHA ? kE / c->tau_syn_in : 1.0;
         c->V_peak = c->V_th;
         c->v_peak_detect = c->V_th;
+        set_cond_reciprocals(c);
         return BSPK_OK;
     }
     if (model == BSPK_IAF_PSC_EXP_MULTISYNAPSE) {
@@ -705,6 +719,15 @@ int upload_projs(bspk_plan *p) {
         for (int64_t e = 0; e < E; ++e)
             edges[e] = static_cast<uint32_t>(J.post_local[e]) |
                        (static_cast<uint32_t>(lag_of(p, J.delay[e])) << kEdgeDelayShift);
+        {
+            J.max_out = 0;
+            for (int i = 0; i < npre; ++i)
+                J.max_out = std::max<int64_t>(J.max_out, J.indptr[i + 1] - J.indptr[i]);
+            std::vector<int64_t> indeg(npost, 0);
+            for (int64_t e = 0; e < E; ++e) indeg[J.post_local[e]]++;
+            J.max_in = 0;
+            for (int64_t d : indeg) J.max_in = std::max(J.max_in, d);
+        }
         int rc = upload_vec(p, &J.d_indptr, J.indptr);
         if (!rc) rc = upload_vec(p, &J.d_edges, edges);
         if (rc) return rc;
@@ -1460,6 +1483,16 @@ int bspk_last_kernel_time(bspk_plan *p, double *ms, int64_t *launches) {
     BSPK_CUDA(cudaEventElapsedTime(&f, p->ev0, p->ev1));
     if (ms) *ms = f;
     if (launches) *launches = p->last_launches;
+    return BSPK_OK;
+}
+
+int bspk_rk_substeps(bspk_plan *p, int64_t *total) {
+    if (!p || !total || !p->uploaded) return fail(BSPK_ERR_ARG, "bad arguments");
+    const int rc = sync_and_check(p);
+    if (rc) return rc;
+    unsigned long long v = 0;
+    BSPK_CUDA(cudaMemcpy(&v, p->d_rk_iters, sizeof(v), cudaMemcpyDeviceToHost));
+    *total = static_cast<int64_t>(v);
     return BSPK_OK;
 }
 

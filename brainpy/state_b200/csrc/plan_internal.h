@@ -39,6 +39,7 @@ struct Proj {
     bspk_stdp_triplet_params trip{};
     int trace_cols() const { return rule == 1 ? 2 : 1; }  // traces per side
     int input_order = 0;
+    int64_t max_out = 0, max_in = 0;  // largest row / column of the CSR (set at upload)
     // device
     int64_t *d_indptr = nullptr;
     uint32_t *d_edges = nullptr;

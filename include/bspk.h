@@ -222,6 +222,12 @@ int64_t bspk_step_count(bspk_plan *plan);
  * launching stream): total ms and number of launches. */
 int bspk_last_kernel_time(bspk_plan *plan, double *ms, int64_t *launches);
 
+/* RKF45 substeps (accepted and rejected) of every conductance-model neuron
+ * since the plan was uploaded: the integrator's work, the counterpart of the
+ * reference's per-neuron iteration count (_nest_base/utils.py:583-718).
+ * Synchronises the plan's stream. */
+int bspk_rk_substeps(bspk_plan *plan, int64_t *total);
+
 /* Checkpoint of every device buffer that evolves (state, rings, spike
  * history, plastic weights and traces, step counter); restore is bit-exact
  * (simulator.py:1822-1839 continues without re-init). */

@@ -64,6 +64,12 @@ def test_aeif_network_fp64_matches_oracle(oracle):
     for name in ("w", "g_ex", "g_in"):
         np.testing.assert_allclose(pl.get_state(0, name), sim.get_state(0, name, 160),
                                    rtol=0, atol=2e-6)
+    # the integrator did the same work: substep counts (accepted + rejected)
+    # agree to 0.1 % (the GPU's reciprocals and err^(-1/5) round differently
+    # from the oracle's divisions, which can move an acceptance at the margin)
+    n_gpu, n_ref = pl.rk_substeps(), sim.rk_substeps
+    assert n_ref >= 200 * 150
+    assert abs(n_gpu - n_ref) <= 1e-3 * n_ref, (n_gpu, n_ref)
 
 
 def test_aeif_fp32_rate_close_to_oracle(oracle):

@@ -69,6 +69,9 @@ def test_cond_network_fp64_matches_oracle(oracle, model):
     assert len(ost) > 0
     assert set(zip(st.tolist(), g.tolist())) == set(zip(ost.tolist(), og.tolist()))
     np.testing.assert_allclose(pl.v_trace(), ov, rtol=0, atol=2e-6)
+    n_gpu, n_ref = pl.rk_substeps(), sim.rk_substeps
+    assert n_ref >= (NE + NI) * 200
+    assert abs(n_gpu - n_ref) <= 1e-3 * n_ref, (n_gpu, n_ref)
     names = ("g_ex", "g_in", "h") if model == "iaf_cond_exp" else ("dg_ex", "g_ex", "dg_in",
                                                                     "g_in", "h")
     for pop, n in ((0, NE), (1, NI)):
