@@ -125,6 +125,19 @@ __device__ __forceinline__ void iaf_cond_vf(const PopCoef<Real> &c, int r, Real 
     }
 }
 
+// err^(-q) of the step-size factor 0.9 (1 / err)^q, as exp(-q log err): no
+// division and a shorter chain than pow on the substep's critical path.  An
+// FP32 state takes it in FP32: the factor only sizes the next trial step,
+// whose error the FP64 norm then judges, so acceptance stays FP64.
+template <typename Real>
+__device__ __forceinline__ double err_pow(double err, double q) {
+    if constexpr (sizeof(Real) == 4)
+        return static_cast<double>(
+            exp2f(-static_cast<float>(q) * log2f(static_cast<float>(err))));
+    else
+        return exp(-q * log(err));
+}
+
 // One dt of the adaptive RKF45 loop (_nest_base/utils.py:583-718) for a
 // conductance model (MODEL 2: aeif_cond_alpha, 3: iaf_cond_exp,
 // 4: iaf_cond_alpha), with the model's in-loop spike/reset event
@@ -231,12 +244,10 @@ __device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
         const double err_sg = err > 1e-30 ? err : 1e-30;
         double fac;
         if (accept) {
-            // 0.9 (1 / err)^(1/5), taken as exp(-log(err) / 5): no division
-            // and a shorter chain than pow on the substep's critical path
-            fac = err_sg <= 1e-30 ? 5.0 : 0.9 * exp(-0.2 * log(err_sg));
+            fac = err_sg <= 1e-30 ? 5.0 : 0.9 * err_pow<Real>(err_sg, 0.2);
             if (!(err_sg <= 1e-30)) fac = fac < 0.2 ? 0.2 : (fac > 5.0 ? 5.0 : fac);
         } else {
-            fac = 0.9 * exp(-0.25 * log(err_sg));
+            fac = 0.9 * err_pow<Real>(err_sg, 0.25);
             fac = fac < 0.2 ? 0.2 : (fac > 1.0 ? 1.0 : fac);
         }
         const double hn = h * fac;
