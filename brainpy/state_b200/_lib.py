@@ -126,6 +126,7 @@ def lib():
             "bspk_adjoint_create": (C.c_int, [C.POINTER(AdjointConfig), vp, vp, i64,
                                               C.POINTER(vp)]),
             "bspk_adjoint_destroy": (C.c_int, [vp]),
+            "bspk_adjoint_ctas_per_trial": (C.c_int, [vp]),
             "bspk_adjoint_forward": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
             "bspk_adjoint_backward": (C.c_int, [vp, vp, vp, vp]),
             "bspk_xla_adjoint_forward": (None, [vp, vp, C.c_char_p, C.c_size_t]),

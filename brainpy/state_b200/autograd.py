@@ -42,6 +42,11 @@ class LifAdjoint:
         self.nnz = int(cl.size)
         self.forward_id = 0
 
+    @property
+    def ctas_per_trial(self):
+        """1, or 2 when each trial runs on a two-CTA cluster."""
+        return int(self._L.bspk_adjoint_ctas_per_trial(self._h))
+
     def close(self):
         if getattr(self, "_h", None):
             self._L.bspk_adjoint_destroy(self._h)

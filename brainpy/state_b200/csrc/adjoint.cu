@@ -25,6 +25,7 @@
 // pre-major transpose (out-edges) for the adjoint of the recurrent input.
 // Per-trial gradient buffers are summed over trials in trial order by a
 // final kernel, so the result does not depend on scheduling.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -69,7 +70,44 @@ struct AdjArgs {
     double *loss_b;          // per-trial loss sums [B]
     unsigned long long *nspk;
     int64_t din_stride;      // din_max * N
+    int split;               // CTAs per trial: 1, or 2 as a thread-block cluster
 };
+
+// A trial's CTA (1 or 2 per trial).  With split = 2 the two CTAs of a
+// cluster own the neurons [lo, hi) and [hi, N) of one trial; each keeps the
+// full spike and adjoint vectors in its shared memory and writes its half
+// of each new vector into its peer's copy too, between two cluster barriers.
+struct Part {
+    int b, rank, lo, hi;
+};
+template <typename Real>
+__device__ __forceinline__ Part part_of(const AdjArgs<Real> &a) {
+    Part q;
+    q.b = blockIdx.x / a.split;
+    q.rank = blockIdx.x % a.split;
+    q.lo = static_cast<int>(static_cast<int64_t>(a.N) * q.rank / a.split);
+    q.hi = static_cast<int>(static_cast<int64_t>(a.N) * (q.rank + 1) / a.split);
+    return q;
+}
+// barrier over the trial's CTAs
+template <typename Real>
+__device__ __forceinline__ void trial_sync(const AdjArgs<Real> &a) {
+    if (a.split > 1) cooperative_groups::this_cluster().sync();
+    else __syncthreads();
+}
+// dst[i] = src[i] for the part's neurons, in this CTA and (split = 2) in the
+// peer's copy of dst; callers bracket it with trial_sync
+template <typename Real>
+__device__ __forceinline__ void publish(const AdjArgs<Real> &a, const Part &q, Real *dst,
+                                        const Real *src) {
+    Real *peer = dst;
+    if (a.split > 1) peer = cooperative_groups::this_cluster().map_shared_rank(dst, q.rank ^ 1);
+    for (int i = q.lo + threadIdx.x; i < q.hi; i += blockDim.x) {
+        const Real v = src[i];
+        dst[i] = v;
+        if (a.split > 1) peer[i] = v;
+    }
+}
 
 template <typename Real>
 struct Smem {
@@ -138,11 +176,11 @@ __device__ void gather_inputs(const AdjArgs<Real> &a, const Smem<Real> &s, int t
 // pointer set, the step's x, V before the spike test, spike and the
 // not-refractory flag are stored at trace row `row`.
 template <typename Real>
-__device__ void forward_step(const AdjArgs<Real> &a, const Smem<Real> &s, int t, int b,
+__device__ void forward_step(const AdjArgs<Real> &a, const Smem<Real> &s, int t, const Part &q,
                              bool has_prev, bool trace, int row, unsigned &nsp) {
-    const int N = a.N, NI = a.NI;
+    const int N = a.N, NI = a.NI, b = q.b;
     const int nact = s.act[NI];
-    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+    for (int i = q.lo + threadIdx.x; i < q.hi; i += blockDim.x) {
         Real x = Real(0);
         if (has_prev) {
             // zero spikes add nothing: skipping them leaves every rounding unchanged
@@ -194,23 +232,26 @@ __device__ void forward_step(const AdjArgs<Real> &a, const Smem<Real> &s, int t,
 }
 
 template <typename Real>
-__device__ void load_checkpoint(const AdjArgs<Real> &a, const Smem<Real> &s, int seg, int b) {
-    const size_t o = (static_cast<size_t>(seg) * a.B + b) * a.N;
-    for (int i = threadIdx.x; i < a.N; i += blockDim.x) {
+__device__ void load_checkpoint(const AdjArgs<Real> &a, const Smem<Real> &s, int seg, const Part &q) {
+    const size_t o = (static_cast<size_t>(seg) * a.B + q.b) * a.N;
+    for (int i = q.lo + threadIdx.x; i < q.hi; i += blockDim.x) {
         s.V[i] = a.ck_V[o + i];
         s.Ie[i] = a.ck_Ie[o + i];
         s.Ii[i] = a.ck_Ii[o + i];
         s.r[i] = a.ck_r[o + i];
-        s.sp[i] = a.ck_s[o + i];
     }
+    // the whole spike vector: the recurrent gather reads every pre
+    for (int i = threadIdx.x; i < a.N; i += blockDim.x) s.sp[i] = a.ck_s[o + i];
+    const int b = q.b;
     const size_t oz = (static_cast<size_t>(seg) * a.B + b) * a.R;
     for (int j = threadIdx.x; j < a.R; j += blockDim.x) s.z[j] = a.ck_z[oz + j];
 }
 
 template <typename Real>
-__device__ void store_checkpoint(const AdjArgs<Real> &a, const Smem<Real> &s, int seg, int b) {
+__device__ void store_checkpoint(const AdjArgs<Real> &a, const Smem<Real> &s, int seg, const Part &q) {
+    const int b = q.b;
     const size_t o = (static_cast<size_t>(seg) * a.B + b) * a.N;
-    for (int i = threadIdx.x; i < a.N; i += blockDim.x) {
+    for (int i = q.lo + threadIdx.x; i < q.hi; i += blockDim.x) {
         a.ck_V[o + i] = s.V[i];
         a.ck_Ie[o + i] = s.Ie[i];
         a.ck_Ii[o + i] = s.Ii[i];
@@ -218,14 +259,16 @@ __device__ void store_checkpoint(const AdjArgs<Real> &a, const Smem<Real> &s, in
         a.ck_s[o + i] = s.sp[i];
     }
     const size_t oz = (static_cast<size_t>(seg) * a.B + b) * a.R;
-    for (int j = threadIdx.x; j < a.R; j += blockDim.x) a.ck_z[oz + j] = s.z[j];
+    if (q.rank == 0)  // the readouts (neurons 0..R-1) belong to the first part
+        for (int j = threadIdx.x; j < a.R; j += blockDim.x) a.ck_z[oz + j] = s.z[j];
 }
 
 template <typename Real>
 __global__ void __launch_bounds__(1024) k_adj_forward(const AdjArgs<Real> a) {
     extern __shared__ __align__(16) unsigned char raw[];
     const Smem<Real> s = carve<Real>(raw, a.N, a.R, a.NI);
-    const int b = blockIdx.x;
+    const Part q = part_of(a);
+    const int b = q.b;
     for (int i = threadIdx.x; i < a.N; i += blockDim.x) {
         s.V[i] = Real(0);
         s.Ie[i] = Real(0);
@@ -238,23 +281,25 @@ __global__ void __launch_bounds__(1024) k_adj_forward(const AdjArgs<Real> a) {
         s.acc[j] = 0.0;
     }
     unsigned nsp = 0;
-    __syncthreads();
+    trial_sync(a);
     for (int t = 0; t < a.T; ++t) {
-        if (t % a.K == 0) store_checkpoint(a, s, t / a.K, b);
+        if (t % a.K == 0) store_checkpoint(a, s, t / a.K, q);
         gather_inputs(a, s, t, b);
         __syncthreads();
-        forward_step(a, s, t, b, t > 0, false, 0, nsp);
-        __syncthreads();
-        const Real *y = a.targets + (static_cast<size_t>(t) * a.B + b) * a.R;
-        for (int j = threadIdx.x; j < a.R; j += blockDim.x) {
-            s.z[j] = s.z[j] * a.alpha + a.cz * s.sc[j];
-            const double d = static_cast<double>(s.z[j] - y[j]);
-            s.acc[j] = s.acc[j] + d * d;
+        forward_step(a, s, t, q, t > 0, false, 0, nsp);
+        trial_sync(a);  // every read of step t - 1's spikes is done
+        if (q.rank == 0) {
+            const Real *y = a.targets + (static_cast<size_t>(t) * a.B + b) * a.R;
+            for (int j = threadIdx.x; j < a.R; j += blockDim.x) {
+                s.z[j] = s.z[j] * a.alpha + a.cz * s.sc[j];
+                const double d = static_cast<double>(s.z[j] - y[j]);
+                s.acc[j] = s.acc[j] + d * d;
+            }
         }
-        for (int i = threadIdx.x; i < a.N; i += blockDim.x) s.sp[i] = s.sc[i];
-        __syncthreads();
+        publish(a, q, s.sp, s.sc);
+        trial_sync(a);
     }
-    if (threadIdx.x == 0) {
+    if (q.rank == 0 && threadIdx.x == 0) {
         double lb = 0.0;
         for (int j = 0; j < a.R; ++j) lb = lb + s.acc[j];
         a.loss_b[b] = lb;
@@ -269,7 +314,8 @@ template <typename Real>
 __global__ void __launch_bounds__(1024) k_adj_backward(const AdjArgs<Real> a) {
     extern __shared__ __align__(16) unsigned char raw[];
     const Smem<Real> s = carve<Real>(raw, a.N, a.R, a.NI);
-    const int b = blockIdx.x, N = a.N, NI = a.NI;
+    const Part q = part_of(a);
+    const int b = q.b, N = a.N, NI = a.NI;
     for (int i = threadIdx.x; i < N; i += blockDim.x) {
         s.lV[i] = Real(0);
         s.lIe[i] = Real(0);
@@ -283,29 +329,32 @@ __global__ void __launch_bounds__(1024) k_adj_backward(const AdjArgs<Real> a) {
     for (int seg = a.nseg - 1; seg >= 0; --seg) {
         const int t0 = seg * a.K, t1 = min(a.T, t0 + a.K);
         // 1. recompute the segment from its checkpoint, keeping the trace
-        __syncthreads();
-        load_checkpoint(a, s, seg, b);
-        __syncthreads();
+        trial_sync(a);
+        load_checkpoint(a, s, seg, q);
+        trial_sync(a);
         for (int t = t0; t < t1; ++t) {
             gather_inputs(a, s, t, b);
             __syncthreads();
-            forward_step(a, s, t, b, t > 0, true, t - t0, nsp_unused);
-            __syncthreads();
-            const size_t oz = (static_cast<size_t>(b) * a.K + (t - t0)) * a.R;
-            for (int j = threadIdx.x; j < a.R; j += blockDim.x) {
-                s.z[j] = s.z[j] * a.alpha + a.cz * s.sc[j];
-                a.tr_z[oz + j] = s.z[j];
+            forward_step(a, s, t, q, t > 0, true, t - t0, nsp_unused);
+            trial_sync(a);  // every read of step t - 1's spikes is done
+            if (q.rank == 0) {
+                const size_t oz = (static_cast<size_t>(b) * a.K + (t - t0)) * a.R;
+                for (int j = threadIdx.x; j < a.R; j += blockDim.x) {
+                    s.z[j] = s.z[j] * a.alpha + a.cz * s.sc[j];
+                    a.tr_z[oz + j] = s.z[j];
+                }
             }
-            for (int i = threadIdx.x; i < N; i += blockDim.x) s.sp[i] = s.sc[i];
-            __syncthreads();
+            publish(a, q, s.sp, s.sc);
+            trial_sync(a);  // the trace rows of both parts are written too
         }
         // 2. adjoint sweep over the segment, last step first
         for (int t = t1 - 1; t >= t0; --t) {
             const int row = t - t0;
             const Real *y = a.targets + (static_cast<size_t>(t) * a.B + b) * a.R;
             const size_t oz = (static_cast<size_t>(b) * a.K + row) * a.R;
-            for (int j = threadIdx.x; j < a.R; j += blockDim.x)
-                s.g[j] = (a.tr_z[oz + j] - y[j]) * a.inv + a.alpha * s.g[j];
+            if (q.rank == 0)
+                for (int j = threadIdx.x; j < a.R; j += blockDim.x)
+                    s.g[j] = (a.tr_z[oz + j] - y[j]) * a.inv + a.alpha * s.g[j];
             gather_inputs(a, s, t, b);
             // spikes of step t - 1 (for the weight gradient) into s.sp
             if (t > 0) {
@@ -314,7 +363,7 @@ __global__ void __launch_bounds__(1024) k_adj_backward(const AdjArgs<Real> a) {
                 for (int i = threadIdx.x; i < N; i += blockDim.x) s.sp[i] = src[i];
             }
             __syncthreads();
-            for (int p = threadIdx.x; p < N; p += blockDim.x) {
+            for (int p = q.lo + threadIdx.x; p < q.hi; p += blockDim.x) {
                 Real l = p < a.R ? a.cz * s.g[p] : Real(0);
                 const int d = a.deg_out[p];
                 for (int k0 = 0; k0 < d; k0 += kAdjUnroll) {
@@ -335,7 +384,7 @@ __global__ void __launch_bounds__(1024) k_adj_backward(const AdjArgs<Real> a) {
             }
             __syncthreads();
             const int nact = s.act[NI];
-            for (int i = threadIdx.x; i < N; i += blockDim.x) {
+            for (int i = q.lo + threadIdx.x; i < q.hi; i += blockDim.x) {
                 const size_t o = (static_cast<size_t>(b) * a.K + row) * N + i;
                 const bool nr = a.tr_a[o] != 0;
                 const Real Vt = a.tr_vt[o], sv = a.tr_s[o];
@@ -392,9 +441,9 @@ __global__ void __launch_bounds__(1024) k_adj_backward(const AdjArgs<Real> a) {
                                 old[u] + lx * static_cast<Real>(s.u[q0 + u]);
                 }
             }
-            __syncthreads();
-            for (int i = threadIdx.x; i < N; i += blockDim.x) s.lxn[i] = s.lxc[i];
-            __syncthreads();
+            trial_sync(a);  // every read of the previous lxn is done
+            publish(a, q, s.lxn, s.lxc);
+            trial_sync(a);
         }
     }
 }
@@ -458,6 +507,7 @@ using namespace bspk;
 struct bspk_adjoint {
     bspk_adjoint_config cfg{};
     int elt = 4, nseg = 0, threads = 0, din_max = 0, dout_max = 0;
+    int split = 1;  // CTAs per trial (2: a thread-block cluster per trial)
     int64_t nnz = 0;
     size_t smem = 0;
     std::vector<void *> allocs;
@@ -533,7 +583,27 @@ AdjArgs<Real> make_args(const bspk_adjoint *h) {
     a.loss_b = h->loss_b;
     a.nspk = h->nspk;
     a.din_stride = static_cast<int64_t>(h->din_max) * c.n;
+    a.split = h->split;
     return a;
+}
+
+// One CTA per trial, or (split = 2) a cluster of two CTAs per trial.
+template <typename Real>
+cudaError_t launch_trials(void (*kernel)(AdjArgs<Real>), const AdjArgs<Real> &a,
+                          const bspk_adjoint *h, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(h->cfg.batch * h->split));
+    cfg.blockDim = dim3(static_cast<unsigned>(h->threads));
+    cfg.dynamicSmemBytes = h->smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = static_cast<unsigned>(h->split);
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, a);
 }
 
 template <typename Real>
@@ -559,8 +629,7 @@ int run_forward(bspk_adjoint *h, const void *w, const void *w_in, double *loss, 
     BSPK_CUDA(cudaGetLastError());
     const AdjArgs<Real> a = make_args<Real>(h);
     BSPK_CUDA(cudaMemsetAsync(h->nspk, 0, sizeof(unsigned long long), st));
-    k_adj_forward<Real><<<c.batch, h->threads, h->smem, st>>>(a);
-    BSPK_CUDA(cudaGetLastError());
+    BSPK_CUDA(launch_trials<Real>(k_adj_forward<Real>, a, h, st));
     const double denom = static_cast<double>(c.batch) * c.n_steps * c.n_readout;
     k_adj_loss<<<1, 32, 0, st>>>(h->loss_b, c.batch, denom, loss);
     BSPK_CUDA(cudaGetLastError());
@@ -577,8 +646,7 @@ int run_backward(bspk_adjoint *h, void *dw, void *dw_in, cudaStream_t st) {
     const size_t nwi = static_cast<size_t>(c.batch) * c.n * c.n_in;
     BSPK_CUDA(cudaMemsetAsync(h->dwb, 0, sizeof(Real) * std::max<size_t>(nw, 1), st));
     BSPK_CUDA(cudaMemsetAsync(h->dwib, 0, sizeof(Real) * std::max<size_t>(nwi, 1), st));
-    k_adj_backward<Real><<<c.batch, h->threads, h->smem, st>>>(a);
-    BSPK_CUDA(cudaGetLastError());
+    BSPK_CUDA(launch_trials<Real>(k_adj_backward<Real>, a, h, st));
     if (h->nnz > 0)
         k_adj_reduce<Real><<<grid_of(h->nnz), 256, 0, st>>>(static_cast<const Real *>(h->dwb),
                                                            a.din_stride, h->in_pos, h->nnz, c.batch,
@@ -594,6 +662,8 @@ int run_backward(bspk_adjoint *h, void *dw, void *dw_in, cudaStream_t st) {
 }  // namespace
 
 extern "C" {
+
+int bspk_adjoint_ctas_per_trial(const bspk_adjoint *h) { return h ? h->split : 0; }
 
 int bspk_adjoint_create(const bspk_adjoint_config *cfg, const int64_t *row_ptr, const int32_t *col,
                         int64_t nnz, bspk_adjoint **out) {
@@ -627,7 +697,17 @@ int bspk_adjoint_create(const bspk_adjoint_config *cfg, const int64_t *row_ptr, 
                              c.n_readout > 0 ? 2.0 / denom : 0.0, c.slope, 0.5 * c.slope, 0.0,
                              static_cast<double>(pc.ref_count)};
     for (int i = 0; i < 16; ++i) h->coef[i] = coef[i];
-    h->threads = std::min(1024, std::max(32, (c.n + 31) / 32 * 32));
+    // Two CTAs per trial (a cluster sharing its spike and adjoint vectors
+    // through distributed shared memory) while the batch leaves every trial
+    // a pair of SMs; the readouts must lie in the first half.
+    {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 0;
+        h->split = (2 * c.batch <= sms && c.n >= 64 && c.n_readout <= c.n / 2) ? 2 : 1;
+    }
+    const int per_cta = (c.n + h->split - 1) / h->split;
+    h->threads = std::min(1024, std::max(32, (per_cta + 31) / 32 * 32));
     h->smem = adj_smem_bytes(c.n, c.n_readout, c.n_in, h->elt);
     if (h->smem > 220 * 1024) {
         delete h;

@@ -326,6 +326,11 @@ typedef struct bspk_adjoint bspk_adjoint;
 int bspk_adjoint_create(const bspk_adjoint_config *cfg, const int64_t *row_ptr,
                         const int32_t *col, int64_t nnz, bspk_adjoint **out);
 int bspk_adjoint_destroy(bspk_adjoint *adj);
+/* CTAs per trial of the forward and adjoint kernels: 1, or 2 as a
+ * thread-block cluster that splits a trial's neurons in half (chosen at
+ * create when the batch leaves each trial two SMs, n >= 64 and the readouts
+ * lie in the first half).  Both give bit-identical results. */
+int bspk_adjoint_ctas_per_trial(const bspk_adjoint *adj);
 int bspk_adjoint_forward(bspk_adjoint *adj, const void *w, const void *w_in,
                          const uint8_t *inputs, const void *targets, double *loss,
                          int64_t *n_spikes, void *stream);

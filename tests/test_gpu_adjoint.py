@@ -30,10 +30,12 @@ def _small(relaxed=False, detach=False, t_ref=2.0, seed=3, n_steps=120):
                      detach_reset=detach, params=params, w_in_scale=900.0, seed=seed)
 
 
-def _gpu(T, precision=64, ckpt=50):
+def _gpu(T, precision=64, ckpt=50, split=None):
     from brainpy.state_b200.autograd import LifAdjoint
     dt = torch.float64 if precision == 64 else torch.float32
     adj = LifAdjoint(T["cfg"], T["row_ptr"], T["col"], precision=precision, ckpt_every=ckpt)
+    if split is not None:
+        assert adj.ctas_per_trial == split
     w = torch.tensor(T["w"], dtype=dt, device="cuda")
     wi = torch.tensor(T["w_in"], dtype=dt, device="cuda")
     inp = torch.tensor(T["inputs"], dtype=torch.uint8, device="cuda")
@@ -57,6 +59,25 @@ def test_fp64_adjoint_bitwise_matches_oracle(oracle, relaxed, detach):
     assert gL == L
     np.testing.assert_array_equal(gdw, dw)
     np.testing.assert_array_equal(gdwi, dwi)
+
+
+@pytest.mark.parametrize("relaxed", [False, True])
+def test_fp64_adjoint_two_cta_clusters_match_oracle(oracle, relaxed):
+    """A network of 150 neurons: each trial runs on a cluster of two CTAs that
+    own 75 neurons each and exchange spike and adjoint vectors through
+    distributed shared memory; still bit-identical to the oracle."""
+    params = [-70.0, 250.0, 10.0, 2.0, -55.0, -70.0, 2.0, 2.0, 0.0]
+    T = make_task(n_exc=120, n_inh=30, n_in=20, batch=3, n_steps=120, relaxed=relaxed,
+                  params=params, w_in_scale=900.0, seed=5)
+    L, dw, dwi, nsp = oracle.lif_bptt(T["cfg"], T["row_ptr"], T["col"], T["w"], T["w_in"],
+                                      T["inputs"], T["targets"])
+    gL, gdw, gdwi, gnsp = _gpu(T, split=2)
+    assert nsp > 0 and gnsp == nsp
+    assert gL == L
+    np.testing.assert_array_equal(gdw, dw)
+    np.testing.assert_array_equal(gdwi, dwi)
+    # the small network keeps one CTA per trial
+    assert _gpu(_small(), split=1)[3] > 0
 
 
 def test_checkpoint_spacing_is_invisible():
