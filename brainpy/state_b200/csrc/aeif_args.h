@@ -43,6 +43,7 @@ struct StepArgs {
     unsigned long long *rk_iters;
     int *err;
     int static_chunks;  // edge work items per row of the widest static projection
+    int n_counters;     // per-step counters at step_nspk (zeroed at the end of each step)
 };
 
 // One plastic projection (pair STDP, eager substrate).

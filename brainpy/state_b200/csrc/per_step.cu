@@ -429,10 +429,21 @@ __global__ void __launch_bounds__(256) k_deliver_static(const StepArgs<Real> a) 
                       w[u]);
         }
     }
-}
-
-__global__ void k_step_end(int64_t *step_ptr) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) *step_ptr += 1;
+    // End of the step, by the last block to finish: zero the step's counters
+    // (spike count, STDP list lengths; counter 1 is this arrival count) and
+    // advance the device step.  Every block read the step and the spike
+    // count before arriving here, and every other kernel of the step ran
+    // before this one.
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        int *ctr = a.step_nspk;
+        if (atomicAdd(ctr + 1, 1) == static_cast<int>(gridDim.x) - 1) {
+            __threadfence();
+            for (int i = 0; i < a.n_counters; ++i) ctr[i] = 0;
+            *a.step_ptr = n + 1;
+        }
+    }
 }
 
 // STDP 1: traces decay-then-add (event_plastic.py:390-420); lists of pres
@@ -624,6 +635,7 @@ StepArgs<Real> step_args(bspk_plan *p, int64_t *step_ptr) {
     for (const Proj &J : p->projs)
         if (!J.plastic && J.max_out > max_out) max_out = J.max_out;
     a.static_chunks = chunks_of(max_out);
+    a.n_counters = p->n_step_counters;
     return a;
 }
 
@@ -683,11 +695,12 @@ std::vector<StdpDev> stdp_descs(bspk_plan *p) {
     return v;
 }
 
+// One step: the STDP kernels of each plastic projection, the neuron update,
+// then static delivery, whose last block also closes the step (counters and
+// step counter), so a step is 2 + 3 n_plastic launches.
 template <typename Real>
 cudaError_t enqueue_step(bspk_plan *p, const StepArgs<Real> &a, const std::vector<StdpDev> &sd,
                          cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(p->d_step_counters, 0, sizeof(int) * p->n_step_counters, st);
-    if (e != cudaSuccess) return e;
     for (const StdpDev &s : sd) {
         const int nmax = s.n_pre > s.n_post ? s.n_pre : s.n_post;
         k_stdp_traces<<<(nmax + 255) / 256, 256, 0, st>>>(s, a.hist, a.step_ptr);
@@ -703,17 +716,17 @@ cudaError_t enqueue_step(bspk_plan *p, const StepArgs<Real> &a, const std::vecto
     else if (a.model == 4) k_neuron_step<Real, 4><<<nb, 128, 0, st>>>(a, dt);
     else k_neuron_step<Real, 5><<<nb, 128, 0, st>>>(a, dt);
     k_deliver_static<Real><<<p->sm_count * 4, 256, 0, st>>>(a);
-    k_step_end<<<1, 32, 0, st>>>(a.step_ptr);
     return cudaGetLastError();
 }
 
 template <typename Real>
 int run_typed(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
     BSPK_CUDA(cudaMemcpyAsync(p->d_step_ptr, &p->step, sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    BSPK_CUDA(cudaMemsetAsync(p->d_step_counters, 0, sizeof(int) * p->n_step_counters, st));
     const StepArgs<Real> a = step_args<Real>(p, p->d_step_ptr);
     const std::vector<StdpDev> sd = stdp_descs(p);
     constexpr int64_t kChunk = 32;
-    const int kernels_per_step = 3 + 3 * static_cast<int>(sd.size());
+    const int kernels_per_step = 2 + 3 * static_cast<int>(sd.size());
     int64_t done = 0;
     if (n_steps >= kChunk) {
         // capture kChunk steps once per run (the arguments embed this run's
