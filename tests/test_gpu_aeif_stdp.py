@@ -90,12 +90,21 @@ def test_aeif_fp32_rate_close_to_oracle(oracle):
 
 
 def test_stdp_network_fp64_matches_oracle(oracle):
-    rng = np.random.default_rng(9)
+    _stdp_parity(oracle, 200, 50, 20, 5, 20.68, seed=9)
+
+
+def test_stdp_rows_wider_than_one_work_item_match_oracle(oracle):
+    """In- and out-degrees of about 300 plastic edges: every STDP row spans
+    two 256-edge work items of the facilitation and depression kernels."""
+    _stdp_parity(oracle, 320, 80, 300, 75, 20.68 * 20 / 300, seed=12, min_rows=257)
+
+
+def _stdp_parity(oracle, NE, NI, KE, KI, J, seed, min_rows=0):
+    rng = np.random.default_rng(seed)
     params = [0.0, 250.0, 20.0, 2.0, 20.0, 10.0, 0.5, 0.5, 0.0, -math.inf]
-    rec = np.arange(0, 250, 5)
-    NE, NI = 200, 50
+    rec = np.arange(0, NE + NI, 5)
     pieces = []
-    for pre, K, w in ((0, 20, 20.68), (1, 5, -103.4)):
+    for pre, K, w in ((0, KE, J), (1, KI, -5.0 * J)):
         for post in (0, 1):
             n_pre, n_post = (NE if pre == 0 else NI), (NE if post == 0 else NI)
             pieces.append((pre, post) + random_csr(rng, n_pre, n_post, K, w, 15))
@@ -111,9 +120,9 @@ def test_stdp_network_fp64_matches_oracle(oracle):
             ids.append((s.add_csr if is_plan else s.add_proj)(pre, post, indptr, idx, w, d))
         # E -> E plastic (tau 20 ms, lambda 0.05, Wmax 3 x initial)
         if is_plan:
-            s.attach_stdp(ids[0], 20.0, 20.0, 0.05, 1.0, 1.0, 1.0, 3 * 20.68)
+            s.attach_stdp(ids[0], 20.0, 20.0, 0.05, 1.0, 1.0, 1.0, 3 * J)
         else:
-            s.set_stdp(ids[0], 20.0, 20.0, 0.05, 1.0, 1.0, 1.0, 3 * 20.68)
+            s.set_stdp(ids[0], 20.0, 20.0, 0.05, 1.0, 1.0, 1.0, 3 * J)
         return ids
 
     pl = _lib.Plan(0.1, precision=64)
@@ -133,10 +142,15 @@ def test_stdp_network_fp64_matches_oracle(oracle):
     assert len(ost) > 0
     assert set(zip(st.tolist(), g.tolist())) == set(zip(ost.tolist(), og.tolist()))
     np.testing.assert_allclose(pl.v_trace(), ov, rtol=0, atol=1e-9)
+    indptr_ee = pieces[0][2]
     E = pieces[0][3].size
+    if min_rows:
+        # widest out-row and in-column of the plastic projection
+        assert np.diff(indptr_ee).max() >= min_rows
+        assert np.bincount(pieces[0][3], minlength=NE).max() >= min_rows
     w_gpu = pl.weights(ids[0])
     w_cpu = sim.weights(0 + 2, E)  # oracle ids count drives too
-    assert np.any(w_cpu != 20.68)
+    assert np.any(w_cpu != J)
     np.testing.assert_allclose(w_gpu, w_cpu, rtol=1e-12, atol=0)
 
 

@@ -23,7 +23,7 @@ DRIVE_NS = {"iaf_cond_exp": 4.0, "iaf_cond_alpha": 2.0}  # about 100 Hz in both 
 NE, NI = 160, 40
 
 
-def _net(target, is_plan, model, seed=4):
+def _net(target, is_plan, model, seed=4, K=(16, 4), w=(1.0, 3.0)):
     """Excitatory projections into receptor 0 (g_ex), inhibitory into 1 (g_in)."""
     rng = np.random.default_rng(seed)
     p = [COND[k] for k in COND_ORDER]
@@ -33,25 +33,25 @@ def _net(target, is_plan, model, seed=4):
     target.add_pop(NI, p)
     add_drive(0, 9000.0, DRIVE_NS[model], 5, 31, receptor=0)
     add_drive(1, 9000.0, DRIVE_NS[model], 5, 32, receptor=0)
-    for pre, K, w, rec in ((0, 16, 1.0, 0), (1, 4, 3.0, 1)):
+    for pre, Kp, wp, rec in ((0, K[0], w[0], 0), (1, K[1], w[1], 1)):
         for post in (0, 1):
             n_pre, n_post = (NE if pre == 0 else NI), (NE if post == 0 else NI)
-            indptr, idx, ww, d = random_csr(rng, n_pre, n_post, K, w,
-                                            rng.integers(5, 20, n_post * K))
+            indptr, idx, ww, d = random_csr(rng, n_pre, n_post, Kp, wp,
+                                            rng.integers(5, 20, n_post * Kp))
             add_proj(pre, post, indptr, idx, ww, d, rec)
     return rng.uniform(-70.0, -55.0, NE + NI)
 
 
-def _pair(oracle, model, precision, rec=None):
+def _pair(oracle, model, precision, rec=None, **net):
     pl = _lib.Plan(0.1, model, precision=precision)
-    v0 = _net(pl, True, model)
+    v0 = _net(pl, True, model, **net)
     if rec is not None:
         pl.record_v(rec)
     pl.upload()
     pl.set_state(0, "V_m", v0[:NE])
     pl.set_state(1, "V_m", v0[NE:])
     sim = oracle.OracleSim(0.1, model)
-    _net(sim, False, model)
+    _net(sim, False, model, **net)
     if rec is not None:
         sim.record_v(rec)
     sim.set_state(0, "V_m", v0[:NE])
@@ -79,6 +79,21 @@ def test_cond_network_fp64_matches_oracle(oracle, model):
             np.testing.assert_allclose(pl.get_state(pop, name), sim.get_state(pop, name, n),
                                        rtol=0, atol=2e-6, err_msg=name)
         np.testing.assert_array_equal(pl.get_state(pop, "r"), sim.get_state(pop, "r", n))
+
+
+def test_static_rows_wider_than_one_work_item_match_oracle(oracle):
+    """In-degrees of 120 excitatory and 80 inhibitory inputs: the I -> E rows
+    average 80 * 160 / 40 = 320 edges per pre neuron, so static delivery
+    splits them into two 256-edge work items."""
+    model = "iaf_cond_alpha"
+    pl, sim = _pair(oracle, model, 64, rec=np.arange(0, NE + NI, 7), K=(120, 80),
+                    w=(16.0 / 120, 12.0 / 80))
+    pl.run(200)
+    st, g = pl.spikes()
+    ost, og, ov = sim.run(200)
+    assert len(ost) > 0
+    assert set(zip(st.tolist(), g.tolist())) == set(zip(ost.tolist(), og.tolist()))
+    np.testing.assert_allclose(pl.v_trace(), ov, rtol=0, atol=2e-6)
 
 
 @pytest.mark.parametrize("model", ["iaf_cond_exp", "iaf_cond_alpha"])
