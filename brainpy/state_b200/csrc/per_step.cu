@@ -128,7 +128,7 @@ __device__ __forceinline__ void iaf_cond_vf(const PopCoef<Real> &c, int r, Real 
 // err^(-q) of the step-size factor 0.9 (1 / err)^q, as exp(-q log err): no
 // division and a shorter chain than pow on the substep's critical path.  An
 // FP32 state takes it in FP32: the factor only sizes the next trial step,
-// whose error the FP64 norm then judges, so acceptance stays FP64.
+// whose error the FP64 norm then tests, so acceptance stays FP64.
 template <typename Real>
 __device__ __forceinline__ double err_pow(double err, double q) {
     if constexpr (sizeof(Real) == 4)
