@@ -135,6 +135,35 @@ __global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64
     const int p = find_pop2(s_off, a.npop, g);
     const uint32_t idx = static_cast<uint32_t>(g - s_off[p]);
     const int q0 = a.pop_drive_ptr[p], q1 = a.pop_drive_ptr[p + 1];
+    if (q1 - q0 == 1) {
+        // one drive (the common case): its descriptor and the first CDF
+        // thresholds in registers for the whole run of steps.  The count is
+        // the number of leading thresholds below the draw, so the first four
+        // compares decide it unless it is 4 or more.
+        const DriveDev d = a.drives[a.pop_drive_list[q0]];
+        const uint64_t *T = a.cdf + d.cdf_off;
+        constexpr uint64_t kNone = ~0ull;  // no threshold: never below a 53-bit draw
+        const uint64_t T0 = d.cdf_n > 0 ? T[0] : kNone, T1 = d.cdf_n > 1 ? T[1] : kNone,
+                       T2 = d.cdf_n > 2 ? T[2] : kNone, T3 = d.cdf_n > 3 ? T[3] : kNone;
+        const Real wd = static_cast<Real>(d.weight);
+        for (int k = k0; k < k1; ++k) {
+            const int64_t se = m0 + k - d.lag;
+            Real add = Real(0);
+            if (d.tmin < se && se <= d.tmax) {
+                const uint64_t u = bits53(d.seed, 0u, static_cast<uint32_t>(se), idx);
+                int cnt;
+                if (u > T3) {
+                    cnt = 4;
+                    while (cnt < d.cdf_n && u > T[cnt]) ++cnt;
+                } else {
+                    cnt = (u > T0) + (u > T1) + (u > T2);
+                }
+                add += static_cast<Real>(cnt) * wd;  // as the general path: 0 + count * weight
+            }
+            out[static_cast<int64_t>(k) * a.N + g] = add;
+        }
+        return;
+    }
     for (int k = k0; k < k1; ++k) {
         const int64_t m = m0 + k;
         Real add = Real(0);
