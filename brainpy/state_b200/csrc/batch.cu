@@ -353,6 +353,39 @@ __global__ void __launch_bounds__(256) k_batch_drive_fill(const BatchArgs<Real> 
     while (pop + 1 < I.npop && I.pop_off[pop + 1] <= li) ++pop;
     const uint32_t idx = static_cast<uint32_t>(li - I.pop_off[pop]);
     const int k0 = blockIdx.y * spb, k1 = min(n, k0 + spb);
+    int nmatch = 0, dsel = 0;
+    for (int d = 0; d < I.ndrive; ++d)
+        if (a.drives[I.drive0 + d].pop == pop) {
+            ++nmatch;
+            dsel = d;
+        }
+    if (nmatch == 1) {
+        // one drive for this population (the sweep's case): descriptor and
+        // first CDF thresholds in registers, counts as in the general path
+        const DriveDev D = a.drives[I.drive0 + dsel];
+        const uint64_t *T = a.cdf + I.cdf0 + D.cdf_off;
+        constexpr uint64_t kNone = ~0ull;  // no threshold: never below a 53-bit draw
+        const uint64_t T0 = D.cdf_n > 0 ? T[0] : kNone, T1 = D.cdf_n > 1 ? T[1] : kNone,
+                       T2 = D.cdf_n > 2 ? T[2] : kNone, T3 = D.cdf_n > 3 ? T[3] : kNone;
+        const Real wd = static_cast<Real>(D.weight);
+        for (int k = k0; k < k1; ++k) {
+            const int64_t se = m0 + k - D.lag;
+            Real add = Real(0);
+            if (D.tmin < se && se <= D.tmax) {
+                const uint64_t u = bits53(D.seed, 0u, static_cast<uint32_t>(se), idx);
+                int cnt;
+                if (u > T3) {
+                    cnt = 4;
+                    while (cnt < D.cdf_n && u > T[cnt]) ++cnt;
+                } else {
+                    cnt = (u > T0) + (u > T1) + (u > T2);
+                }
+                add += static_cast<Real>(cnt) * wd;
+            }
+            out[static_cast<int64_t>(k) * a.n_total + g] = add;
+        }
+        return;
+    }
     for (int k = k0; k < k1; ++k) {
         const int64_t m = m0 + k;
         Real add = Real(0);
