@@ -701,9 +701,9 @@ int bspk_adjoint_create(const bspk_adjoint_config *cfg, const int64_t *row_ptr, 
     // through distributed shared memory) while the batch leaves every trial
     // a pair of SMs; the readouts must lie in the first half.
     {
-        int dev = 0, sms = 0;
-        cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 0;
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device) != cudaSuccess)
+            sms = 0;
         h->split = (2 * c.batch <= sms && c.n >= 64 && c.n_readout <= c.n / 2) ? 2 : 1;
     }
     const int per_cta = (c.n + h->split - 1) / h->split;
