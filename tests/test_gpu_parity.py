@@ -179,9 +179,8 @@ def test_tiled_fp32_is_deterministic():
 
 
 def test_tiled_large_tiles_drive_pass(oracle):
-    """30 000 neurons: tiles of 203 neurons leave too few idle threads, so
-    the drive comes from the separate drive pass (and the CSR bounds from
-    global memory); spikes must match the oracle."""
+    """30 000 neurons: tiles of 203 neurons, with the CSR bounds read from
+    global memory instead of shared memory; spikes must match the oracle."""
     net = Net(NE=24000, NI=6000, CE=20, CI=5, J=60.0, delay=15, seed=9)
     rec = np.arange(0, 30000, 997)
     pl = net.to_plan(precision=64, semantics=1, rec=rec)
@@ -190,6 +189,25 @@ def test_tiled_large_tiles_drive_pass(oracle):
     st, g = pl.spikes()
     ost, og, ov = sim.run(60)
     assert len(st) > 0
+    assert _raster(st, g) == _raster(ost, og)
+    np.testing.assert_allclose(pl.v_trace(), ov, rtol=0, atol=1e-9)
+
+
+def test_tiled_drive_pass_general_and_register_paths(oracle):
+    """The drive pass's two paths on the tiled kernel: E has one drive (the
+    register path), I two drives of different rates, weights and delays
+    (the general loop over a population's drives).  Spikes and V_m must
+    match the oracle."""
+    net = Net(NE=800, NI=200, CE=40, CI=10, J=20.68, delay=15, seed=21)
+    net.drives = [(0, 17789.0, 20.68, 15, 101), (1, 17789.0, 20.68, 15, 102),
+                  (1, 2000.0, 60.0, 12, 103)]
+    rec = np.arange(0, 1000, 37)
+    pl = net.to_plan(precision=64, semantics=1, rec=rec)
+    sim = net.to_oracle(oracle, semantics=1, rec=rec)
+    pl.run(400)
+    st, g = pl.spikes()
+    ost, og, ov = sim.run(400)
+    assert len(st) > 0 and np.any(g >= 800)
     assert _raster(st, g) == _raster(ost, og)
     np.testing.assert_allclose(pl.v_trace(), ov, rtol=0, atol=1e-9)
 
