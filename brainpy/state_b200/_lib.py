@@ -74,6 +74,12 @@ def lib():
                                                        C.POINTER(C.c_int)]),
             "bspk_drive_add_poisson": (C.c_int, [vp, C.c_int, dbl, dbl, C.c_int, u32, i64, i64,
                                                  C.c_int, C.POINTER(C.c_int)]),
+            "bspk_drive_add_poisson_keyed": (C.c_int, [vp, C.c_int, dbl, dbl, C.c_int, vp, i64,
+                                                       i64, i64, C.c_int, C.POINTER(C.c_int)]),
+            "bspk_jax_fold_in": (C.c_int, [vp, u32, vp]),
+            "bspk_jax_uniform": (C.c_int, [vp, i64, C.c_int, dbl, dbl, vp]),
+            "bspk_jax_normal": (C.c_int, [vp, i64, C.c_int, vp]),
+            "bspk_kernel_poisson_table": (C.c_int, [dbl, dbl, C.c_int, vp, C.POINTER(C.c_int)]),
             "bspk_stdp_attach": (C.c_int, [vp, C.c_int, C.POINTER(StdpParams)]),
             "bspk_stdp_triplet_attach": (C.c_int, [vp, C.c_int, C.POINTER(StdpTripletParams)]),
             "bspk_proj_csr_get": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
@@ -93,6 +99,7 @@ def lib():
             "bspk_state_get": (C.c_int, [vp, C.c_int, C.c_char_p, vp]),
             "bspk_state_set": (C.c_int, [vp, C.c_int, C.c_char_p, vp]),
             "bspk_step_count": (i64, [vp]),
+            "bspk_plan_engine": (C.c_char_p, [vp]),
             "bspk_last_kernel_time": (C.c_int, [vp, C.POINTER(dbl), C.POINTER(i64)]),
             "bspk_rk_substeps": (C.c_int, [vp, C.POINTER(i64)]),
             "bspk_checkpoint_size": (C.c_int, [vp, C.POINTER(i64)]),
@@ -161,6 +168,44 @@ def kernel_fixed_indegree(seed, proj_id, parts, n_pre, self_pos, K):
                                           ptr(sp) if sp is not None else None, int(n_pre), int(K),
                                           ptr(out)))
     return out[:n_post * int(K)].reshape(n_post, int(K)).astype(np.int64)
+
+
+def _key(key):
+    k = np.ascontiguousarray(np.asarray(key, dtype=np.uint32).reshape(2))
+    return k
+
+
+def jax_fold_in(key, data):
+    """jax.random.fold_in(key, data) of a raw uint32[2] key."""
+    out = np.zeros(2, np.uint32)
+    check(lib().bspk_jax_fold_in(ptr(_key(key)), int(data) & 0xFFFFFFFF, ptr(out)))
+    return out
+
+
+def jax_uniform(key, n, bits=32, lo=0.0, hi=1.0):
+    """jax.random.uniform(key, (n,), float32 / float64, lo, hi), widened to
+    float64 (the float32 values are exact in it)."""
+    out = np.zeros(int(n), np.float64)
+    check(lib().bspk_jax_uniform(ptr(_key(key)), int(n), int(bits), float(lo), float(hi),
+                                 ptr(out)))
+    return out
+
+
+def jax_normal(key, n, bits=32):
+    """jax.random.normal(key, (n,), float32 / float64), widened to float64."""
+    out = np.zeros(int(n), np.float64)
+    check(lib().bspk_jax_normal(ptr(_key(key)), int(n), int(bits), ptr(out)))
+    return out
+
+
+def kernel_poisson_table(rate_hz, dt_ms):
+    """Integer thresholds of the kernel path's float32 Poisson CDF inversion."""
+    n = C.c_int()
+    check(lib().bspk_kernel_poisson_table(float(rate_hz), float(dt_ms), 0, None, C.byref(n)))
+    out = np.zeros(n.value, np.uint64)
+    check(lib().bspk_kernel_poisson_table(float(rate_hz), float(dt_ms), n.value, ptr(out),
+                                          C.byref(n)))
+    return out
 
 
 def check(rc):
@@ -241,6 +286,18 @@ class Plan:
                                              int(delay_steps), int(seed) & 0xFFFFFFFF,
                                              int(t_min), int(t_max), int(receptor),
                                              C.byref(out)))
+        return out.value
+
+    def add_poisson_keyed(self, post, rate_hz, weight, delay_steps, obj_key, unit_off=0,
+                          t_min=0, t_max=2 ** 62, receptor=0):
+        """Poisson drive on the reference kernel path's block-key stream of
+        the device population with object key ``obj_key`` (uint32[2]); unit
+        ``unit_off + i`` drives neuron i of ``post``."""
+        out = C.c_int()
+        check(self._L.bspk_drive_add_poisson_keyed(
+            self._h, int(post), float(rate_hz), float(weight), int(delay_steps),
+            ptr(_key(obj_key)), int(unit_off), int(t_min), int(t_max), int(receptor),
+            C.byref(out)))
         return out.value
 
     def csr(self, proj):
@@ -341,6 +398,12 @@ class Plan:
     @property
     def step(self):
         return self._L.bspk_step_count(self._h)
+
+    @property
+    def engine(self):
+        """Kernel family of the uploaded plan: 'tiled', 'global_ring', 'exact'
+        or 'per_step'."""
+        return self._L.bspk_plan_engine(self._h).decode()
 
     def kernel_time(self):
         ms, n = C.c_double(), C.c_int64()

@@ -91,6 +91,66 @@ def build_plan(order=2500, precision=32, delay_steps=(10, 30), noise_delay=15, s
     return pl, p
 
 
+# ------------------------------------------------- kernel-path network
+
+KERNEL_NAMES = dict(E="E", I="I", noise="noise", noise_proj="noise_EI", e_proj="E_EI",
+                    i_proj="I_EI")
+
+
+def build_kernel_network(order=2500, seed=1234, delay=(1.0, 3.0), noise_delay=1.5, V_reset=10.0,
+                         v_init=(0.0, 20.0), g=5.0, eta=2.0, n_rec=0, record_v=False):
+    """The Brunel network as the reference's kernel path builds it
+    (``_kernel/validation/brunel.py:59-139``, used by
+    ``benchmarks/k1a4_delays.py --net brunel``): populations 'E', 'I' and a
+    'noise' poisson_generator of one unit per neuron connected one_to_one onto
+    E + I (port 'ex', 1.5 ms); 'E_EI' = fixed_indegree(CE) from E onto E + I
+    (port 'ex') and 'I_EI' = fixed_indegree(CI) from I (port 'in_') with
+    per-edge delays ``Uniform(delay[0] ms, delay[1] ms)`` rounded to the step
+    grid (NEST rounding), or a fixed delay when ``delay`` is a number.  The
+    neuron parameters are the configuration's (V_reset 10 mV, V_m initialised
+    ``Uniform(0, 20) mV``); every random draw comes from the kernel's streams
+    for ``seed``.  Returns (Network, params, observers)."""
+    from .kernel import Network, fixed_indegree, iaf_psc_alpha, one_to_one, poisson_generator
+    from .streams import Uniform
+    from .units import Hz, mV, ms, pA, pF
+    p = brunel_params(order, g=g, eta=eta, V_reset=V_reset)
+    npar = dict(C_m=250.0 * pF, tau_m=20.0 * ms, tau_syn_ex=0.5 * ms, tau_syn_in=0.5 * ms,
+                t_ref=2.0 * ms, E_L=0.0 * mV, V_reset=V_reset * mV, V_th=20.0 * mV)
+    init = dict(V_m=Uniform(v_init[0] * mV, v_init[1] * mV)) if v_init is not None else None
+    net = Network(dt=0.1 * ms, seed=seed)
+    E = net.add(iaf_psc_alpha, p["NE"], params=npar, init=init, name=KERNEL_NAMES["E"])
+    I = net.add(iaf_psc_alpha, p["NI"], params=npar, init=init, name=KERNEL_NAMES["I"])
+    noise = net.add(poisson_generator, p["NE"] + p["NI"], params=dict(rate=p["rate"] * Hz),
+                    name=KERNEL_NAMES["noise"])
+    net.connect(noise, E + I, one_to_one(), port="ex", weight=p["J_ex"] * pA,
+                delay=noise_delay * ms, name=KERNEL_NAMES["noise_proj"])
+    d = Uniform(delay[0] * ms, delay[1] * ms) if isinstance(delay, tuple) else delay * ms
+    net.connect(E, E + I, fixed_indegree(p["CE"]), port="ex", weight=p["J_ex"] * pA, delay=d,
+                name=KERNEL_NAMES["e_proj"])
+    net.connect(I, E + I, fixed_indegree(p["CI"]), port="in_", weight=p["J_in"] * pA, delay=d,
+                name=KERNEL_NAMES["i_proj"])
+    obs = {}
+    if n_rec:
+        obs["spikes"] = net.observe(E + I, "spike", name="rec_spikes")
+    if record_v:
+        step = max(1, p["NE"] // 100)
+        obs["V_m"] = net.observe(E[::step][:100], "V_m", name="rec_V")
+    return net, p, obs
+
+
+def kernel_out_degree(prog):
+    """Out-degree of every library neuron of a compiled kernel network."""
+    deg = np.zeros(prog.n_lib, np.int64)
+    offs = {}
+    g0 = 0
+    for q, n in enumerate(prog.plan.pop_sizes):
+        offs[q] = g0
+        g0 += n
+    for a, _, indptr, _, _, _, _ in prog.realised:
+        deg[offs[a]:offs[a] + indptr.size - 1] += np.diff(indptr)
+    return deg
+
+
 # ------------------------------------------------------------ sweep batches
 
 def sweep_instances(n=256, seed=1234, ne_range=(500, 8000), g_range=(3.0, 8.0),

@@ -34,10 +34,11 @@ SOURCES = {
     "adjoint.cu": ["-fmad=false"],
     "checkpoint.cpp": [],
     "xla_ffi.cpp": [],
+    "jax_rng.cpp": [],
 }
 HEADERS = ["common.cuh", "device_types.h", "lif_args.h", "aeif_args.h", "stdp_args.h",
            "host_rng.h", "batch_args.h", "plan_internal.h", "conn_gen.h", "conn_gen.cuh",
-           "coef_cast.h"]
+           "coef_cast.h", "jax_rng.h"]
 
 
 def _mtime(p):

@@ -80,6 +80,13 @@ struct DriveDev {
     int receptor;
     double weight;
     int64_t tmin, tmax;
+    // stream: 0 = the library's counter stream (53-bit thresholds);
+    // 1 = the reference kernel path's block-key stream (23-bit thresholds)
+    // of the device population with object key (key0, key1), whose unit
+    // unit_off + i drives neuron i of `pop`
+    int kind;
+    uint32_t key0, key1;
+    int64_t unit_off;
 };
 
 // One projection (CSR over the pre population's local indices).

@@ -46,6 +46,7 @@ struct LifArgs {
 // word = post_in_tile | lag << 16 | projection << 24); per-window spike
 // records list[kRecBufs][G][kRecWords] (tagged count word + kRecInline
 // tagged entries) with an overflow area ovf[kRecBufs][G][list_cap];
+// (with separate receptor ports, bit 15 of the edge word is the port);
 // per-CTA spike-record counts rec_count[G] (running across the launches of
 // one run); the Poisson drive of every (step, neuron) of the launch, drawn
 // by a separate kernel, drive[(step - drive_step0) * N + neuron].
@@ -89,6 +90,9 @@ struct TiledArgs {
     // test hook: CTA hold_cta does not publish the header of its record of
     // window hold_win (-1: none), so every bounded wait for it runs out
     int hold_cta, hold_win;
+    // 1: the receptor ports 'ex' and 'in_' have rings of their own (edge
+    // word bit 15 = port; drives feed 'ex'); 0: one ring, sum split by sign
+    int ports;
 };
 
 struct TiledLayout {
@@ -117,7 +121,9 @@ cudaError_t launch_lif_tiled(const LifArgs<Real> &a, const TiledArgs<Real> &t2, 
 template <typename Real>
 cudaError_t launch_drive_fill(const LifArgs<Real> &a, int64_t m0, int n, Real *out,
                               cudaStream_t st);
-size_t lif_tiled_smem(int tile, int L, int W, int N, int npop, int nproj, bool dbl, bool smem_ptr);
+// ports: two rings ('ex', 'in_') instead of one
+size_t lif_tiled_smem(int tile, int L, int W, int N, int npop, int nproj, bool dbl, bool smem_ptr,
+                      bool ports = false);
 // Recorded spikes of the tiled kernel's per-CTA regions into one list.
 cudaError_t launch_compact_spikes(int G, int64_t region, const long long *rec_count,
                                   const int64_t *in_step, const int32_t *in_gid, int64_t *out_step,

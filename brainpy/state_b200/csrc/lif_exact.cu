@@ -69,8 +69,8 @@ __global__ void __launch_bounds__(256) k_lif_exact(const LifArgs<double> a) {
                             const int64_t se = n0 + k - d.lag;
                             double y = 0.0;
                             if (d.tmin < se && se <= d.tmax) {
-                                const uint64_t u = bits53(d.seed, 0u, static_cast<uint32_t>(se),
-                                                           static_cast<uint32_t>(gl));
+                                const uint64_t u = drive_draw(d, static_cast<uint32_t>(se),
+                                                              static_cast<uint32_t>(gl));
                                 const int cnt = poisson_from_table(s_cdf + d.cdf_off, d.cdf_n, u);
                                 y = static_cast<double>(cnt) * d.weight;
                             }
@@ -169,13 +169,16 @@ cudaError_t launch_lif_exact(const LifArgs<double> &a, int grid, int block, cuda
 // for one iaf_psc_alpha population (one Poisson drive, then one recurrent
 // projection) without a plan and without any device allocation.  It is for
 // callers that cannot call cudaMalloc: code running inside another
-// framework's memory pool or allocator hooks (an XLA custom call, a CUDA
-// graph being captured, a plugin whose host forbids allocations).  The
-// caller passes every input and output buffer; everything else the kernel
-// needs lives in one file-scope device array of fixed size (parameter
-// tables, Poisson CDF, 64-step spike-history words, barrier counter, error
-// flag, spike counter), so at most kNoAllocMaxNeurons neurons and a CDF of
-// kNoAllocMaxCdf entries.
+// framework's memory pool or allocator hooks (an XLA custom call, a plugin
+// whose host forbids device allocations).  The caller passes every input and
+// output buffer; everything else the kernel needs lives in one file-scope
+// device array of fixed size (parameter tables, Poisson CDF, 64-step
+// spike-history words, barrier counter, error flag, spike counter), so at
+// most kNoAllocMaxNeurons neurons and a CDF of kNoAllocMaxCdf entries.  The
+// kernel is a cooperative launch of up to 256 threads per CTA, so the
+// network must also fit the CTAs the GPU can hold at once (256 per SM times
+// the SM count on a B200, 37 888 neurons): the call checks that before it
+// launches.
 namespace {
 
 constexpr int kNoAllocMaxNeurons = 1 << 16;
@@ -201,6 +204,17 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocS
 std::mutex g_noalloc_mu;
 void *g_noalloc_addr[256] = {};
 
+// Copies the spike counter and error flag of the scratch array to the
+// caller's outputs; a count above the caller's capacity (entries dropped)
+// turns a zero status into the overflow code.
+__global__ void k_noalloc_finish(const NoAllocScratch *S, int64_t cap, int64_t *count, int *status) {
+    const unsigned long long n = S->spk_count;
+    *count = static_cast<int64_t>(n);
+    int e = S->err;
+    if (e == 0 && n > static_cast<unsigned long long>(cap)) e = bspk::BSPK_DEV_ERR_OVERFLOW;
+    *status = e;
+}
+
 }  // namespace
 
 extern "C" int bspk_iaf_exact_run_noalloc(double dt, const double *params, int n_params, int n,
@@ -214,8 +228,8 @@ extern "C" int bspk_iaf_exact_run_noalloc(double dt, const double *params, int n
                                           int64_t spike_cap, int64_t *spike_count, int *status,
                                           void *stream) {
     using namespace bspk;
-    if (!params || !in_indptr || !state || !refr || !spike_step || !spike_gid || !spike_count ||
-        !status || n <= 0 || n_steps < 0 || spike_cap < 0 || !(dt > 0))
+    if (!params || !in_indptr || !in_edges || !state || !refr || !spike_step || !spike_gid ||
+        !spike_count || !status || n <= 0 || n_steps < 0 || spike_cap < 0 || !(dt > 0))
         return fail(BSPK_ERR_ARG, "bad argument");
     if (n > kNoAllocMaxNeurons)
         return fail(BSPK_ERR_ARG, "no-allocation entry point: more than 65536 neurons");
@@ -247,6 +261,22 @@ extern "C" int bspk_iaf_exact_run_noalloc(double dt, const double *params, int n
         }
         base = g_noalloc_addr[dev];
     }
+    int sm = 0;
+    BSPK_CUDA(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev));
+    int block = ((n + sm - 1) / sm + 31) / 32 * 32;
+    block = block < 64 ? 64 : (block > 256 ? 256 : block);
+    const int grid = (n + block - 1) / block;
+    // every CTA of the cooperative launch must be resident at once
+    int per_sm = 0;
+    BSPK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, k_lif_exact<0>, block,
+        lif_exact_smem(block, 1, 1, 1, static_cast<int>(cdf.size()))));
+    if (static_cast<int64_t>(per_sm) * sm < grid)
+        return fail(BSPK_ERR_UNSUPPORTED,
+                    "no-allocation entry point: " + std::to_string(n) + " neurons need " +
+                        std::to_string(grid) + " co-resident CTAs of " + std::to_string(block) +
+                        " threads; this GPU holds " + std::to_string(per_sm * sm) + " (at most " +
+                        std::to_string(static_cast<int64_t>(per_sm) * sm * 256) + " neurons)");
     NoAllocScratch *S = static_cast<NoAllocScratch *>(base);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
@@ -282,11 +312,6 @@ extern "C" int bspk_iaf_exact_run_noalloc(double dt, const double *params, int n
     // the copies above came from pageable host memory, so they completed
     // before cudaMemcpyAsync returned; the host tables may go out of scope
 
-    int sm = 0;
-    BSPK_CUDA(cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev));
-    int block = ((n + sm - 1) / sm + 31) / 32 * 32;
-    block = block < 64 ? 64 : (block > 256 ? 256 : block);
-    const int grid = (n + block - 1) / block;
     const int max_lag = max_delay_steps + 1, min_lag = min_delay_steps + 1;
     int W = min_lag < kMaxWindow ? min_lag : kMaxWindow;
     if (W > 64 - max_lag) W = 64 - max_lag;
@@ -334,7 +359,7 @@ extern "C" int bspk_iaf_exact_run_noalloc(double dt, const double *params, int n
         if (e != cudaSuccess)
             return fail(BSPK_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
     }
-    BSPK_CUDA(cudaMemcpyAsync(spike_count, &S->spk_count, sizeof(int64_t), cudaMemcpyDeviceToDevice, st));
-    BSPK_CUDA(cudaMemcpyAsync(status, &S->err, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    k_noalloc_finish<<<1, 1, 0, st>>>(S, spike_cap, spike_count, status);
+    BSPK_CUDA(cudaGetLastError());
     return BSPK_OK;
 }

@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(512) k_lif_fast(const LifArgs<Real> a) {
                     if (k < Wk) {
                         const int64_t se = n0 + k - d.lag;
                         if (d.tmin < se && se <= d.tmax) {
-                            const uint64_t u = bits53(d.seed, 0u, static_cast<uint32_t>(se), idx);
+                            const uint64_t u = drive_draw(d, static_cast<uint32_t>(se), idx);
                             const int cnt = poisson_from_table(s_cdf + d.cdf_off, d.cdf_n, u);
                             in[k] += static_cast<Real>(cnt) * w;
                         }

@@ -130,11 +130,69 @@ __global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64
     if (threadIdx.x == 0) s_off[a.npop] = a.N;
     __syncthreads();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= a.N) return;
+    const bool valid = g < a.N;
+    const int gc = valid ? g : a.N - 1;  // a lane beyond the network looks up the last neuron
     const int k0 = blockIdx.y * spb, k1 = min(n, k0 + spb);
-    const int p = find_pop2(s_off, a.npop, g);
-    const uint32_t idx = static_cast<uint32_t>(g - s_off[p]);
+    const int p = find_pop2(s_off, a.npop, gc);
+    const uint32_t idx = static_cast<uint32_t>(gc - s_off[p]);
     const int q0 = a.pop_drive_ptr[p], q1 = a.pop_drive_ptr[p + 1];
+    {
+        // The reference kernel path's stream (kind 1) draws a step's numbers
+        // for a block of 1024 units from one step key, fold(fold(block key,
+        // step), 0): two threefry rounds that every lane of a warp would
+        // repeat.  When all 32 lanes have one such drive with the same block
+        // key, lag and window, lane l derives the step key of step kc + l and
+        // the warp shares the 32 keys by shuffles: one threefry per draw.
+        constexpr unsigned kFull = 0xffffffffu;
+        const bool one = q1 - q0 == 1;
+        DriveDev d{};
+        if (one) d = a.drives[a.pop_drive_list[q0]];
+        const uint64_t unit = static_cast<uint64_t>(d.unit_off) + idx;
+        uint32_t kb0 = d.key0, kb1 = d.key1;
+        const bool keyed = one && d.kind == 1;
+        if (keyed) fold_key(kb0, kb1, static_cast<uint32_t>(unit >> 10));
+        const uint32_t r0 = __shfl_sync(kFull, kb0, 0), r1 = __shfl_sync(kFull, kb1, 0);
+        const int lag0 = __shfl_sync(kFull, d.lag, 0);
+        const long long tmin0 = __shfl_sync(kFull, static_cast<long long>(d.tmin), 0);
+        const long long tmax0 = __shfl_sync(kFull, static_cast<long long>(d.tmax), 0);
+        if (__all_sync(kFull, keyed && kb0 == r0 && kb1 == r1 && d.lag == lag0 &&
+                                  d.tmin == tmin0 && d.tmax == tmax0)) {
+            const int lane = threadIdx.x & 31;
+            const uint64_t *T = a.cdf + d.cdf_off;
+            constexpr uint64_t kNone = ~0ull;
+            const uint64_t T0 = d.cdf_n > 0 ? T[0] : kNone, T1 = d.cdf_n > 1 ? T[1] : kNone,
+                           T2 = d.cdf_n > 2 ? T[2] : kNone, T3 = d.cdf_n > 3 ? T[3] : kNone;
+            const Real wd = static_cast<Real>(d.weight);
+            const uint32_t ln = static_cast<uint32_t>(unit & 1023u);
+            for (int kc = k0; kc < k1; kc += 32) {
+                uint32_t s0 = kb0, s1 = kb1;
+                fold_key(s0, s1, static_cast<uint32_t>(m0 + kc + lane - lag0));
+                fold_key(s0, s1, 0u);
+                const int kend = min(32, k1 - kc);
+                for (int j = 0; j < kend; ++j) {
+                    const uint32_t t0 = __shfl_sync(kFull, s0, j), t1 = __shfl_sync(kFull, s1, j);
+                    const int64_t se = m0 + kc + j - lag0;
+                    Real add = Real(0);
+                    if (tmin0 < se && se <= tmax0) {
+                        uint32_t y0, y1;
+                        threefry2x32(t0, t1, 0u, ln, y0, y1);
+                        const uint64_t u = (y0 ^ y1) >> 9;
+                        int cnt;
+                        if (u > T3) {
+                            cnt = 4;
+                            while (cnt < d.cdf_n && u > T[cnt]) ++cnt;
+                        } else {
+                            cnt = (u > T0) + (u > T1) + (u > T2);
+                        }
+                        add += static_cast<Real>(cnt) * wd;
+                    }
+                    if (valid) out[static_cast<int64_t>(kc + j) * a.N + g] = add;
+                }
+            }
+            return;
+        }
+    }
+    if (!valid) return;
     if (q1 - q0 == 1) {
         // one drive (the common case): its descriptor and the first CDF
         // thresholds in registers for the whole run of steps.  The count is
@@ -150,7 +208,7 @@ __global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64
             const int64_t se = m0 + k - d.lag;
             Real add = Real(0);
             if (d.tmin < se && se <= d.tmax) {
-                const uint64_t u = bits53(d.seed, 0u, static_cast<uint32_t>(se), idx);
+                const uint64_t u = drive_draw(d, static_cast<uint32_t>(se), idx);
                 int cnt;
                 if (u > T3) {
                     cnt = 4;
@@ -171,7 +229,7 @@ __global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64
             const DriveDev &d = a.drives[a.pop_drive_list[q]];
             const int64_t se = m - d.lag;
             if (d.tmin < se && se <= d.tmax) {
-                const uint64_t u = bits53(d.seed, 0u, static_cast<uint32_t>(se), idx);
+                const uint64_t u = drive_draw(d, static_cast<uint32_t>(se), idx);
                 const int cnt = poisson_from_table(a.cdf + d.cdf_off, d.cdf_n, u);
                 add += static_cast<Real>(cnt) * static_cast<Real>(d.weight);
             }
@@ -180,13 +238,20 @@ __global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64
     }
 }
 
-template <typename Real, int MODEL>
+// PORTS: the receptor ports 'ex' / 'in_' keep rings of their own,
+// ring_s[(port * L + slot) * tile + t] (the kernel models' ports,
+// _kernel/models/iaf_psc_alpha.py 'ex' / 'in_'); otherwise one ring whose
+// sum is split by sign (_base.py:312-382).
+template <typename Real, int MODEL, bool PORTS>
 __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a, const TiledArgs<Real> t2) {
     using Fix = typename FixOf<Real>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int W = a.W;
+    constexpr int R = PORTS ? 2 : 1;
+    constexpr uint32_t kPostMask = PORTS ? 0x7FFFu : 0xFFFFu;
     const TiledLayout lay = tiled_layout(sizeof(PopCoef<Real>), sizeof(ProjDev<Real>), sizeof(Real),
-                                         a.npop, a.nproj, a.tile, a.L, W, t2.smem_ptr ? a.N + 1 : 0);
+                                         a.npop, a.nproj, a.tile, a.L * R, W,
+                                         t2.smem_ptr ? a.N + 1 : 0);
     PopCoef<Real> *s_coef = reinterpret_cast<PopCoef<Real> *>(smem_raw + lay.coef);
     ProjDev<Real> *s_proj = reinterpret_cast<ProjDev<Real> *>(smem_raw + lay.proj);
     Fix *ring_s = reinterpret_cast<Fix *>(smem_raw + lay.ring);  // fixed-point arrivals
@@ -219,11 +284,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
     }
     if (t2.smem_ptr)
         for (int i = tid; i <= N; i += B) s_ptr[i] = gptr[i];
-    // arrival ring of this tile (fixed point): global [L][N] -> shared [L][tile]
+    // arrival ring of this tile (fixed point): global [L][R][N] -> shared
+    // [R][L][tile]
     const Fix *ring_g = reinterpret_cast<const Fix *>(a.ring);
-    for (int i = tid; i < L * tile; i += B) {
-        const int slot = i / tile, tt = i % tile;
-        ring_s[i] = tt < nloc ? ring_g[static_cast<size_t>(slot) * N + cta0 + tt] : Fix(0);
+    for (int i = tid; i < R * L * tile; i += B) {
+        const int pl = i / tile, tt = i % tile;
+        const int port = pl / L, slot = pl % L;
+        ring_s[i] = tt < nloc ? ring_g[(static_cast<size_t>(slot) * R + port) * N + cta0 + tt] : Fix(0);
     }
     if (tid == 0) {
         s_abort = 0;
@@ -328,7 +395,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
                         if (!t2.wfix) wv[u] = s_wproj[ed[u] >> 24];
                         int slot = nm[u] + static_cast<int>((ed[u] >> 16) & 0xFFu);
                         if (slot >= L) slot -= L;
-                        fix_add(ring_s + slot * tile + (ed[u] & 0xFFFFu), wv[u]);
+                        if (PORTS) slot += static_cast<int>((ed[u] >> 15) & 1u) * L;
+                        fix_add(ring_s + slot * tile + (ed[u] & kPostMask), wv[u]);
                     }
                 }
             }
@@ -498,8 +566,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
                 const Real x = static_cast<Real>(ring_s[slot * tile + tid]) * t2.inv_scale + drv[k * tile];
                 ring_s[slot * tile + tid] = Fix(0);
                 bool sp;
-                if (MODEL == 0) sp = iaf_alpha_step<Real>(cf, st, r, x);
-                else sp = iaf_exp_step<Real>(cf, st, r, x);
+                if (PORTS) {
+                    const Real xi = static_cast<Real>(ring_s[(L + slot) * tile + tid]) * t2.inv_scale;
+                    ring_s[(L + slot) * tile + tid] = Fix(0);
+                    if (MODEL == 0) sp = iaf_alpha_step_ports<Real>(cf, st, r, x, xi);
+                    else sp = iaf_exp_step_ports<Real>(cf, st, r, x, xi);
+                } else {
+                    if (MODEL == 0) sp = iaf_alpha_step<Real>(cf, st, r, x);
+                    else sp = iaf_exp_step<Real>(cf, st, r, x);
+                }
                 if (sp) {
                     const int pos = atomicAdd(&s_nsp[j & 1], 1);
                     const uint32_t ent = (static_cast<uint32_t>(tid) << 5) | static_cast<uint32_t>(k);
@@ -551,17 +626,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
         a.r[g] = r;
     }
     Fix *ring_out = reinterpret_cast<Fix *>(a.ring);
-    for (int i = tid; i < L * nloc; i += B) {
-        const int slot = i / nloc, tt = i % nloc;
-        ring_out[static_cast<size_t>(slot) * N + cta0 + tt] = ring_s[slot * tile + tt];
+    for (int i = tid; i < R * L * nloc; i += B) {
+        const int pl = i / nloc, tt = i % nloc;
+        const int port = pl / L, slot = pl % L;
+        ring_out[(static_cast<size_t>(slot) * R + port) * N + cta0 + tt] = ring_s[pl * tile + tt];
     }
     if (tid == 0) t2.rec_count[c] = rec_n;
 }
 
-size_t lif_tiled_smem(int tile, int L, int W, int N, int npop, int nproj, bool dbl, bool smem_ptr) {
+size_t lif_tiled_smem(int tile, int L, int W, int N, int npop, int nproj, bool dbl, bool smem_ptr,
+                      bool ports) {
     return tiled_layout(dbl ? sizeof(PopCoef<double>) : sizeof(PopCoef<float>),
                         dbl ? sizeof(ProjDev<double>) : sizeof(ProjDev<float>), dbl ? 8 : 4, npop,
-                        nproj, tile, L, W, smem_ptr ? N + 1 : 0)
+                        nproj, tile, L * (ports ? 2 : 1), W, smem_ptr ? N + 1 : 0)
         .total;
 }
 
@@ -569,10 +646,13 @@ template <typename Real>
 cudaError_t launch_lif_tiled(const LifArgs<Real> &a, const TiledArgs<Real> &t2, int grid,
                              cudaStream_t st) {
     const size_t smem = lif_tiled_smem(a.tile, a.L, a.W, a.N, a.npop, a.nproj, sizeof(Real) == 8,
-                                       t2.smem_ptr != 0);
+                                       t2.smem_ptr != 0, t2.ports != 0);
     void *args[] = {const_cast<LifArgs<Real> *>(&a), const_cast<TiledArgs<Real> *>(&t2)};
-    const void *fn = a.model == 0 ? reinterpret_cast<const void *>(&k_lif_tiled<Real, 0>)
-                                  : reinterpret_cast<const void *>(&k_lif_tiled<Real, 1>);
+    const void *fn =
+        t2.ports ? (a.model == 0 ? reinterpret_cast<const void *>(&k_lif_tiled<Real, 0, true>)
+                                 : reinterpret_cast<const void *>(&k_lif_tiled<Real, 1, true>))
+                 : (a.model == 0 ? reinterpret_cast<const void *>(&k_lif_tiled<Real, 0, false>)
+                                 : reinterpret_cast<const void *>(&k_lif_tiled<Real, 1, false>));
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;

@@ -328,8 +328,8 @@ __global__ void __launch_bounds__(128) k_neuron_step(const StepArgs<Real> a, dou
         const DriveDev d = a.drives[a.pop_drive_list[q]];
         const int64_t se = n - d.lag;
         if (d.tmin < se && se <= d.tmax) {
-            const uint64_t u = bits53(d.seed, 0u, static_cast<uint32_t>(se),
-                                      static_cast<uint32_t>(g - c.off));
+            const uint64_t u = drive_draw(d, static_cast<uint32_t>(se),
+                                          static_cast<uint32_t>(g - c.off));
             const int cnt = poisson_from_table(a.cdf + d.cdf_off, d.cdf_n, u);
             in[d.receptor < a.R ? d.receptor : 0] += static_cast<Real>(cnt) * static_cast<Real>(d.weight);
         }

@@ -20,6 +20,7 @@
 #include "coef_cast.h"
 #include "device_types.h"
 #include "host_rng.h"
+#include "jax_rng.h"
 #include "lif_args.h"
 #include "stdp_args.h"
 #include "plan_internal.h"
@@ -514,6 +515,38 @@ int bspk_drive_add_poisson(bspk_plan *p, int post_pop, double rate_hz, double we
     return BSPK_OK;
 }
 
+int bspk_drive_add_poisson_keyed(bspk_plan *p, int post_pop, double rate_hz, double weight,
+                                 int delay_steps, const uint32_t *obj_key, int64_t unit_off,
+                                 int64_t t_min_step, int64_t t_max_step, int receptor,
+                                 int *drive_id) {
+    if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    if (!obj_key) return fail(BSPK_ERR_ARG, "null key");
+    if (unit_off < 0 || unit_off > 0xFFFFFFFFll)
+        return fail(BSPK_ERR_ARG, "unit offset out of range");
+    const float lam = kernel_poisson_lam(rate_hz, p->cfg.dt);
+    if (!(lam >= 0.0f) || lam >= 10.0f)
+        return fail(BSPK_ERR_UNSUPPORTED,
+                    "the kernel stream's CDF inversion needs rate*dt/1000 < 10 (larger means use "
+                    "jax.random.poisson, which is not restated)");
+    int id = -1;
+    const int rc = bspk_drive_add_poisson(p, post_pop, rate_hz, weight, delay_steps, 0u, t_min_step,
+                                          t_max_step, receptor, &id);
+    if (rc) return rc;
+    if (unit_off + p->pops[post_pop].n - 1 > 0xFFFFFFFFll) {
+        p->drives.pop_back();
+        p->input_kind.pop_back();
+        return fail(BSPK_ERR_ARG, "units beyond 2^32");
+    }
+    Drive &D = p->drives[id];
+    D.kind = 1;
+    D.key0 = obj_key[0];
+    D.key1 = obj_key[1];
+    D.unit_off = unit_off;
+    D.thr = kernel_poisson_table(lam);
+    if (drive_id) *drive_id = id;
+    return BSPK_OK;
+}
+
 int bspk_proj_csr_get(bspk_plan *p, int proj_id, int64_t *indptr, int32_t *post_local,
                       int32_t *delay_steps, double *w) {
     if (!p || proj_id < 0 || proj_id >= static_cast<int>(p->projs.size()))
@@ -856,7 +889,8 @@ int build_tiled(bspk_plan *p) {
                 const int q = fill[static_cast<size_t>(c) * (N + 1) + pre_off + i]++;
                 edges[q] = static_cast<uint32_t>(post - c * tile) |
                            (static_cast<uint32_t>(lag_of(p, J.delay[e])) << 16) |
-                           (static_cast<uint32_t>(j) << 24);
+                           (static_cast<uint32_t>(j) << 24) |
+                           (p->ports_tiled && J.receptor == 1 ? 1u << 15 : 0u);
                 if (hetero) w[q] = J.w[e];
             }
     }
@@ -931,9 +965,17 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
     p->sm_count = prop.multiProcessorCount;
     const bool dbl = p->cfg.precision == 64;
     const bool exact = p->cfg.deterministic != 0;
-    const bool aeif = plan_per_step(p);  // per-step engine (RKF45, multisynapse, ports)
     bool plastic = false;
     for (auto &J : p->projs) plastic |= J.plastic;
+    // separate receptor ports of the iaf models run on the tiled kernel (one
+    // ring per port) when it takes the network and every drive feeds 'ex';
+    // otherwise on the per-step engine
+    p->ports_tiled = 0;
+    if (p->ports_sep && !model_per_step(p->cfg.model) && !exact && !plastic) {
+        bool drives0 = true;
+        for (auto &D : p->drives) drives0 &= D.receptor == 0;
+        p->ports_tiled = drives0 ? 1 : 0;  // confirmed below once the geometry is known
+    }
 
     // window and ring length
     int min_lag = 1 << 30, max_lag = 0;
@@ -950,6 +992,17 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
         if (max_lag + 1 > 63) return fail(BSPK_ERR_UNSUPPORTED, "deterministic mode needs lags <= 62 steps");
         p->W = std::max(1, std::min(p->W, 64 - max_lag));
     }
+    if (p->ports_tiled) {
+        // the tiled geometry (as below) must fit, else the per-step engine
+        const int grid = std::max(1, std::min(p->sm_count, (p->N + 31) / 32));
+        const int tile = (p->N + grid - 1) / grid;
+        const int L = p->W + max_lag + 1;
+        if (!(tile <= 256 && grid <= 160 &&
+              lif_tiled_smem(tile, L, p->W, p->N, static_cast<int>(p->pops.size()),
+                             static_cast<int>(p->projs.size()), dbl, false, true) <= 190 * 1024))
+            p->ports_tiled = 0;
+    }
+    const bool aeif = plan_per_step(p);  // per-step engine (RKF45, multisynapse, ports)
     if (aeif || plastic) p->W = 1;
     p->L = p->W + max_lag + 1;
 
@@ -1010,12 +1063,21 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
         d.lag = D.lag;
         d.seed = D.seed;
         d.cdf_off = static_cast<int>(cdf.size());
-        d.cdf_n = static_cast<int>(D.cdf.size());
         d.receptor = D.receptor;
         d.weight = D.weight;
         d.tmin = D.tmin;
         d.tmax = D.tmax;
-        for (double F : D.cdf) cdf.push_back(static_cast<uint64_t>(std::floor(std::ldexp(F, 53))));
+        d.kind = D.kind;
+        d.key0 = D.key0;
+        d.key1 = D.key1;
+        d.unit_off = D.unit_off;
+        if (D.kind == 1) {
+            d.cdf_n = static_cast<int>(D.thr.size());
+            cdf.insert(cdf.end(), D.thr.begin(), D.thr.end());
+        } else {
+            d.cdf_n = static_cast<int>(D.cdf.size());
+            for (double F : D.cdf) cdf.push_back(static_cast<uint64_t>(std::floor(std::ldexp(F, 53))));
+        }
         dd.push_back(d);
     }
     p->cdf_total = static_cast<int>(cdf.size());
@@ -1104,13 +1166,16 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
     // dynamic shared memory budget of the tiled kernel: 227 KB minus its ~34 KB
     // of static arrays
     const size_t tiled_budget = 190 * 1024;
+    const bool two = p->ports_tiled != 0;
     if (!exact && !aeif && !plastic && p->tile <= 256 && p->grid <= 160 &&
-        lif_tiled_smem(p->tile, p->L, p->tW, p->N, npop, nproj_t, dbl, false) <= tiled_budget) {
+        lif_tiled_smem(p->tile, p->L, p->tW, p->N, npop, nproj_t, dbl, false, two) <= tiled_budget) {
         rc = build_tiled(p);
         if (rc) return rc;
         p->tiled = true;
-        p->smem_ptr = lif_tiled_smem(p->tile, p->L, p->tW, p->N, npop, nproj_t, dbl, true) <= tiled_budget;
+        p->smem_ptr =
+            lif_tiled_smem(p->tile, p->L, p->tW, p->N, npop, nproj_t, dbl, true, two) <= tiled_budget;
     }
+    if (two && !p->tiled) return fail(BSPK_ERR_CUDA, "separate ports: tiled geometry check differs");
     p->uploaded = true;
     p->step = 0;
     return BSPK_OK;
@@ -1202,7 +1267,8 @@ int run_tiled(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
                            static_cast<const Fix *>(p->d_twproj), static_cast<Real>(p->tinv_scale),
                            p->d_tlist, p->d_tovf, p->d_trec, p->list_cap, p->smem_ptr ? 1 : 0,
                            static_cast<const Real *>(p->d_tdrive), a.step0,
-                           done == 0 ? p->hold_cta : -1, done == 0 ? p->hold_win : -1};
+                           done == 0 ? p->hold_cta : -1, done == 0 ? p->hold_win : -1,
+                           p->ports_tiled};
         e = launch_lif_tiled<Real>(a, t2, p->grid, st);
         if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
         launches += 2;
@@ -1475,6 +1541,16 @@ int bspk_state_set(bspk_plan *p, int pop, const char *name, const double *values
 }
 
 int64_t bspk_step_count(bspk_plan *p) { return p ? p->step : -1; }
+
+const char *bspk_plan_engine(bspk_plan *p) {
+    if (!p || !p->uploaded) return "";
+    bool per_step = plan_per_step(p);
+    for (auto &J : p->projs) per_step |= J.plastic;
+    if (per_step) return "per_step";
+    if (p->cfg.deterministic) return "exact";
+    if (p->tiled) return "tiled";
+    return "global_ring";
+}
 
 int bspk_last_kernel_time(bspk_plan *p, double *ms, int64_t *launches) {
     if (!p || !p->uploaded) return fail(BSPK_ERR_ARG, "bad arguments");

@@ -58,8 +58,12 @@ struct Drive {
     double rate = 0, weight = 0;
     uint32_t seed = 0;
     int64_t tmin = 0, tmax = 0;
-    std::vector<double> cdf;
+    std::vector<double> cdf;       // kind 0: the CDF in float64
     int input_order = 0;
+    int kind = 0;                  // 1: the reference kernel path's stream
+    uint32_t key0 = 0, key1 = 0;   // kind 1: the device population's object key
+    int64_t unit_off = 0;          // kind 1: unit of the population's first neuron
+    std::vector<uint64_t> thr;     // kind 1: integer thresholds (jax_rng.h)
 };
 
 }  // namespace bspk
@@ -135,6 +139,9 @@ struct bspk_plan {
     // iaf models with receptor ports kept apart (0 = 'ex', 1 = 'in_', signs
     // kept), stepped by the per-step engine; 0 = one summed input split by sign
     int ports_sep = 0;
+    // set at upload: a separate-port plan that the tiled kernel runs (two
+    // rings in shared memory) instead of the per-step engine
+    int ports_tiled = 0;
     int tW = 1;                    // tiled window (half the smallest lag when pipelined)
     int tpipe = 0;                 // 1: window j - 1 is delivered after window j's update
     void *d_tdrive = nullptr;      // Poisson drive of one launch, [steps][N]
@@ -161,6 +168,6 @@ inline int plan_n_receptors(const bspk_plan *p) {
     return p->ports_sep ? 2 : model_n_receptors(p->cfg.model);
 }
 inline bool plan_per_step(const bspk_plan *p) {
-    return model_per_step(p->cfg.model) || p->ports_sep != 0;
+    return model_per_step(p->cfg.model) || (p->ports_sep != 0 && !p->ports_tiled);
 }
 }  // namespace bspk

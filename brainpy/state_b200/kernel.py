@@ -9,50 +9,50 @@ A ``Network`` collects populations, projections and observers without state;
   step n + d, with NEST's rounding of delays to steps, floor(d / dt + 0.5)
   (``_kernel/delays.py:50-100``);
 * the iaf models' receptor ports ``ex`` and ``in_`` stay apart and keep their
-  weights' signs (the kernel models' ``Ports``), so the plan runs on the
-  library's per-step engine;
+  weights' signs (the kernel models' ``Ports``); such plans run on the
+  library's tiled kernel (one shared-memory ring per port) when every drive
+  feeds ``ex``, else on its per-step engine;
 * recording follows the kernel's dense rules (``_kernel/observers.py:1-20``):
   per interval of k steps, spike counts are summed and states are sampled at
   the window's last step; runs are whole multiples of every interval;
-* ``fixed_indegree`` (with multapses) draws its sources from the kernel's key
-  chain (projection name, post population name, local id; blake2b name ids,
-  ``_kernel/rng.py:106-300``) with the library's restatement of
-  ``jax.random.randint``, so adding an unrelated population leaves the
-  realised edges unchanged.
+* every random draw follows the kernel's streams for the network's seed
+  (``_kernel/rng.py``, ``_kernel/compiler.py:819-850``, module ``streams``):
+  ``fixed_indegree`` (with multapses) draws its sources from the key chain
+  (projection name, post population name, local id; blake2b name ids) with
+  the library's restatement of ``jax.random.randint``; distributed weights
+  and delays (``Uniform`` / ``Normal`` / ``LogNormal``) draw one value per
+  edge in the rule's canonical order (post-major, pre ascending) from the
+  projection's WEIGHT / DELAY streams; distributed initial ``V_m`` from the
+  population's INIT stream; and each ``poisson_generator`` unit draws its
+  counts from its population's block keys by the kernel's float32 CDF
+  inversion (``_kernel/models/devices.py:46-145``).  Delays are drawn in the
+  plan's precision (float32 or float64, as the reference does with
+  ``jax_enable_x64`` off or on).
 
 Limits of this front end: the neuron models are ``iaf_psc_alpha`` and
 ``iaf_psc_exp`` (one per network; the kernel's conductance models integrate
 with fixed-substep RK4, which the library does not run); the one device is
-``poisson_generator``, connected ``one_to_one`` onto whole neuron populations,
-drawing from the library's counter-based Poisson stream (not the kernel's
-block keys); ``fixed_indegree`` needs ``allow_multapses=True``; no batched
-trials, plasticity or learners.
+``poisson_generator`` with rate * dt below 10 per step (the reference's CDF
+inversion range), connected ``one_to_one`` onto whole neuron populations;
+``fixed_indegree`` needs ``allow_multapses=True``; no batched trials,
+plasticity or learners.
 """
 from __future__ import annotations
-
-import hashlib
 
 import numpy as np
 
 from . import _lib
+from . import streams as S
 from .simulator import iaf_psc_alpha, iaf_psc_exp
+from .streams import LogNormal, Normal, Uniform, name_id
 from .units import Hz, mV, ms, pA, mantissa
 
 __all__ = ["Network", "PopulationView", "Projection", "Observer", "Program", "Runner", "Results",
            "Recording", "poisson_generator", "all_to_all", "one_to_one", "fixed_indegree",
-           "iaf_psc_alpha", "iaf_psc_exp", "name_id"]
+           "iaf_psc_alpha", "iaf_psc_exp", "name_id", "Uniform", "Normal", "LogNormal"]
 
 GID_BLOCK = 1024          # ids per connectivity key block (_kernel/rng.py:79)
 _PORTS = {"ex": 0, "in_": 1}
-
-
-def name_id(name):
-    """Stable 64-bit id of an object name as (hi, lo): the first eight bytes
-    of blake2b(name) read big-endian (_kernel/rng.py:122-150)."""
-    if not isinstance(name, str) or not name:
-        raise TypeError(f"object name must be a non-empty str, got {name!r}")
-    d = hashlib.blake2b(name.encode("utf-8"), digest_size=8).digest()
-    return int.from_bytes(d[:4], "big"), int.from_bytes(d[4:], "big")
 
 
 # ------------------------------------------------------------------ devices
@@ -270,6 +270,8 @@ class Network:
         for k in init:
             if k != "V_m":
                 raise NotImplementedError(f"initial value of {k!r}: only V_m can be set")
+            if model is poisson_generator:
+                raise ValueError("a device has no initial state")
         name = self._unique(name, model.__name__)
         pop = Population(len(self.populations), name, model, int(n), self.n_neurons, vals, init)
         self.populations.append(pop)
@@ -295,11 +297,17 @@ class Network:
         if isinstance(rule, one_to_one) and pre.size != post.size:
             raise ValueError(f"one_to_one needs equal sizes, got {pre.size} and {post.size}")
         w = 1.0 if weight is None else weight
-        w = np.asarray(mantissa(w, pA), dtype=np.float64)
+        if not isinstance(w, S.Distribution):
+            w = np.asarray(mantissa(w, pA), dtype=np.float64)
         d = self.dt if delay is None else delay
-        d = np.asarray(mantissa(d, ms), dtype=np.float64)
-        if np.any(d <= 0):
-            raise ValueError("delays must be > 0")
+        if isinstance(d, S.Distribution):
+            lo = -np.inf if d.low is None else d.low
+            if lo < 0:
+                raise ValueError("a delay distribution must be bounded below by 0")
+        else:
+            d = np.asarray(mantissa(d, ms), dtype=np.float64)
+            if np.any(d <= 0):
+                raise ValueError("delays must be > 0")
         name = self._unique(name, _RULE_NAMES[type(rule)])
         proj = Projection(len(self.projections), name, pre, post, rule, port, w, d)
         self.projections.append(proj)
@@ -326,21 +334,33 @@ class Network:
         self.observers.append(obs)
         return obs
 
-    def compile(self, precision="float32"):
-        """Realise connectivity and build the library plan: a :class:`Program`."""
+    def compile(self, precision="float32", *, upload=True, spike_capacity=None):
+        """Realise connectivity and build the library plan: a :class:`Program`.
+        ``upload=False`` stops before the device (the realised structure stays
+        readable on the host: ``Program.realised``, ``Program.initial_v``)."""
         if precision not in ("float32", "float64"):
             raise ValueError("precision must be 'float32' or 'float64'")
-        return Program(self, 64 if precision == "float64" else 32)
+        return Program(self, 64 if precision == "float64" else 32, upload=upload,
+                       spike_capacity=spike_capacity)
 
 
 # ----------------------------------------------------------------- compiled
 
-def _delay_steps(d, dt):
-    """NEST rounding of delays to steps, floor(d / dt + 0.5), at least 1."""
-    s = np.floor(d / dt + 0.5).astype(np.int64)
+def _delay_steps(d, dt, bits=64):
+    """NEST rounding of delays to steps (``streams.delay_steps``), at least 1."""
+    s = S.delay_steps(d, dt, bits)
     if np.any(s < 1):
         raise ValueError(f"a delay rounds to 0 steps at dt={dt} ms")
     return s
+
+
+def _grid_steps(t_ms, dt):
+    """Steps of a device time, rounded up to the grid with values within
+    1e-6 steps of a grid point snapped to it (NEST's Time conversion,
+    ``_kernel/units.py:229-270``)."""
+    r = float(t_ms) / dt
+    k = round(r)
+    return int(k) if abs(r - k) <= 1e-6 * max(1.0, abs(r)) else int(np.ceil(r))
 
 
 def realise_positions(net, proj):
@@ -350,7 +370,7 @@ def realise_positions(net, proj):
     pre, post, rule = proj.pre, proj.post, proj.rule
     if isinstance(rule, one_to_one):
         return np.arange(pre.size, dtype=np.int64), np.arange(post.size, dtype=np.int64)
-    if isinstance(rule, all_to_all):
+    if isinstance(rule, all_to_all):  # already canonical
         src = np.tile(np.arange(pre.size, dtype=np.int64), post.size)
         dst = np.repeat(np.arange(post.size, dtype=np.int64), pre.size)
         if not rule.allow_autapses:
@@ -364,17 +384,22 @@ def realise_positions(net, proj):
         self_pos = np.array([where.get(int(g), -1) for g in post.gids], np.int64)
     parts = [(name_id(p.name), local) for p, local in post.parts()]
     pos = _lib.kernel_fixed_indegree(net.seed, name_id(proj.name), parts, pre.size, self_pos, K)
-    return pos.reshape(-1), np.repeat(np.arange(post.size, dtype=np.int64), K)
+    src, dst = pos.reshape(-1), np.repeat(np.arange(post.size, dtype=np.int64), K)
+    # the rule's canonical edge order: post-major, pre ascending, stable
+    # (_kernel/connectivity/rules.py:83-88)
+    order = np.lexsort((src, dst))
+    return src[order], dst[order]
 
 
 class Program:
     """A compiled network: the library plan plus the gid maps (``runner()``)."""
 
-    def __init__(self, net, precision):
+    def __init__(self, net, precision, upload=True, spike_capacity=None):
         self.net, self.precision, self.dt = net, precision, net.dt
         neurons = [p for p in net.populations if not p.is_device]
         model = neurons[0].model if neurons else iaf_psc_alpha
-        pl = _lib.Plan(net.dt, model.model_name, precision=precision, semantics=_lib.RING)
+        kw = {} if spike_capacity is None else {"spike_capacity": int(spike_capacity)}
+        pl = _lib.Plan(net.dt, model.model_name, precision=precision, semantics=_lib.RING, **kw)
         pl.set_ports(True)
         self.lib_gid0 = {}  # population index -> first library gid
         g0 = 0
@@ -384,7 +409,8 @@ class Program:
             g0 += p.n
         self.n_lib = g0
         self.realised = []  # (pre lib pop, post lib pop, indptr, post local, w, delay steps, port)
-        self.drives = []    # (post lib pop, rate, w, delay steps, seed, t_min, t_max, port)
+        self.edge_delays = {}  # projection name -> delay steps in canonical edge order
+        self.drives = []    # (post lib pop, rate, w, delay steps, object key, first unit, t_min, t_max, port)
         for proj in net.projections:
             self._realise(pl, proj)
         rec_v = sorted({int(self._lib_gid(g)) for o in net.observers if "V_m" in o.recordables
@@ -392,16 +418,32 @@ class Program:
         self.rec_v = np.array(rec_v, np.int64)
         if rec_v:
             pl.record_v(self.rec_v)
+        self.plan = pl
+        self._ck0 = None
+        if not upload:
+            return
         pl.upload()
         for p in neurons:
-            v0 = p.init.get("V_m")
-            if v0 is None:
-                v = np.full(p.n, p.params[p.model.order.index("E_L")])
-            else:
-                v = np.broadcast_to(np.asarray(mantissa(v0, mV), np.float64), (p.n,))
-            pl.set_state(p.lib_pop, "V_m", np.ascontiguousarray(v, np.float64))
-        self.plan = pl
+            pl.set_state(p.lib_pop, "V_m", self.initial_v(p))
         self._ck0 = pl.checkpoint()
+
+    @property
+    def bits(self):
+        """Width of the plan's floating-point draws (32 or 64)."""
+        return 64 if self.precision == 64 else 32
+
+    def initial_v(self, p):
+        """Initial V_m of population ``p``: E_L, a value, or a distribution
+        drawn from name_key(fold(object_key, INIT_STREAM), 'V_m') in the
+        plan's precision (``_kernel/params.py:652-693``)."""
+        v0 = p.init.get("V_m")
+        if v0 is None:
+            return np.full(p.n, p.params[p.model.order.index("E_L")])
+        if isinstance(v0, S.Distribution):
+            key = S.name_key(S.fold_in(S.object_key(self.net.seed, p.name), S.INIT_STREAM), "V_m")
+            return v0.sample_in(key, p.n, mV, self.bits)
+        v = np.broadcast_to(np.asarray(mantissa(v0, mV), np.float64), (p.n,))
+        return np.ascontiguousarray(v, np.float64)
 
     def _lib_gid(self, gid):
         for p in self.net.populations:
@@ -422,8 +464,18 @@ class Program:
         src, dst = realise_positions(net, proj)
         pre, post = proj.pre, proj.post
         E = src.size
-        w = np.broadcast_to(proj.weight, (E,)).astype(np.float64)
-        ds = _delay_steps(np.broadcast_to(proj.delay, (E,)).astype(np.float64), dt)
+        okey = S.object_key(net.seed, proj.name)
+        if isinstance(proj.weight, S.Distribution):
+            w = proj.weight.sample_in(S.fold_in(okey, S.WEIGHT_STREAM), E, pA, self.bits)
+        else:
+            w = np.broadcast_to(proj.weight, (E,)).astype(np.float64)
+        if isinstance(proj.delay, S.Distribution):
+            # jax's default float: float32 unless the run enables x64
+            dq = proj.delay.sample_in(S.fold_in(okey, S.DELAY_STREAM), E, ms, self.bits)
+            ds = _delay_steps(dq, dt, self.bits)
+        else:
+            ds = _delay_steps(np.broadcast_to(proj.delay, (E,)).astype(np.float64), dt)
+        self.edge_delays[proj.name] = ds
         pre_lib = np.array([self._lib_gid(g) for g in pre.gids], np.int64)[src]
         post_lib = np.array([self._lib_gid(g) for g in post.gids], np.int64)[dst]
         neurons = [p for p in net.populations if not p.is_device]
@@ -445,22 +497,34 @@ class Program:
                 self.realised.append((a, b, indptr, idx, ww, dd, port))
 
     def _realise_drive(self, pl, proj, port):
+        """A poisson_generator connected one_to_one: unit u of the device
+        population (its position in the device's view) drives the neuron at
+        the same position of the post view, on the kernel's block-key stream
+        of the device population's name (``_kernel/models/devices.py``)."""
         dev = proj.pre.populations[0]
         prm = dev.params
         for p, local in proj.post.parts():
             if local.size != p.n or not np.array_equal(local, np.arange(p.n)):
                 raise NotImplementedError("a poisson_generator drives whole neuron populations")
-        if proj.weight.size != 1 or proj.delay.size != 1:
+        if isinstance(proj.weight, S.Distribution) or isinstance(proj.delay, S.Distribution) or \
+                proj.weight.size != 1 or proj.delay.size != 1:
             raise NotImplementedError("a poisson_generator takes one weight and one delay")
         w = float(proj.weight)
         ds = int(_delay_steps(np.array([float(proj.delay)]), self.dt)[0])
-        t_min = int(round(prm["start"] / self.dt))
-        t_max = 2 ** 62 if prm["stop"] is None else int(round(prm["stop"] / self.dt))
+        t_min = _grid_steps(prm["start"], self.dt)
+        t_max = 2 ** 62 if prm["stop"] is None else _grid_steps(prm["stop"], self.dt)
+        units = proj.pre.gids - dev.gid_start  # device-local unit of each view position
+        okey = S.object_key(self.net.seed, dev.name)
+        pos = 0
         for p, _ in proj.post.parts():
-            hi, lo = name_id(f"{dev.name}/{proj.name}/{p.name}")
-            seed = (hi ^ lo ^ self.net.seed) & 0xFFFFFFFF
-            pl.add_poisson(p.lib_pop, prm["rate"], w, ds, seed, t_min, t_max, receptor=port)
-            self.drives.append((p.lib_pop, prm["rate"], w, ds, seed, t_min, t_max, port))
+            u = units[pos:pos + p.n]
+            pos += p.n
+            if u.size and not np.array_equal(u, np.arange(u[0], u[0] + u.size)):
+                raise NotImplementedError("a population's drive units must be contiguous")
+            u0 = int(u[0]) if u.size else 0
+            pl.add_poisson_keyed(p.lib_pop, prm["rate"], w, ds, okey, u0, t_min, t_max,
+                                 receptor=port)
+            self.drives.append((p.lib_pop, prm["rate"], w, ds, okey, u0, t_min, t_max, port))
 
     def runner(self):
         return Runner(self)

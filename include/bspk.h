@@ -94,7 +94,7 @@ int bspk_plan_create(const bspk_config *cfg, bspk_plan **out);
 int bspk_plan_destroy(bspk_plan *plan);
 
 /* Population of `n` neurons with per-population NEST parameters in the
- * model's fixed order (see DESIGN: iaf_psc_alpha E_L C_m tau_m t_ref V_th
+ * model's fixed order (iaf_psc_alpha: E_L C_m tau_m t_ref V_th
  * V_reset tau_syn_ex tau_syn_in I_e V_min; iaf_psc_exp the same without V_min;
  * aeif_cond_alpha V_peak V_reset t_ref g_L C_m E_ex E_in E_L Delta_T tau_w a b
  * V_th tau_syn_ex tau_syn_in I_e gsl_error_tol; iaf_cond_exp and
@@ -134,6 +134,43 @@ int bspk_proj_add_fixed_indegree(bspk_plan *plan, int pre_pop, int post_pop, int
 int bspk_drive_add_poisson(bspk_plan *plan, int post_pop, double rate_hz, double weight,
                            int delay_steps, uint32_t seed, int64_t t_min_step,
                            int64_t t_max_step, int receptor, int *drive_id);
+
+/* Poisson drive on the reference kernel path's stream: the poisson_generator
+ * device population with object key obj_key = fold(fold(PRNGKey(seed),
+ * hi), lo) of its name id (_kernel/rng.py:153-176), whose unit
+ * unit_off + i drives neuron i of post_pop one_to_one.  Per emission step n
+ * the units of block b draw jax.random.uniform(fold(fold(fold(obj, b), n), 0),
+ * (1024,), float32) (block keys, _kernel/rng.py:338-420) and the count is
+ * the CDF inversion of _kernel/models/devices.py:46-67 in float32, active iff
+ * t_min < n <= t_max; the counts arrive delay_steps later with weight.
+ * Replaces poisson_counts (_kernel/models/devices.py:70-145); rate*dt/1000
+ * must be below 10 (the reference switches to jax.random.poisson there,
+ * which is not restated: BSPK_ERR_UNSUPPORTED). */
+int bspk_drive_add_poisson_keyed(bspk_plan *plan, int post_pop, double rate_hz, double weight,
+                                 int delay_steps, const uint32_t *obj_key, int64_t unit_off,
+                                 int64_t t_min_step, int64_t t_max_step, int receptor,
+                                 int *drive_id);
+
+/* The reference's random draws on the host (JAX's threefry PRNG,
+ * partitionable layout): fold_in (jax.random.fold_in), uniform
+ * (jax.random.uniform(key, (n,), float32 if bits == 32 else float64, lo,
+ * hi), results widened to double) and normal (jax.random.normal, the same
+ * dtypes).  The front ends draw the reference's per-edge delays, distributed
+ * weights and initial states with them (_kernel/params.py:183-330,
+ * _kernel/compiler.py:819-850, _dist.py:40-77).  uniform and fold_in are
+ * bit-exact restatements; normal evaluates erfinv as XLA does for float32
+ * (M. Giles' polynomial on -log1p(-x^2)) and to within an ulp or two for
+ * float64, so its last bits can differ from XLA's where log1p or erfinv
+ * round differently. */
+int bspk_jax_fold_in(const uint32_t *key, uint32_t data, uint32_t *out);
+int bspk_jax_uniform(const uint32_t *key, int64_t n, int bits, double lo, double hi,
+                     double *out);
+int bspk_jax_normal(const uint32_t *key, int64_t n, int bits, double *out);
+/* The kernel-path Poisson table of bspk_drive_add_poisson_keyed for one
+ * rate: up to cap integer thresholds t_k = ceil(F_k * 2^23) - 1 of the
+ * float32 CDF, *n_out = the table's length (tests and tools). */
+int bspk_kernel_poisson_table(double rate_hz, double dt_ms, int cap, uint64_t *thresholds,
+                              int *n_out);
 
 /* Copy a projection's CSR (host copy: indptr[n_pre+1], post_local[E],
  * delay_steps[E], w[E] as given or as sampled).  Replaces the structure
@@ -217,6 +254,12 @@ int bspk_weights_get(bspk_plan *plan, int proj_id, double *w_csr_order);
 int bspk_state_get(bspk_plan *plan, int pop, const char *name, double *values);
 int bspk_state_set(bspk_plan *plan, int pop, const char *name, const double *values);
 int64_t bspk_step_count(bspk_plan *plan);
+/* The kernel family an uploaded plan runs on: "tiled" (target-partitioned
+ * persistent kernel, ring in shared memory), "global_ring" (persistent
+ * kernel with the ring in global memory, for tiles too large for shared
+ * memory), "exact" (deterministic FP64 pull), "per_step" (conductance
+ * models, separate ports or plasticity); "" before upload. */
+const char *bspk_plan_engine(bspk_plan *plan);
 
 /* Timing of the dominant kernel of the last bspk_run (CUDA events on the
  * launching stream): total ms and number of launches. */
@@ -349,20 +392,29 @@ int bspk_adjoint_backward(bspk_adjoint *adj, void *dw, void *dw_in, void *stream
  * Network: a Poisson drive (rate, weight, delay, seed; created first), then
  * one recurrent projection given as in-edges per post neuron:
  * in_indptr[n+1], in_edges[E] = pre | (delay_steps + 1) << 24 in ascending
- * pre order, per-edge weights in_w[E] or NULL with w_const; min/max delay in
- * steps.  Reference Simulator timing (a spike of step m arrives at m + D + 1).
+ * pre order (pre < n and min_delay_steps <= delay_steps <= max_delay_steps
+ * for every edge; the kernel does not check them), per-edge weights in_w[E]
+ * or NULL with w_const; in_edges must not be NULL, even for E = 0.
+ * Reference Simulator timing (a spike of step m arrives at m + D + 1).
  * state: [6][n] doubles (V_m, I_syn_ex, dI_syn_ex, I_syn_in, dI_syn_in, y0),
- * refr: [n] refractory counters, both read and written.  Outputs: spikes as
- * (step within this call, neuron) pairs up to spike_cap, *spike_count, and
- * *status (0 = ok, nonzero = device error code), all device memory.
+ * refr: [n] refractory counters, both read and written.  Outputs, all device
+ * memory: spikes as (step within this call, neuron) pairs; *spike_count is
+ * the number of spikes of the call, which may exceed spike_cap: only the
+ * first min(*spike_count, spike_cap) pairs are written, and *status is then
+ * BSPK_DEV_ERR_OVERFLOW (2).  *status is 0 when the call completed, else a
+ * device error code (1 = a bounded wait ran out).
  *
- * Limits: n <= 65536 neurons, delays <= 61 steps, drive CDF <= 4096 entries;
- * larger sizes are rejected with BSPK_ERR_ARG.  Each call starts with an
- * empty spike history (spikes of earlier calls are not delivered).  All
- * calls on a device share the scratch array, so calls that overlap on the
- * GPU race; serialise them.  The first call on a device looks up the
- * scratch array's device address (once per device, with that device
- * current); make that first call before capturing any stream. */
+ * Limits: n <= 65536 neurons (the scratch array) and no more than the
+ * cooperative launch can keep resident, 256 neurons per SM on a B200
+ * (37 888 neurons on 148 SMs; larger networks return BSPK_ERR_UNSUPPORTED
+ * with the limit in bspk_last_error()); delays <= 61 steps; drive CDF <=
+ * 4096 entries (BSPK_ERR_ARG beyond).  Each call starts with an empty spike
+ * history (spikes of earlier calls are not delivered) and restarts the
+ * drive's random stream at step 0, so calls that continue a run need a new
+ * drive_seed each.  All calls on a device share the scratch array, so calls
+ * that overlap on the GPU race; serialise them.  The first call on a device
+ * looks up the scratch array's device address (once per device, with that
+ * device current); make that first call before capturing any stream. */
 int bspk_iaf_exact_run_noalloc(double dt, const double *params, int n_params, int n,
                                const int64_t *in_indptr, const uint32_t *in_edges,
                                const double *in_w, double w_const, int min_delay_steps,

@@ -71,6 +71,12 @@ void bo_jax_random_bits(const uint32_t key[2], int nbits, int64_t n, uint64_t *o
     }
 }
 
+void bo_jax_random_bits_at(const uint32_t key[2], int nbits, int64_t i, uint64_t *out) {
+    uint32_t y0, y1;
+    bo_threefry2x32(key[0], key[1], (uint32_t)((uint64_t)i >> 32), (uint32_t)i, &y0, &y1);
+    *out = nbits == 64 ? (((uint64_t)y0 << 32) | y1) : (uint64_t)(y0 ^ y1);
+}
+
 /* jax.random.randint(key, (n,), minval, maxval): two bit streams from
  * split(key), remainder combination with multiplier 2**nbits % span, all in
  * nbits-wide unsigned arithmetic. */
@@ -175,6 +181,142 @@ int bo_poisson(double lam, double exp_neg_lam, double u) {
     return k;
 }
 
+/* ------------------------------------------ jax.random distributions */
+
+/* jax.random.uniform(key, (n,), dtype, minval, maxval) (jax/_src/random.py
+ * _uniform): nbits random bits per element (partitionable layout), the top
+ * nmant bits OR-ed under the exponent of 1.0, bitcast, minus 1.0, then
+ * floats * (maxval - minval) + minval and max(minval, .).  float32 for
+ * nbits 32, float64 for 64; every operation rounds in that type. */
+void bo_jax_uniform(const uint32_t key[2], int nbits, int64_t n, double lo, double hi,
+                    double *out) {
+    for (int64_t i = 0; i < n; ++i) {
+        uint64_t bits;
+        bo_jax_random_bits_at(key, nbits, i, &bits);
+        if (nbits == 32) {
+            uint32_t b = ((uint32_t)bits >> (32 - 23)) | 0x3F800000u;
+            float f;
+            memcpy(&f, &b, 4);
+            volatile float floats = f - 1.0f;
+            volatile float span = (float)hi - (float)lo;
+            volatile float scaled = floats * span;
+            volatile float v = scaled + (float)lo;
+            out[i] = v > (float)lo ? v : (float)lo;
+        } else {
+            uint64_t b = (bits >> (64 - 52)) | 0x3FF0000000000000ull;
+            double f;
+            memcpy(&f, &b, 8);
+            volatile double floats = f - 1.0;
+            volatile double scaled = floats * (hi - lo);
+            volatile double v = scaled + lo;
+            out[i] = v > lo ? v : lo;
+        }
+    }
+}
+
+/* XLA's float32 ErfInv (M. Giles, "Approximating the erfinv function",
+ * single-precision form): w = -log1p(-x*x); w < 5: Horner in w - 2.5, else
+ * in sqrt(w) - 3; times x; +-1 -> +-inf. */
+static float erfinv32(float x) {
+    static const float lt5[9] = {2.81022636e-08f, 3.43273939e-07f, -3.5233877e-06f,
+                                 -4.39150654e-06f, 0.00021858087f, -0.00125372503f,
+                                 -0.00417768164f, 0.246640727f, 1.50140941f};
+    static const float ge5[9] = {-0.000200214257f, 0.000100950558f, 0.00134934322f,
+                                 -0.00367342844f, 0.00573950773f, -0.0076224613f,
+                                 0.00943887047f, 1.00167406f, 2.83297682f};
+    volatile float xx = x * x;
+    float w = -log1pf(-xx);
+    const float *c = w < 5.0f ? lt5 : ge5;
+    w = w < 5.0f ? w - 2.5f : sqrtf(w) - 3.0f;
+    float p = c[0];
+    for (int i = 1; i < 9; ++i) {
+        volatile float pw = p * w;
+        p = c[i] + pw;
+    }
+    if (fabsf(x) == 1.0f) return x * INFINITY;
+    return p * x;
+}
+
+/* float64 erfinv by bisection on erfl (long double), a different route from
+ * the library's Newton steps; the result is the double nearest the root. */
+static double erfinv64(double x) {
+    if (fabs(x) == 1.0) return x * INFINITY;
+    if (x == 0.0) return x;
+    long double ax = fabsl((long double)x), a = 0.0L, b = 10.0L;
+    for (int it = 0; it < 200; ++it) {
+        long double m = 0.5L * (a + b);
+        long double f = ax < 0.5L ? erfl(m) - ax : (1.0L - ax) - erfcl(m);
+        if (f > 0) b = m; else a = m;  /* f grows with m on both branches */
+        if (b - a <= 1e-30L * b) break;
+    }
+    double y = (double)(0.5L * (a + b));
+    return x < 0 ? -y : y;
+}
+
+/* jax.random.normal(key, (n,), dtype) (jax/_src/random.py _normal_real):
+ * u = uniform(key, minval = nextafter(-1, 0), maxval = 1), then
+ * sqrt(2) * erfinv(u) in the dtype. */
+void bo_jax_normal(const uint32_t key[2], int nbits, int64_t n, double *out) {
+    double *u = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    if (nbits == 32) {
+        bo_jax_uniform(key, 32, n, (double)nextafterf(-1.0f, 0.0f), 1.0, u);
+        for (int64_t i = 0; i < n; ++i) {
+            volatile float e = erfinv32((float)u[i]);
+            out[i] = (float)(1.41421354f * e);
+        }
+    } else {
+        bo_jax_uniform(key, 64, n, nextafter(-1.0, 0.0), 1.0, u);
+        for (int64_t i = 0; i < n; ++i) out[i] = 1.4142135623730951 * erfinv64(u[i]);
+    }
+    free(u);
+}
+
+/* ------------------------------------- kernel-path poisson_generator */
+
+static float ftz32(float v) { return fabsf(v) < 1.17549435e-38f ? 0.0f : v; }
+
+/* One unit's count (_kernel/models/devices.py:46-67, _inversion), from the
+ * step key of its block and its lane: u = jax.random.uniform(key, (1024,),
+ * float32)[lane]; p = exp(-lam); F = p; k = 0; twelve terms k += u >= F,
+ * p = p * lam / i, F += p (i = 1..12); then while u >= F and p > 0 the same
+ * with i = 13, 14, ...  float32 throughout, subnormal results flushed to
+ * zero (XLA's CPU setting). */
+int64_t bo_kernel_poisson_count(const uint32_t step_key[2], uint32_t lane, float lam) {
+    uint32_t y0, y1;
+    bo_threefry2x32(step_key[0], step_key[1], 0u, lane, &y0, &y1);
+    uint32_t b = ((y0 ^ y1) >> 9) | 0x3F800000u;
+    float f;
+    memcpy(&f, &b, 4);
+    float u = f - 1.0f;
+    float p = ftz32((float)exp(-(double)lam));
+    float F = p;
+    int64_t k = 0;
+    for (int i = 1; i <= 12; ++i) {
+        k += u >= F;
+        volatile float pl = p * lam;
+        p = ftz32(ftz32(pl) / (float)i);
+        volatile float Fn = F + p;
+        F = Fn;
+    }
+    for (int i = 13; u >= F && p > 0.0f; ++i) {
+        k += 1;
+        volatile float pl = p * lam;
+        p = ftz32(ftz32(pl) / (float)i);
+        volatile float Fn = F + p;
+        F = Fn;
+    }
+    return k;
+}
+
+/* The step key of block b of a device population at step n, trial 0:
+ * fold(fold(fold(obj, b), n), 0) (_kernel/rng.py:338-420). */
+void bo_kernel_step_key(const uint32_t obj[2], uint32_t block, uint32_t step, uint32_t out[2]) {
+    uint32_t a[2], c[2];
+    bo_jax_fold_in(obj, block, a);
+    bo_jax_fold_in(a, step, c);
+    bo_jax_fold_in(c, 0u, out);
+}
+
 /* ----------------------------------------------------------- propagators */
 
 /* _nest_base/utils.py:177-229 (alpha_propagator_p31_p32), NEST
@@ -245,6 +387,11 @@ typedef struct {
     int ddelay;
     uint32_t seed;
     int64_t tmin, tmax;
+    /* keyed drive (the kernel path's stream): object key, first unit, lam */
+    int keyed;
+    uint32_t okey[2];
+    int64_t unit_off;
+    float lam32;
     /* stdp */
     int plastic;
     int rule; /* 0: stdp_synapse (pair), 1: stdp_triplet_synapse */
@@ -492,6 +639,22 @@ int bo_add_drive(bo_sim *s, int post_pop, double rate_hz, double weight, int del
     return s->nin++;
 }
 
+int bo_add_drive_keyed(bo_sim *s, int post_pop, double rate_hz, double weight, int delay_steps,
+                       const uint32_t okey[2], int64_t unit_off, int64_t t_min_step,
+                       int64_t t_max_step, int receptor) {
+    int id = bo_add_drive(s, post_pop, rate_hz, weight, delay_steps, 0u, t_min_step, t_max_step,
+                          receptor);
+    if (id < 0) return id;
+    input_t *in = &s->ins[id];
+    in->keyed = 1;
+    in->okey[0] = okey[0];
+    in->okey[1] = okey[1];
+    in->unit_off = unit_off;
+    /* lam = rate [kHz] * dt [ms] in float32 (_kernel/models/devices.py:203) */
+    in->lam32 = (float)(rate_hz * s->dt / 1000.0);
+    return id;
+}
+
 int bo_set_stdp(bo_sim *s, int proj, double tau_plus, double tau_minus, double lambda_,
                 double alpha, double mu_plus, double mu_minus, double wmax) {
     if (proj < 0 || proj >= s->nin || s->ins[proj].kind != 0) return -1;
@@ -610,6 +773,14 @@ static inline int fired(bo_sim *s, int64_t m, int gid) {
 static int64_t drive_count(const input_t *in, int64_t emit_step, int t) {
     /* active iff t_min < step <= t_max (poisson_generator.py:566-567) */
     if (!(in->tmin < emit_step && emit_step <= in->tmax) || in->rate <= 0.0) return 0;
+    if (in->keyed) {
+        /* the kernel path: unit = unit_off + t, block unit >> 10, lane
+         * unit & 1023 (_kernel/rng.py draw_blocked, GID_BLOCK = 1024) */
+        uint64_t unit = (uint64_t)in->unit_off + (uint64_t)t;
+        uint32_t sk[2];
+        bo_kernel_step_key(in->okey, (uint32_t)(unit >> 10), (uint32_t)emit_step, sk);
+        return bo_kernel_poisson_count(sk, (uint32_t)(unit & 1023u), in->lam32);
+    }
     double u = bo_uniform01(in->seed, 0u, (uint32_t)emit_step, (uint32_t)t);
     return bo_poisson(in->lam, in->enl, u);
 }

@@ -58,6 +58,14 @@ void bo_jax_split(const uint32_t key[2], int num, uint32_t *out /* num*2 */);
 void bo_jax_random_bits(const uint32_t key[2], int nbits, int64_t n, uint64_t *out);
 void bo_jax_randint(const uint32_t key[2], int64_t n, int64_t minval, int64_t maxval,
                     int nbits, int64_t *out);
+void bo_jax_random_bits_at(const uint32_t key[2], int nbits, int64_t i, uint64_t *out);
+/* jax.random.uniform / normal (float32 for nbits 32, float64 for 64) */
+void bo_jax_uniform(const uint32_t key[2], int nbits, int64_t n, double lo, double hi,
+                    double *out);
+void bo_jax_normal(const uint32_t key[2], int nbits, int64_t n, double *out);
+/* kernel-path poisson_generator: step key of a block, count of one unit */
+void bo_kernel_step_key(const uint32_t obj[2], uint32_t block, uint32_t step, uint32_t out[2]);
+int64_t bo_kernel_poisson_count(const uint32_t step_key[2], uint32_t lane, float lam);
 /* legacy fixed-indegree sampler (connectivity.py:101-135): post-major edges */
 int bo_fixed_indegree(int64_t seed, int n_pre, int n_post, int K, int pre_is_post,
                       int allow_autapses, int nbits, int32_t *pre_out, int32_t *post_out);
@@ -85,6 +93,11 @@ int bo_add_proj(bo_sim *s, int pre_pop, int post_pop, int64_t n_edges,
                 const int32_t *delay_steps, int receptor);
 int bo_add_drive(bo_sim *s, int post_pop, double rate_hz, double weight, int delay_steps,
                  uint32_t seed, int64_t t_min_step, int64_t t_max_step, int receptor);
+/* drive on the kernel path's stream of the device population with object
+ * key okey; unit unit_off + t drives neuron t of post_pop */
+int bo_add_drive_keyed(bo_sim *s, int post_pop, double rate_hz, double weight, int delay_steps,
+                       const uint32_t okey[2], int64_t unit_off, int64_t t_min_step,
+                       int64_t t_max_step, int receptor);
 int bo_set_stdp(bo_sim *s, int proj, double tau_plus, double tau_minus, double lambda_,
                 double alpha, double mu_plus, double mu_minus, double wmax);
 int bo_set_stdp_triplet(bo_sim *s, int proj, double tau_plus, double tau_plus_triplet,

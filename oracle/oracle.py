@@ -90,6 +90,13 @@ def lib():
         L.bo_fixed_indegree.argtypes = [i64, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                         C.c_int, vp, vp]
         L.bo_csr_structure.argtypes = [vp, vp, i64, C.c_int, vp, vp, vp]
+        L.bo_jax_uniform.argtypes = [vp, C.c_int, i64, dbl, dbl, vp]
+        L.bo_jax_normal.argtypes = [vp, C.c_int, i64, vp]
+        L.bo_kernel_step_key.argtypes = [vp, u32, u32, vp]
+        L.bo_kernel_poisson_count.restype = i64
+        L.bo_kernel_poisson_count.argtypes = [vp, u32, C.c_float]
+        L.bo_add_drive_keyed.argtypes = [vp, C.c_int, dbl, dbl, C.c_int, vp, i64, i64, i64,
+                                         C.c_int]
         L.bo_uniform01.restype = dbl
         L.bo_uniform01.argtypes = [u32, u32, u32, u32]
         L.bo_poisson.argtypes = [dbl, dbl, dbl]
@@ -201,6 +208,34 @@ def csr_structure(pre, post, n_pre):
     return order, indices, indptr
 
 
+def jax_uniform(key, n, bits=32, lo=0.0, hi=1.0):
+    """jax.random.uniform(key, (n,), float32 / float64, lo, hi) as float64."""
+    k = np.asarray(key, np.uint32).copy()
+    out = np.zeros(int(n), np.float64)
+    lib().bo_jax_uniform(_p(k), int(bits), int(n), float(lo), float(hi), _p(out))
+    return out
+
+
+def jax_normal(key, n, bits=32):
+    """jax.random.normal(key, (n,), float32 / float64) as float64."""
+    k = np.asarray(key, np.uint32).copy()
+    out = np.zeros(int(n), np.float64)
+    lib().bo_jax_normal(_p(k), int(bits), int(n), _p(out))
+    return out
+
+
+def kernel_step_key(obj_key, block, step):
+    k = np.asarray(obj_key, np.uint32).copy()
+    out = np.zeros(2, np.uint32)
+    lib().bo_kernel_step_key(_p(k), int(block), int(step) & 0xFFFFFFFF, _p(out))
+    return out
+
+
+def kernel_poisson_count(step_key, lane, lam32):
+    k = np.asarray(step_key, np.uint32).copy()
+    return int(lib().bo_kernel_poisson_count(_p(k), int(lane), float(lam32)))
+
+
 def uniform01(seed, stream, step, idx):
     return lib().bo_uniform01(seed, stream, step, idx)
 
@@ -276,6 +311,15 @@ class OracleSim:
                                  int(t_max), int(receptor))
         if r < 0:
             raise ValueError("add_drive failed")
+        return r
+
+    def add_drive_keyed(self, post_pop, rate_hz, weight, delay_steps, obj_key, unit_off=0,
+                        t_min=0, t_max=2 ** 62, receptor=0):
+        k = np.asarray(obj_key, np.uint32).copy()
+        r = self._L.bo_add_drive_keyed(self._h, post_pop, rate_hz, weight, delay_steps, _p(k),
+                                       unit_off, t_min, t_max, receptor)
+        if r < 0:
+            raise ValueError("bad drive")
         return r
 
     def set_stdp(self, proj, tau_plus, tau_minus, lambda_, alpha, mu_plus, mu_minus, wmax):

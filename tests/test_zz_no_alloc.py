@@ -54,13 +54,7 @@ def _reference(n, csr, v0, n_steps):
     return st, g, pl.get_state(0, "V_m")
 
 
-def test_noalloc_matches_plan_path_twice():
-    import torch
-    n, csr, csc, v0, dmin, dmax = _network()
-    n_steps = 600
-    ref_st, ref_g, ref_v = _reference(n, csr, v0, n_steps)
-    assert ref_st.size > 0
-
+def _fn():
     L = _lib.lib()
     fn = L.bspk_iaf_exact_run_noalloc
     fn.restype = C.c_int
@@ -68,35 +62,92 @@ def test_noalloc_matches_plan_path_twice():
     fn.argtypes = [C.c_double, vp, C.c_int, C.c_int, vp, vp, vp, C.c_double, C.c_int, C.c_int,
                    C.c_double, C.c_double, C.c_int, C.c_uint32, vp, vp, C.c_int64, vp, vp,
                    C.c_int64, vp, vp, vp]
+    return L, fn
+
+
+def _call(fn, n, csc, v0, dmin, dmax, n_steps, cap):
+    """One call with caller-owned torch buffers; returns (rc, status, count,
+    steps, gids, V_m) with the spike pairs cut to min(count, cap)."""
+    import torch
     dev = torch.device("cuda")
     indptr = torch.tensor(csc[0], dtype=torch.int64, device=dev)
     edges = torch.tensor(csc[1].view(np.int32), dtype=torch.int32, device=dev)
     w = torch.tensor(csc[2], dtype=torch.float64, device=dev)
-    cap = 200000
     params = np.asarray(PARAMS, np.float64)
+    state = torch.zeros((6, n), dtype=torch.float64, device=dev)
+    state[0] = torch.tensor(v0, dtype=torch.float64)
+    refr = torch.zeros(n, dtype=torch.int32, device=dev)
+    spk_step = torch.full((max(cap, 1),), -1, dtype=torch.int64, device=dev)
+    spk_gid = torch.full((max(cap, 1),), -1, dtype=torch.int32, device=dev)
+    count = torch.zeros(1, dtype=torch.int64, device=dev)
+    status = torch.full((1,), -99, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = fn(0.1, params.ctypes.data_as(C.c_void_p), params.size, n, indptr.data_ptr(),
+            edges.data_ptr(), w.data_ptr(), 0.0, dmin, dmax, 17789.0, 20.68, 15, 77,
+            state.data_ptr(), refr.data_ptr(), n_steps, spk_step.data_ptr(),
+            spk_gid.data_ptr(), cap, count.data_ptr(), status.data_ptr(), stream)
+    if rc != 0:
+        return rc, None, None, None, None, None
+    torch.cuda.synchronize()
+    m = int(count.item())
+    k = min(m, cap)
+    return (rc, int(status.item()), m, spk_step[:k].cpu().numpy(), spk_gid[:k].cpu().numpy(),
+            state[0].cpu().numpy())
+
+
+def test_noalloc_matches_plan_path_twice():
+    n, csr, csc, v0, dmin, dmax = _network()
+    n_steps = 600
+    ref_st, ref_g, ref_v = _reference(n, csr, v0, n_steps)
+    assert ref_st.size > 0
+    L, fn = _fn()
     for call in range(2):
-        state = torch.zeros((6, n), dtype=torch.float64, device=dev)
-        state[0] = torch.tensor(v0, dtype=torch.float64)
-        refr = torch.zeros(n, dtype=torch.int32, device=dev)
-        spk_step = torch.full((cap,), -1, dtype=torch.int64, device=dev)
-        spk_gid = torch.full((cap,), -1, dtype=torch.int32, device=dev)
-        count = torch.zeros(1, dtype=torch.int64, device=dev)
-        status = torch.full((1,), -99, dtype=torch.int32, device=dev)
-        stream = torch.cuda.current_stream().cuda_stream
-        rc = fn(0.1, params.ctypes.data_as(vp), params.size, n, indptr.data_ptr(),
-                edges.data_ptr(), w.data_ptr(), 0.0, dmin, dmax, 17789.0, 20.68, 15, 77,
-                state.data_ptr(), refr.data_ptr(), n_steps, spk_step.data_ptr(),
-                spk_gid.data_ptr(), cap, count.data_ptr(), status.data_ptr(), stream)
+        rc, status, m, st, g, v = _call(fn, n, csc, v0, dmin, dmax, n_steps, 200000)
         assert rc == 0, L.bspk_last_error()
-        torch.cuda.synchronize()
-        assert int(status.item()) == 0
-        m = int(count.item())
-        st = spk_step[:m].cpu().numpy()
-        g = spk_gid[:m].cpu().numpy()
+        assert status == 0
+        assert m == ref_st.size
         order = np.lexsort((g, st))
         np.testing.assert_array_equal(st[order], ref_st)
         np.testing.assert_array_equal(g[order], ref_g)
-        np.testing.assert_array_equal(state[0].cpu().numpy(), ref_v)
+        np.testing.assert_array_equal(v, ref_v)
+
+
+def test_noalloc_flags_spikes_beyond_capacity():
+    """A capacity below the call's spike count: the count is the true total,
+    only `cap` pairs are written (each one of the plan path's spikes) and the
+    status is the overflow code (2)."""
+    n, csr, csc, v0, dmin, dmax = _network()
+    ref_st, ref_g, _ = _reference(n, csr, v0, 300)
+    L, fn = _fn()
+    rc, status, m, st, g, _ = _call(fn, n, csc, v0, dmin, dmax, 300, 5)
+    assert rc == 0, L.bspk_last_error()
+    assert m == ref_st.size > 5
+    assert status == 2
+    ref = set(zip(ref_st.tolist(), ref_g.tolist()))
+    assert st.size == 5 and all((int(a), int(b)) in ref for a, b in zip(st, g))
+
+
+def test_noalloc_largest_resident_network():
+    """The largest network the cooperative launch keeps resident (256 neurons
+    per SM) matches the plan path; one neuron more is refused up front."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    n_max = 256 * sms
+    n, csr, csc, v0, dmin, dmax = _network(n=n_max, K=20, seed=5)
+    n_steps = 60
+    ref_st, ref_g, ref_v = _reference(n, csr, v0, n_steps)
+    L, fn = _fn()
+    rc, status, m, st, g, v = _call(fn, n, csc, v0, dmin, dmax, n_steps, 500000)
+    assert rc == 0, L.bspk_last_error()
+    assert status == 0 and m == ref_st.size
+    order = np.lexsort((g, st))
+    np.testing.assert_array_equal(st[order], ref_st)
+    np.testing.assert_array_equal(g[order], ref_g)
+    np.testing.assert_array_equal(v, ref_v)
+    n1, _, csc1, v1, dmin1, dmax1 = _network(n=n_max + 1, K=2, seed=6)
+    rc, *_ = _call(fn, n1, csc1, v1, dmin1, dmax1, 10, 1000)
+    assert rc == -4
+    assert b"co-resident" in L.bspk_last_error()
 
 
 def test_noalloc_rejects_oversized_network():
