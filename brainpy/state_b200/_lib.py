@@ -74,6 +74,9 @@ def lib():
                                                        C.POINTER(C.c_int)]),
             "bspk_drive_add_poisson": (C.c_int, [vp, C.c_int, dbl, dbl, C.c_int, u32, i64, i64,
                                                  C.c_int, C.POINTER(C.c_int)]),
+            "bspk_proj_add_fixed_indegree_w": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, i64,
+                                                         C.c_int, C.c_int, dbl, vp, vp, C.c_int,
+                                                         C.c_int, C.POINTER(C.c_int)]),
             "bspk_drive_add_poisson_keyed": (C.c_int, [vp, C.c_int, dbl, dbl, C.c_int, vp, i64,
                                                        i64, i64, C.c_int, C.POINTER(C.c_int)]),
             "bspk_jax_fold_in": (C.c_int, [vp, u32, vp]),
@@ -100,6 +103,7 @@ def lib():
             "bspk_state_set": (C.c_int, [vp, C.c_int, C.c_char_p, vp]),
             "bspk_step_count": (i64, [vp]),
             "bspk_plan_engine": (C.c_char_p, [vp]),
+            "bspk_plan_ring_fraction_bits": (C.c_int, [vp, C.POINTER(C.c_int)]),
             "bspk_last_kernel_time": (C.c_int, [vp, C.POINTER(dbl), C.POINTER(i64)]),
             "bspk_rk_substeps": (C.c_int, [vp, C.POINTER(i64)]),
             "bspk_checkpoint_size": (C.c_int, [vp, C.POINTER(i64)]),
@@ -268,13 +272,17 @@ class Plan:
         return out.value
 
     def add_fixed_indegree(self, pre, post, K, seed, weight, delay_steps=None, delay_const=0,
-                           allow_autapses=True, nbits=32, receptor=0):
+                           allow_autapses=True, nbits=32, receptor=0, w_draw=None):
+        """``delay_steps`` and ``w_draw`` (per-edge weights) are in the
+        sampler's edge order (post-major, before the CSR sort)."""
         d = None if delay_steps is None else np.ascontiguousarray(delay_steps, np.int32)
+        wd = None if w_draw is None else np.ascontiguousarray(w_draw, np.float64)
         out = C.c_int()
-        check(self._L.bspk_proj_add_fixed_indegree(self._h, pre, post, int(K), int(seed),
-                                                   int(bool(allow_autapses)), int(nbits),
-                                                   float(weight), ptr(d), int(delay_const),
-                                                   int(receptor), C.byref(out)))
+        check(self._L.bspk_proj_add_fixed_indegree_w(self._h, pre, post, int(K), int(seed),
+                                                     int(bool(allow_autapses)), int(nbits),
+                                                     float(weight), ptr(wd), ptr(d),
+                                                     int(delay_const), int(receptor),
+                                                     C.byref(out)))
         self._proj_edges.append(int(K) * self.pop_sizes[post])
         self._proj_pre_n.append(self.pop_sizes[pre])
         return out.value
@@ -409,6 +417,13 @@ class Plan:
         ms, n = C.c_double(), C.c_int64()
         check(self._L.bspk_last_kernel_time(self._h, C.byref(ms), C.byref(n)))
         return ms.value, n.value
+
+    @property
+    def ring_fraction_bits(self):
+        """k of the tiled kernel's fixed-point ring (weights rint(w * 2^k))."""
+        k = C.c_int()
+        check(self._L.bspk_plan_ring_fraction_bits(self._h, C.byref(k)))
+        return k.value
 
     def rk_substeps(self):
         """RKF45 substeps, accepted and rejected, of every conductance-model

@@ -459,6 +459,15 @@ int bspk_proj_add_fixed_indegree(bspk_plan *p, int pre_pop, int post_pop, int K,
                                  int allow_autapses, int nbits, double weight,
                                  const int32_t *delay_steps, int delay_const, int receptor,
                                  int *proj_id) {
+    return bspk_proj_add_fixed_indegree_w(p, pre_pop, post_pop, K, seed, allow_autapses, nbits,
+                                          weight, nullptr, delay_steps, delay_const, receptor,
+                                          proj_id);
+}
+
+int bspk_proj_add_fixed_indegree_w(bspk_plan *p, int pre_pop, int post_pop, int K, int64_t seed,
+                                   int allow_autapses, int nbits, double weight,
+                                   const double *w_draw, const int32_t *delay_steps,
+                                   int delay_const, int receptor, int *proj_id) {
     if (!p) return fail(BSPK_ERR_ARG, "null plan");
     const int npop = static_cast<int>(p->pops.size());
     if (pre_pop < 0 || pre_pop >= npop || post_pop < 0 || post_pop >= npop)
@@ -478,6 +487,8 @@ int bspk_proj_add_fixed_indegree(bspk_plan *p, int pre_pop, int post_pop, int K,
     std::vector<int32_t> dl(E);
     for (int64_t e = 0; e < E; ++e) dl[e] = delay_steps ? delay_steps[order[e]] : delay_const;
     std::vector<double> w(E, weight);
+    if (w_draw)
+        for (int64_t e = 0; e < E; ++e) w[e] = w_draw[order[e]];
     return bspk_proj_add_csr(p, pre_pop, post_pop, E, indptr.data(), indices.data(), w.data(),
                              dl.data(), receptor, proj_id);
 }
@@ -1541,6 +1552,13 @@ int bspk_state_set(bspk_plan *p, int pop, const char *name, const double *values
 }
 
 int64_t bspk_step_count(bspk_plan *p) { return p ? p->step : -1; }
+
+int bspk_plan_ring_fraction_bits(bspk_plan *p, int *bits) {
+    if (!p || !bits) return fail(BSPK_ERR_ARG, "null argument");
+    if (!p->uploaded || !p->tiled) return fail(BSPK_ERR_STATE, "not an uploaded plan on the tiled path");
+    *bits = static_cast<int>(std::lround(-std::log2(p->tinv_scale)));
+    return BSPK_OK;
+}
 
 const char *bspk_plan_engine(bspk_plan *p) {
     if (!p || !p->uploaded) return "";

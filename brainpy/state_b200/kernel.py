@@ -418,6 +418,12 @@ class Program:
         self.rec_v = np.array(rec_v, np.int64)
         if rec_v:
             pl.record_v(self.rec_v)
+        # spikes: of the observed neurons when any observer records them, of
+        # every neuron otherwise (plan-level users read them all)
+        rec_s = sorted({int(self._lib_gid(g)) for o in net.observers if "spike" in o.recordables
+                        for g in o.view.gids})
+        if rec_s:
+            pl.record_spikes_of(np.array(rec_s, np.int32))
         self.plan = pl
         self._ck0 = None
         if not upload:
@@ -555,6 +561,7 @@ class Runner:
             raise TypeError(f"Runner needs a Program, got {type(program).__name__}")
         self.program = program
         self.n = 0
+        self.h2d_bytes = self.d2h_bytes = 0
 
     @property
     def t(self):
@@ -563,6 +570,7 @@ class Runner:
     def reset(self):
         self.program.plan.restore(self.program._ck0)
         self.n = 0
+        self.h2d_bytes = int(self.program._ck0.nbytes)
 
     def simulate(self, duration):
         self.reset()
@@ -576,7 +584,10 @@ class Runner:
         pl = prog.plan
         pl.run(n_steps)
         st, g = pl.spikes()
-        v = pl.v_trace() if prog.rec_v.size else None
+        v = pl.v_trace(np.float32 if prog.precision == 32 else np.float64) \
+            if prog.rec_v.size else None
+        # bytes read back from the device by this call (spike pairs, V_m)
+        self.d2h_bytes = int(st.nbytes + g.nbytes + (v.nbytes if v is not None else 0))
         recs = {}
         for o in prog.net.observers:
             k, ns = o.interval, o.n_samples(n_steps)

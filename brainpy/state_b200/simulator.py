@@ -27,6 +27,7 @@ import math
 import numpy as np
 
 from . import _lib
+from . import streams as _streams
 from .units import Hz, Quantity, mV, ms, nS, pA, pF, mantissa
 
 # ----------------------------------------------------------------- models
@@ -271,33 +272,34 @@ class stdp_triplet_synapse:
 # ----------------------------------------------------------- distributions
 
 
-class Uniform:
-    """Uniform(low, high), sampled once at connect (seeded numpy stream)."""
+# The legacy ``_dist.py`` forms (sampled once at connect on the reference's
+# keys; brainpy.state_b200.streams holds the stream restatements).
+_DELAY_STREAM = _streams.DELAY_STREAM
+_INIT_STREAM = _streams.INIT_STREAM
+
+
+class Uniform(_streams.Uniform):
+    """``low + (high - low) * jax.random.uniform(key, shape)`` (_dist.py:66-77)."""
 
     def __init__(self, low, high):
-        self.low, self.high = low, high
-
-    def sample(self, n, rng, unit):
-        lo, hi = mantissa(self.low, unit), mantissa(self.high, unit)
-        return lo + (hi - lo) * rng.random(n)
+        super().__init__(low, high, legacy=True)
 
 
-class Normal:
-    def __init__(self, mean, std):
-        self.mean, self.std = mean, std
-
-    def sample(self, n, rng, unit):
-        return mantissa(self.mean, unit) + mantissa(self.std, unit) * rng.standard_normal(n)
-
-
-class LogNormal:
-    """exp(mean + std * N(0, 1)) (_dist.py LogNormal)."""
+class Normal(_streams.Normal):
+    """``mean + std * jax.random.normal(key, shape)`` (_dist.py:37-52)."""
 
     def __init__(self, mean, std):
-        self.mean, self.std = float(mean), float(std)
+        super().__init__(mean, std, legacy=True)
 
-    def sample(self, n, rng, unit):
-        return np.exp(self.mean + self.std * rng.standard_normal(n))
+
+class LogNormal(_streams.LogNormal):
+    """``exp(mean + std * jax.random.normal(key, shape))`` (_dist.py:55-63)."""
+
+    def __init__(self, mean, std):
+        super().__init__(mean, std, legacy=True)
+
+
+_DISTS = (_streams.Distribution,)
 
 
 # ----------------------------------------------------------------- views
@@ -537,15 +539,17 @@ class Simulator:
             return None
         full_pre = ps.indices.size == src.n and np.all(ps.indices == np.arange(src.n))
         pseed = self._derive_seed(seed, ordinal)
-        rng = np.random.default_rng(pseed)
+        # the projection's keys: k_conn, k_w, k_rec = split(key(seed), 3)
+        # (_nest_network/event_proj.py:147-149); distributed weights draw from
+        # k_w, one value per edge in the sampler's order, before the CSR sort
+        pkey = _streams.root_key(pseed)
+        k_w = _streams.fold_in(pkey, 1)
         receptor = self._receptor(receptor_type)
         if isinstance(rule, _FixedIndegree) and full_pre and full_post:
             E = rule.K * dst.n
-            dl = self._delays(delay, E, rng)
-            if isinstance(weight, (Uniform, Normal, LogNormal)):
-                # edges from the library's sampler, weights drawn per edge in
-                # CSR order from this projection's seeded stream
-                wv = np.asarray(weight.sample(E, rng, w_unit), dtype=np.float64)
+            dl = self._delays(delay, E, pkey)
+            if isinstance(weight, _DISTS):
+                wv = np.asarray(weight.sample_in(k_w, E, w_unit, self._bits), dtype=np.float64)
             else:
                 wv = float(mantissa(weight if weight is not None else 1.0, w_unit))
             op = ("fixed_indegree", src.pop_id, dst.pop_id, rule.K, pseed, allow_autapses, wv,
@@ -568,12 +572,12 @@ class Simulator:
         else:
             raise TypeError(f"unsupported rule {rule!r}")
         E = pre_l.size
-        if isinstance(weight, (Uniform, Normal, LogNormal)):
-            w = weight.sample(E, rng, w_unit)
+        if isinstance(weight, _DISTS):
+            w = weight.sample_in(k_w, E, w_unit, self._bits)
         else:
             w = np.broadcast_to(mantissa(weight if weight is not None else 1.0, w_unit),
                                 (E,)).astype(np.float64)
-        dl = self._delays(delay, E, rng)
+        dl = self._delays(delay, E, pkey)
         order = np.argsort(pre_l, kind="stable")
         indptr = np.concatenate([[0], np.cumsum(np.bincount(pre_l, minlength=src.n))])
         self._ops.append(("csr", src.pop_id, dst.pop_id, indptr.astype(np.int64),
@@ -581,11 +585,21 @@ class Simulator:
                           dl[order].astype(np.int32), receptor, synapse))
         return _ProjHandle(len([o for o in self._ops if o[0] != "drive"]) - 1, E)
 
-    def _delays(self, delay, E, rng):
+    @property
+    def _bits(self):
+        return 64 if self.precision == 64 else 32
+
+    def _delays(self, delay, E, pkey):
+        """Delay steps of E edges (sampler order).  Per-edge delay
+        distributions have no counterpart in the legacy reference (its delays
+        are one value per projection, _nest_network/delay.py:29-128); they
+        draw from fold(key(seed), DELAY_STREAM) of the projection so a run is
+        reproducible."""
         if delay is None:
             steps = np.zeros(E, np.int64)
-        elif isinstance(delay, (Uniform, Normal, LogNormal)):
-            steps = self._steps(delay.sample(E, rng, ms))
+        elif isinstance(delay, _DISTS):
+            d = delay.sample_in(_streams.fold_in(pkey, _DELAY_STREAM), E, ms, self._bits)
+            steps = self._steps(d)
         else:
             steps = np.broadcast_to(self._steps(mantissa(delay, ms)), (E,)).astype(np.int64)
         if self.delivery == "nest" and np.any(steps < 1):
@@ -603,7 +617,9 @@ class Simulator:
         return ops[h.proj_id][-1] is not None
 
     # -- build
-    def _build(self):
+    def _build(self, upload=True):
+        """The library plan of the network; ``upload=False`` stops before the
+        device (the realised structure stays readable through ``Plan.csr``)."""
         if self._model is None:
             raise RuntimeError("no neuron population")
         sem = _lib.LEGACY if self.delivery == "legacy" else _lib.RING
@@ -621,9 +637,8 @@ class Simulator:
                 nbits = 64 if self.precision == 64 else 32
                 per_edge = isinstance(w, np.ndarray)
                 j = pl.add_fixed_indegree(a, b, K, seed, 1.0 if per_edge else w, delay_steps=dl,
-                                          allow_autapses=auto, nbits=nbits, receptor=rec)
-                if per_edge:
-                    pl.set_weights(j, w)
+                                          allow_autapses=auto, nbits=nbits, receptor=rec,
+                                          w_draw=w if per_edge else None)
                 self._attach(pl, j, syn)
             else:
                 _, a, b, indptr, post, w, dl, rec, syn = op
@@ -644,6 +659,8 @@ class Simulator:
                   for pop, idx in segs]
         pl.record_spikes_of(np.unique(np.concatenate(tapped)).astype(np.int32) if tapped
                             else np.zeros(0, np.int32))
+        if not upload:
+            return pl
         pl.upload()
         self._plan = pl
         return pl
@@ -661,8 +678,13 @@ class Simulator:
                 v = np.full(p.n, p.spec.v_init_const)
             elif init is None:
                 v = np.full(p.n, p.params[p.spec.order.index(p.spec.v_default)])
-            elif isinstance(init, (Uniform, Normal)):
-                v = init.sample(p.n, np.random.default_rng(1_000_003 + p.pop_id), mV)
+            elif isinstance(init, _DISTS):
+                # the reference draws V_initializer from brainstate's global
+                # random state, which no Simulator seed sets; the facade draws
+                # it from fold(fold(key(0), INIT_STREAM), population ordinal)
+                k = _streams.fold_in(_streams.fold_in(_streams.root_key(0), _INIT_STREAM),
+                                     p.pop_id)
+                v = init.sample_in(k, p.n, mV, self._bits)
             elif callable(init):
                 v = np.broadcast_to(np.asarray(init(p.n), np.float64), (p.n,))
             else:

@@ -127,6 +127,16 @@ int bspk_proj_add_fixed_indegree(bspk_plan *plan, int pre_pop, int post_pop, int
                                  const int32_t *delay_steps, int delay_const, int receptor,
                                  int *proj_id);
 
+/* The same with per-edge weights w_draw[n_post * K] in the sampler's edge
+ * order (post-major, draw order, before the CSR sort) -- the order in which
+ * the reference draws distributed weights from the projection's k_w key
+ * (_nest_network/event_proj.py:148-149, 286-291); NULL means `weight` for
+ * every edge.  delay_steps, when given, is in the same order. */
+int bspk_proj_add_fixed_indegree_w(bspk_plan *plan, int pre_pop, int post_pop, int K,
+                                   int64_t seed, int allow_autapses, int nbits, double weight,
+                                   const double *w_draw, const int32_t *delay_steps,
+                                   int delay_const, int receptor, int *proj_id);
+
 /* Poisson drive, one independent train per target neuron of post_pop (the
  * Simulator realises a generator per target, simulator.py:1437-1463):
  * count ~ Poisson(rate*dt/1000) per step, active iff t_min < step <= t_max
@@ -260,6 +270,10 @@ int64_t bspk_step_count(bspk_plan *plan);
  * memory), "exact" (deterministic FP64 pull), "per_step" (conductance
  * models, separate ports or plasticity); "" before upload. */
 const char *bspk_plan_engine(bspk_plan *plan);
+/* The tiled kernel sums arrivals in fixed point: weights are rounded once to
+ * rint(w * 2^k) (int32 for FP32 plans, int64 for FP64 plans) with k chosen so
+ * that no ring slot can overflow; *bits = k of an uploaded tiled plan. */
+int bspk_plan_ring_fraction_bits(bspk_plan *plan, int *bits);
 
 /* Timing of the dominant kernel of the last bspk_run (CUDA events on the
  * launching stream): total ms and number of launches. */

@@ -21,6 +21,7 @@ reference's streams, with no call into the product library:
 """
 from __future__ import annotations
 
+import math
 import zlib
 
 import numpy as np
@@ -29,6 +30,34 @@ from . import oracle as O
 
 INIT_STREAM = 0xFFFFFFFE
 DELAY_STREAM = 0xFFFFFFFC
+
+
+def psp_norm(tau_mem, c_mem, tau_syn):
+    """PSC amplitude (pA) of a 1 mV alpha-PSP peak
+    (_kernel/validation/brunel.py:25-36)."""
+    from scipy.special import lambertw
+    a = tau_mem / tau_syn
+    b = 1.0 / tau_syn - 1.0 / tau_mem
+    x = -math.exp(-1.0 / a) / a
+    t_max = 1.0 / b * (-lambertw(x, k=-1 if x < 0 else 0).real - 1.0 / a)
+    return (math.exp(1.0) / (tau_syn * c_mem * b)
+            * ((math.exp(-t_max / tau_mem) - math.exp(-t_max / tau_syn)) / b
+               - t_max * math.exp(-t_max / tau_syn)))
+
+
+def brunel_params(order, g=5.0, eta=2.0, epsilon=0.1, V_reset=10.0):
+    """Sizes, in-degrees, weights (pA) and Poisson rate (Hz) of Brunel model A
+    (_kernel/validation/brunel.py:39-56); neuron parameters in the library's
+    iaf_psc_alpha order (E_L C_m tau_m t_ref V_th V_reset tau_syn_ex tau_syn_in
+    I_e V_min) with the configuration's V_reset."""
+    ne, ni = 4 * order, order
+    ce, ci = int(epsilon * ne), int(epsilon * ni)
+    tau_syn, tau_mem, c_mem, theta = 0.5, 20.0, 250.0, 20.0
+    j_ex = 0.1 / psp_norm(tau_mem, c_mem, tau_syn)
+    nu_th = (theta * c_mem) / (j_ex * ce * math.exp(1) * tau_mem * tau_syn)
+    return dict(NE=ne, NI=ni, CE=ce, CI=ci, J_ex=j_ex, J_in=-g * j_ex,
+                rate=1000.0 * eta * nu_th * ce,
+                neuron=[0.0, c_mem, tau_mem, 2.0, theta, V_reset, tau_syn, tau_syn, 0.0, -math.inf])
 
 
 def object_key(seed, name):

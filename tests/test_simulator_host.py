@@ -39,3 +39,29 @@ def test_validation():
     a = nest.create(iaf_psc_alpha, 3)
     with pytest.raises(ValueError, match="delays"):
         nest.connect(a, a, weight=1.0 * pA, delay=0.0 * ms, rule=all_to_all)
+
+
+def test_distributed_weights_follow_the_reference_k_w_stream(oracle):
+    """connect(weight=Uniform(...), rule=fixed_indegree(K), seed=s): the
+    reference draws the weights from k_w = split(key(derived seed), 3)[1] in
+    the sampler's post-major edge order, as low + (high - low) * uniform01 in
+    float32, and sorts them into CSR order with the edges
+    (_nest_network/event_proj.py:147-149, 286-291; _dist.py:66-77).  The
+    realised CSR weights must equal the oracle's restatement bit for bit."""
+    from brainpy.state_b200.units import pA
+    sim = Simulator(dt=0.1 * ms)
+    a = sim.create(iaf_psc_alpha, 120)
+    sim.connect(a, a, weight=Uniform(10.0 * pA, 30.0 * pA), delay=1.5 * ms,
+                rule=fixed_indegree(9), seed=5)
+    pl = sim._build(upload=False)
+    indptr, post, _, w = pl.csr(0)
+    pseed = (5 * 1_000_003 + 0 + 1) & 0x7FFFFFFF
+    pre_o, post_o = oracle.fixed_indegree(pseed, 120, 120, 9, pre_is_post=True,
+                                          allow_autapses=True)
+    order, idx, iptr = oracle.csr_structure(pre_o, post_o, 120)
+    k_w = oracle.jax_fold_in(oracle.jax_key(pseed), 1)
+    u = oracle.jax_uniform(k_w, pre_o.size, 32, 0.0, 1.0).astype(np.float32)
+    w_draw = np.float32(10.0) + np.float32(20.0) * u
+    np.testing.assert_array_equal(iptr, indptr)
+    np.testing.assert_array_equal(idx, post)
+    np.testing.assert_array_equal(w, w_draw[order].astype(np.float64))
