@@ -509,10 +509,13 @@ def bptt_numbers(args):
                             "grads_per_s": round(1000.0 / (fw + bw), 3),
                             "trial_steps_per_s": round(64 * 1000 * 1000.0 / (fw + bw), 1)}
         adj.close()
-    # finite differences, h = 1e-3, 64 random weights
+    # finite differences on 64 random weights (32 recurrent, 32 input) at the
+    # configured 1000 steps, FP64, relaxed forward with t_ref = 0 (smooth in
+    # the weights): central differences with the configuration's h = 1e-3 and
+    # with h = 1e-5 (inside the linear range of the relaxed soft reset)
     params = list(T["cfg"]["params"])
     params[3] = 0.0
-    Tf = make_task(relaxed=True, params=params, n_steps=200)
+    Tf = make_task(relaxed=True, params=params, n_steps=1000)
     adj = LifAdjoint(Tf["cfg"], Tf["row_ptr"], Tf["col"], precision=64, ckpt_every=50)
     w = torch.tensor(Tf["w"], dtype=torch.float64, device="cuda")
     wi = torch.tensor(Tf["w_in"], dtype=torch.float64, device="cuda")
@@ -522,20 +525,25 @@ def bptt_numbers(args):
     dw, dwi = adj.backward()
     dw, dwi = dw.cpu().numpy(), dwi.cpu().numpy().reshape(-1)
     rng = np.random.default_rng(7)
-    a_, f_ = [], []
-    for arr, grad in ((w, dw), (wi.reshape(-1), dwi)):
-        for q in rng.choice(arr.numel(), 32, replace=False):
+    picks = [(w, dw, q) for q in rng.choice(w.numel(), 32, replace=False)] + \
+            [(wi.reshape(-1), dwi, q) for q in rng.choice(wi.numel(), 32, replace=False)]
+    fd = {}
+    for h in (1e-3, 1e-5):
+        a_, f_ = [], []
+        for arr, grad, q in picks:
             wp = arr.clone()
-            wp[q] += 1e-3
+            wp[q] += h
             lp = float(adj.forward(*((wp, wi) if arr is w else (w, wp.reshape(wi.shape))), inp, tg))
-            wp[q] -= 2e-3
+            wp[q] -= 2 * h
             lm = float(adj.forward(*((wp, wi) if arr is w else (w, wp.reshape(wi.shape))), inp, tg))
             a_.append(grad[q])
-            f_.append((lp - lm) / 2e-3)
-    a_, f_ = np.array(a_), np.array(f_)
-    rel = np.abs(a_ - f_) / np.maximum(np.abs(f_), 1e-3 * np.abs(f_).max())
-    res["fd_check"] = {"h": 1e-3, "weights": 64, "steps": 200, "batch": 64, "forward": "relaxed",
-                       "max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel))}
+            f_.append((lp - lm) / (2 * h))
+        a_, f_ = np.array(a_), np.array(f_)
+        rel = np.abs(a_ - f_) / np.maximum(np.abs(f_), 1e-3 * np.abs(f_).max())
+        fd[f"h={h:g}"] = {"max_rel_err": float(rel.max()), "median_rel_err": float(np.median(rel)),
+                          "within_1e-3": int((rel <= 1e-3).sum())}
+    res["fd_check"] = {"weights": 64, "steps": 1000, "batch": 64, "precision": "fp64",
+                       "forward": "relaxed, t_ref = 0", **fd}
     adj.close()
     return res
 

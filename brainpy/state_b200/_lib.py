@@ -103,6 +103,8 @@ def lib():
             "bspk_state_set": (C.c_int, [vp, C.c_int, C.c_char_p, vp]),
             "bspk_step_count": (i64, [vp]),
             "bspk_plan_engine": (C.c_char_p, [vp]),
+            "bspk_record_weights": (C.c_int, [vp, C.c_int, C.c_int]),
+            "bspk_weight_trace_get": (C.c_int, [vp, C.c_int, C.POINTER(i64), vp]),
             "bspk_plan_ring_fraction_bits": (C.c_int, [vp, C.POINTER(C.c_int)]),
             "bspk_last_kernel_time": (C.c_int, [vp, C.POINTER(dbl), C.POINTER(i64)]),
             "bspk_rk_substeps": (C.c_int, [vp, C.POINTER(i64)]),
@@ -387,6 +389,17 @@ class Plan:
         else:
             out = np.empty((self._last_steps, self.n_rec_v), np.float64)
             check(self._L.bspk_v_get(self._h, ptr(out)))
+        return out
+
+    def record_weights(self, proj, on=True):
+        check(self._L.bspk_record_weights(self._h, int(proj), int(bool(on))))
+
+    def weight_trace(self, proj):
+        """(n_steps, n_edges) FP64 weights after every step of the last run."""
+        n = C.c_int64()
+        check(self._L.bspk_weight_trace_get(self._h, int(proj), C.byref(n), None))
+        out = np.empty((n.value, self._proj_edges[proj]), np.float64)
+        check(self._L.bspk_weight_trace_get(self._h, int(proj), C.byref(n), ptr(out)))
         return out
 
     def weights(self, proj):

@@ -64,6 +64,10 @@ struct StdpDev {
     double *pre_trace, *post_trace;    // fast traces
     double *pre_trace2, *post_trace2;  // slow traces (triplet rule)
     int *pre_list, *post_list, *counts;  // counts[0] pres, counts[1] posts of this step
+    // weight trajectory: after every step, row (step - run_step0 - 1) of
+    // wtrace[n_steps][n_edges] receives the weights (nullptr: not recorded)
+    double *wtrace;
+    int64_t n_edges, run_step0;
 };
 
 int run_per_step(bspk_plan *p, int64_t n_steps, cudaStream_t st);

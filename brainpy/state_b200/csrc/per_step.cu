@@ -18,6 +18,7 @@
 // steps is replayed for every chunk of K steps.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -448,6 +449,19 @@ __global__ void __launch_bounds__(256) k_deliver_static(const StepArgs<Real> a) 
 
 // STDP 1: traces decay-then-add (event_plastic.py:390-420); lists of pres
 // whose delayed spike arrives now and of posts that fired at n - 1.
+// Weights of a plastic projection after the step that just closed
+// (*step_ptr already advanced) into its row of the run's trajectory, the
+// counterpart of the reference's per-step weight tap
+// (_nest_network/simulator.py:1868-1880).
+__global__ void k_weight_tap(const double *w, int64_t n_edges, double *wtrace,
+                             const int64_t *step_ptr, int64_t run_step0) {
+    const int64_t row = *step_ptr - 1 - run_step0;
+    double *dst = wtrace + row * n_edges;
+    for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < n_edges;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        dst[e] = w[e];
+}
+
 __global__ void k_stdp_traces(StdpDev s, const uint64_t *hist, const int64_t *step_ptr) {
     const int64_t n = *step_ptr;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -689,6 +703,9 @@ std::vector<StdpDev> stdp_descs(bspk_plan *p) {
         s.pre_list = J.d_pre_list;
         s.post_list = J.d_post_list;
         s.counts = p->d_step_counters + 2 + 2 * k;
+        s.wtrace = J.rec_w ? J.d_wtrace : nullptr;
+        s.n_edges = static_cast<int64_t>(J.post_local.size());
+        s.run_step0 = p->step;
         v.push_back(s);
         ++k;
     }
@@ -716,6 +733,10 @@ cudaError_t enqueue_step(bspk_plan *p, const StepArgs<Real> &a, const std::vecto
     else if (a.model == 4) k_neuron_step<Real, 4><<<nb, 128, 0, st>>>(a, dt);
     else k_neuron_step<Real, 5><<<nb, 128, 0, st>>>(a, dt);
     k_deliver_static<Real><<<p->sm_count * 4, 256, 0, st>>>(a);
+    for (const StdpDev &s : sd)
+        if (s.wtrace && s.n_edges > 0)
+            k_weight_tap<<<static_cast<int>(std::min<int64_t>(p->sm_count * 4, (s.n_edges + 255) / 256)),
+                           256, 0, st>>>(s.w, s.n_edges, s.wtrace, a.step_ptr, s.run_step0);
     return cudaGetLastError();
 }
 
@@ -726,7 +747,9 @@ int run_typed(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
     const StepArgs<Real> a = step_args<Real>(p, p->d_step_ptr);
     const std::vector<StdpDev> sd = stdp_descs(p);
     constexpr int64_t kChunk = 32;
-    const int kernels_per_step = 2 + 3 * static_cast<int>(sd.size());
+    int taps = 0;
+    for (const StdpDev &s : sd) taps += s.wtrace && s.n_edges > 0 ? 1 : 0;
+    const int kernels_per_step = 2 + 3 * static_cast<int>(sd.size()) + taps;
     int64_t done = 0;
     if (n_steps >= kChunk) {
         // capture kChunk steps once per run (the arguments embed this run's

@@ -1323,6 +1323,22 @@ extern "C" int bspk_run(bspk_plan *p, int64_t n_steps, void *stream) {
     bool per_step = plan_per_step(p);
     for (auto &J : p->projs) per_step |= J.plastic;
     if (p->tiled) BSPK_CUDA(cudaMemsetAsync(p->d_trec, 0, sizeof(long long) * p->grid, st));
+    for (auto &J : p->projs) {
+        if (!J.rec_w) continue;
+        const int64_t need = n_steps * static_cast<int64_t>(J.post_local.size());
+        if (need > J.wtrace_cap) {
+            if (J.d_wtrace) {
+                cudaFree(J.d_wtrace);
+                p->allocs.erase(std::remove(p->allocs.begin(), p->allocs.end(), J.d_wtrace),
+                                p->allocs.end());
+                J.d_wtrace = nullptr;
+            }
+            int rc = dalloc(p, &J.d_wtrace, need);
+            if (rc) return rc;
+            J.wtrace_cap = need;
+        }
+        J.wtrace_steps = n_steps;
+    }
     if (per_step) {
         int rc = run_per_step(p, n_steps, st);
         if (rc) return rc;
@@ -1552,6 +1568,30 @@ int bspk_state_set(bspk_plan *p, int pop, const char *name, const double *values
 }
 
 int64_t bspk_step_count(bspk_plan *p) { return p ? p->step : -1; }
+
+int bspk_record_weights(bspk_plan *p, int proj_id, int on) {
+    if (!p || proj_id < 0 || proj_id >= static_cast<int>(p->projs.size()))
+        return fail(BSPK_ERR_ARG, "bad projection");
+    if (!p->projs[proj_id].plastic)
+        return fail(BSPK_ERR_ARG, "record_weights needs a plastic projection");
+    p->projs[proj_id].rec_w = on != 0;
+    return BSPK_OK;
+}
+
+int bspk_weight_trace_get(bspk_plan *p, int proj_id, int64_t *n_steps, double *out) {
+    if (!p || proj_id < 0 || proj_id >= static_cast<int>(p->projs.size()))
+        return fail(BSPK_ERR_ARG, "bad projection");
+    Proj &J = p->projs[proj_id];
+    if (!J.rec_w || !J.d_wtrace) return fail(BSPK_ERR_STATE, "no weight trajectory recorded");
+    if (n_steps) *n_steps = J.wtrace_steps;
+    if (!out) return BSPK_OK;
+    int rc = sync_and_check(p);
+    if (rc) return rc;
+    BSPK_CUDA(cudaMemcpy(out, J.d_wtrace,
+                         sizeof(double) * J.wtrace_steps * static_cast<int64_t>(J.post_local.size()),
+                         cudaMemcpyDeviceToHost));
+    return BSPK_OK;
+}
 
 int bspk_plan_ring_fraction_bits(bspk_plan *p, int *bits) {
     if (!p || !bits) return fail(BSPK_ERR_ARG, "null argument");

@@ -51,6 +51,10 @@ struct Proj {
     int64_t *d_cperm = nullptr;     // CSC position -> CSR edge id
     void *d_pre_trace = nullptr, *d_post_trace = nullptr;  // [trace_cols][n]
     int *d_pre_list = nullptr, *d_post_list = nullptr;  // per-step STDP work lists
+    // weight trajectory of the last run (bspk_record_weights): [steps][E]
+    bool rec_w = false;
+    double *d_wtrace = nullptr;
+    int64_t wtrace_cap = 0, wtrace_steps = 0;
 };
 
 struct Drive {

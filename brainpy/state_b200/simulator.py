@@ -659,6 +659,8 @@ class Simulator:
                   for pop, idx in segs]
         pl.record_spikes_of(np.unique(np.concatenate(tapped)).astype(np.int32) if tapped
                             else np.zeros(0, np.int32))
+        for h in self._weight_taps.values():
+            pl.record_weights(h.proj_id)
         if not upload:
             return pl
         pl.upload()
@@ -748,7 +750,8 @@ class Simulator:
             v = pl.v_trace(np.float32 if self.precision == 32 else np.float64)
             for rid, sl in self._v_slices.items():
                 traces[(rid, "V_m")] = v[:, sl]
-        weights = {k: pl.weights(h.proj_id)[None, :] for k, h in self._weight_taps.items()}
+        # (n_steps, n_edges) FP64 weights after every step, CSR order
+        weights = {k: pl.weight_trace(h.proj_id) for k, h in self._weight_taps.items()}
         times = (step0 + np.arange(n)) * self.dt
         return SimulationResult(spikes, traces, events, n * self.dt, self.dt, times, weights)
 

@@ -261,6 +261,15 @@ int bspk_v_get(bspk_plan *plan, double *out);
  * plan, rounded for a precision-64 one). */
 int bspk_v_get_f32(bspk_plan *plan, float *out);
 int bspk_weights_get(bspk_plan *plan, int proj_id, double *w_csr_order);
+/* Per-step weight trajectory of a plastic projection (Simulator.record_weight
+ * and SimulationResult.weight_trace, _nest_network/simulator.py:382-396,
+ * :884-910, :1868-1880): with recording on, every bspk_run stores the FP64
+ * weights after each of its steps, [n_steps][n_edges] in CSR order, on the
+ * device (n_steps * n_edges * 8 bytes).  weight_trace_get synchronises and
+ * copies the last run's trajectory (*n_steps = its length; out may be NULL to
+ * query it). */
+int bspk_record_weights(bspk_plan *plan, int proj_id, int on);
+int bspk_weight_trace_get(bspk_plan *plan, int proj_id, int64_t *n_steps, double *out);
 int bspk_state_get(bspk_plan *plan, int pop, const char *name, double *values);
 int bspk_state_set(bspk_plan *plan, int pop, const char *name, const double *values);
 int64_t bspk_step_count(bspk_plan *plan);

@@ -217,3 +217,52 @@ def test_stdp_synapse_hom_is_the_pair_rule():
         out.append(sim._plan.weights(proj.proj_id))
     assert np.any(out[0] != 20.68)
     np.testing.assert_array_equal(out[0], out[1])
+
+
+def test_weight_trace_per_step_matches_oracle(oracle):
+    """record_weight / weight_trace: the (n_steps, n_edges) FP64 trajectory of
+    a plastic projection after every step (_nest_network/simulator.py:382-396,
+    :1868-1880), CSR order, against the oracle stepped one step at a time;
+    two runs in a row (the second continues the first)."""
+    rng = np.random.default_rng(23)
+    NE, NI, J = 120, 30, 20.68
+    params = [0.0, 250.0, 20.0, 2.0, 20.0, 10.0, 0.5, 0.5, 0.0, -math.inf]
+    pieces = []
+    for pre, K, w in ((0, 15, J), (1, 4, -5.0 * J)):
+        for post in (0, 1):
+            n_pre, n_post = (NE if pre == 0 else NI), (NE if post == 0 else NI)
+            pieces.append((pre, post) + random_csr(rng, n_pre, n_post, K, w, 15))
+    v0 = rng.uniform(0.0, 20.0, NE + NI)
+
+    def build(s, is_plan):
+        s.add_pop(NE, params)
+        s.add_pop(NI, params)
+        (s.add_poisson if is_plan else s.add_drive)(0, 17789.0, 20.68, 15, 5)
+        (s.add_poisson if is_plan else s.add_drive)(1, 17789.0, 20.68, 15, 6)
+        ids = [(s.add_csr if is_plan else s.add_proj)(pre, post, indptr, idx, w, d)
+               for pre, post, indptr, idx, w, d in pieces]
+        (s.attach_stdp if is_plan else s.set_stdp)(ids[0], 20.0, 20.0, 0.05, 1.0, 1.0, 1.0,
+                                                   3 * J)
+        return ids
+
+    pl = _lib.Plan(0.1, precision=64)
+    ids = build(pl, True)
+    pl.record_weights(ids[0])
+    pl.upload()
+    pl.set_state(0, "V_m", v0[:NE])
+    pl.set_state(1, "V_m", v0[NE:])
+    sim = oracle.OracleSim(0.1)
+    build(sim, False)
+    sim.set_state(0, "V_m", v0[:NE])
+    sim.set_state(1, "V_m", v0[NE:])
+    E = pieces[0][3].size
+    for n in (70, 45):
+        pl.run(n)
+        tr = pl.weight_trace(ids[0])
+        assert tr.shape == (n, E)
+        ref = np.empty((n, E))
+        for k in range(n):
+            sim.run(1)
+            ref[k] = sim.weights(0 + 2, E)   # oracle ids count the drives
+        np.testing.assert_allclose(tr, ref, rtol=1e-12, atol=0)
+    assert np.any(ref[-1] != J)
