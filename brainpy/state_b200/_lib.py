@@ -145,6 +145,10 @@ def lib():
             "bspk_xla_adjoint_forward": (None, [vp, vp, C.c_char_p, C.c_size_t]),
             "bspk_xla_adjoint_backward": (None, [vp, vp, C.c_char_p, C.c_size_t]),
             "bspk_xla_run": (None, [vp, vp, C.c_char_p, C.c_size_t]),
+            "bspk_xla_step": (None, [vp, vp, C.c_char_p, C.c_size_t]),
+            "bspk_step_fused": (C.c_int, [vp, vp]),
+            "bspk_adjoint_sizes": (C.c_int, [vp, C.POINTER(i64), C.POINTER(i64),
+                                             C.POINTER(C.c_int)]),
             "bspk_xla_batch_run": (None, [vp, vp, C.c_char_p, C.c_size_t]),
         }
         for name, (res, args) in sig.items():

@@ -529,6 +529,15 @@ struct bspk_adjoint {
     bool have_forward = false;
 };
 
+extern "C" int bspk_adjoint_sizes(const bspk_adjoint *adj, int64_t *nnz, int64_t *n_w_in,
+                                  int *precision) {
+    if (!adj) return bspk::fail(BSPK_ERR_ARG, "null handle");
+    if (nnz) *nnz = adj->nnz;
+    if (n_w_in) *n_w_in = static_cast<int64_t>(adj->cfg.n) * adj->cfg.n_in;
+    if (precision) *precision = adj->cfg.precision;
+    return BSPK_OK;
+}
+
 namespace {
 
 int aalloc(bspk_adjoint *h, void **p, size_t bytes) {

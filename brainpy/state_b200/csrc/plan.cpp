@@ -1569,6 +1569,8 @@ int bspk_state_set(bspk_plan *p, int pop, const char *name, const double *values
 
 int64_t bspk_step_count(bspk_plan *p) { return p ? p->step : -1; }
 
+int bspk_step_fused(bspk_plan *p, void *stream) { return bspk_run(p, 1, stream); }
+
 int bspk_record_weights(bspk_plan *p, int proj_id, int on) {
     if (!p || proj_id < 0 || proj_id >= static_cast<int>(p->projs.size()))
         return fail(BSPK_ERR_ARG, "bad projection");

@@ -17,7 +17,8 @@ import jax.numpy as jnp
 from . import _lib
 
 _TARGETS = ("bspk_xla_adjoint_forward", "bspk_xla_adjoint_backward", "bspk_xla_run",
-            "bspk_xla_batch_run")
+            "bspk_xla_step", "bspk_xla_batch_run")
+_STATUS = jax.ShapeDtypeStruct((), jnp.int32)
 _registered = False
 
 
@@ -52,17 +53,20 @@ def lif_bptt_loss(adj):
 
     @jax.custom_vjp
     def loss_fn(w, w_in, inputs, targets):
-        return _call("bspk_xla_adjoint_forward", jax.ShapeDtypeStruct((), jnp.float64), op,
-                     w, w_in, inputs, targets).astype(real)
+        loss, _status = _call("bspk_xla_adjoint_forward",
+                              (jax.ShapeDtypeStruct((), jnp.float64), _STATUS), op,
+                              w, w_in, inputs, targets)
+        return loss.astype(real)   # NaN when the call failed
 
     def fwd(w, w_in, inputs, targets):
         return loss_fn(w, w_in, inputs, targets), (w, w_in, inputs, targets)
 
     def bwd(res, g):
         w, w_in, inputs, targets = res
-        dw, dwi = _call("bspk_xla_adjoint_backward",
-                        (jax.ShapeDtypeStruct(w.shape, real), jax.ShapeDtypeStruct(w_in.shape, real)),
-                        op, w, w_in, inputs, targets)
+        dw, dwi, _status = _call("bspk_xla_adjoint_backward",
+                                 (jax.ShapeDtypeStruct(w.shape, real),
+                                  jax.ShapeDtypeStruct(w_in.shape, real), _STATUS),
+                                 op, w, w_in, inputs, targets)
         return dw * g, dwi * g, None, None
 
     loss_fn.defvjp(fwd, bwd)
@@ -70,13 +74,21 @@ def lif_bptt_loss(adj):
 
 
 def run(plan, n_steps):
-    """Advance a plan inside a jitted program; returns the plan's step counter."""
+    """Advance a plan inside a jitted program; returns (step counter, status)."""
     register()
-    return _call("bspk_xla_run", jax.ShapeDtypeStruct((), jnp.int64), _opaque(plan._h, n_steps))
+    return _call("bspk_xla_run", (jax.ShapeDtypeStruct((), jnp.int64), _STATUS),
+                 _opaque(plan._h, n_steps))
+
+
+def step(plan):
+    """One step of a plan (bspk_step_fused); returns (step counter, status)."""
+    register()
+    return _call("bspk_xla_step", (jax.ShapeDtypeStruct((), jnp.int64), _STATUS),
+                 _opaque(plan._h))
 
 
 def batch_run(batch, n_steps):
-    """Advance a batch inside a jitted program; returns its step counter."""
+    """Advance a batch inside a jitted program; returns (step counter, status)."""
     register()
-    return _call("bspk_xla_batch_run", jax.ShapeDtypeStruct((), jnp.int64),
+    return _call("bspk_xla_batch_run", (jax.ShapeDtypeStruct((), jnp.int64), _STATUS),
                  _opaque(batch._h, n_steps))

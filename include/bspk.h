@@ -250,6 +250,9 @@ int bspk_plan_upload(bspk_plan *plan, void *stream);
 /* Advance n_steps (Simulator.simulate/cont, simulator.py:1790-1883; kernel
  * Program.rollout, _kernel/runner.py:689-779).  Asynchronous on `stream`. */
 int bspk_run(bspk_plan *plan, int64_t n_steps, void *stream);
+/* One step of the network (the single-step target a jax.ffi program calls
+ * inside its own loop; bspk_run(plan, 1, stream)). */
+int bspk_step_fused(bspk_plan *plan, void *stream);
 
 /* Synchronise and copy out what the last bspk_run recorded.
  * spikes: (step, gid) pairs in no particular order, *n_out = count. */
@@ -401,6 +404,9 @@ int bspk_adjoint_forward(bspk_adjoint *adj, const void *w, const void *w_in,
                          const uint8_t *inputs, const void *targets, double *loss,
                          int64_t *n_spikes, void *stream);
 int bspk_adjoint_backward(bspk_adjoint *adj, void *dw, void *dw_in, void *stream);
+/* Element counts of the gradient operands (nnz recurrent weights, n * n_in
+ * input weights) and the precision (32 / 64) of a handle. */
+int bspk_adjoint_sizes(const bspk_adjoint *adj, int64_t *nnz, int64_t *n_w_in, int *precision);
 
 /* No-allocation entry point (no counterpart in the reference).  For callers
  * that cannot call cudaMalloc -- code running inside another framework's

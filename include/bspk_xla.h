@@ -17,15 +17,22 @@
 extern "C" {
 #endif
 
-/* buffers [w, w_in, inputs, targets | loss];  opaque: bspk_adjoint* */
+/* Every target ends its outputs with an int32 status (0 = ok, else a BSPK_ERR_*
+ * code), written on the call's stream; on failure the other outputs hold NaN
+ * (losses, gradients) or -1 (step counters).  No target synchronises. */
+/* buffers [w, w_in, inputs, targets | loss, status];  opaque: bspk_adjoint* */
 void bspk_xla_adjoint_forward(void *stream, void **buffers, const char *opaque, size_t len);
-/* buffers [w, w_in, inputs, targets | dw, dw_in];  opaque: bspk_adjoint* (the forward pass
- * is recomputed inside the call) */
+/* buffers [w, w_in, inputs, targets | dw, dw_in, status];  opaque: bspk_adjoint* (the
+ * forward pass is recomputed inside the call) */
 void bspk_xla_adjoint_backward(void *stream, void **buffers, const char *opaque, size_t len);
-/* buffers [| step];  opaque: bspk_plan*, int64 n_steps (Simulator.simulate/cont,
+/* buffers [| step, status];  opaque: bspk_plan*, int64 n_steps (Simulator.simulate/cont,
  * _nest_network/simulator.py:1790-1883) */
 void bspk_xla_run(void *stream, void **buffers, const char *opaque, size_t len);
-/* buffers [| step];  opaque: bspk_batch*, int64 n_steps */
+/* buffers [| step, status];  opaque: bspk_plan*.  One step (bspk_step_fused): the
+ * single-step target for programs whose time loop stays in JAX (the reference's
+ * scan body, _kernel/runner.py:571-674) */
+void bspk_xla_step(void *stream, void **buffers, const char *opaque, size_t len);
+/* buffers [| step, status];  opaque: bspk_batch*, int64 n_steps */
 void bspk_xla_batch_run(void *stream, void **buffers, const char *opaque, size_t len);
 
 #ifdef __cplusplus

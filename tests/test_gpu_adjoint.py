@@ -175,16 +175,58 @@ def test_xla_custom_call_targets_match_the_c_abi():
     loss = torch.zeros((), dtype=dt, device="cuda")
     dw = torch.zeros_like(w)
     dwi = torch.zeros_like(wi)
+    st1 = torch.full((), -99, dtype=torch.int32, device="cuda")
+    st2 = torch.full((), -99, dtype=torch.int32, device="cuda")
     L = _lib.lib()
     st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     op = struct.pack("<Q", adj._h.value)
-    bufs = (C.c_void_p * 5)(*[t.data_ptr() for t in (w, wi, inp, tg, loss)])
+    bufs = (C.c_void_p * 6)(*[t.data_ptr() for t in (w, wi, inp, tg, loss, st1)])
     L.bspk_xla_adjoint_forward(st, bufs, op, len(op))
-    bufs = (C.c_void_p * 6)(*[t.data_ptr() for t in (w, wi, inp, tg, dw, dwi)])
+    bufs = (C.c_void_p * 7)(*[t.data_ptr() for t in (w, wi, inp, tg, dw, dwi, st2)])
     L.bspk_xla_adjoint_backward(st, bufs, op, len(op))
     torch.cuda.synchronize()
     ref = _gpu(T)
+    assert int(st1) == 0 and int(st2) == 0
     assert float(loss) == ref[0]
     np.testing.assert_array_equal(dw.cpu().numpy(), ref[1])
     np.testing.assert_array_equal(dwi.cpu().numpy(), ref[2])
+    # a bad opaque (null handle): status BSPK_ERR_ARG, NaN loss, no hang
+    bad = struct.pack("<Q", 0)
+    bufs = (C.c_void_p * 6)(*[t.data_ptr() for t in (w, wi, inp, tg, loss, st1)])
+    L.bspk_xla_adjoint_forward(st, bufs, bad, len(bad))
+    torch.cuda.synchronize()
+    assert int(st1) == -1 and torch.isnan(loss).item()
     adj.close()
+
+
+def test_xla_run_and_step_targets_write_step_and_status():
+    """bspk_xla_run / bspk_xla_step as XLA calls them: the step counter and a
+    zero status land in device buffers without a host synchronisation; the
+    states equal a plan advanced through bspk_run; a null plan gives status
+    BSPK_ERR_ARG and step -1."""
+    import ctypes as C
+    import struct
+    from brainpy.state_b200 import _lib
+    from tests.netbuild import Net
+    L = _lib.lib()
+    net = Net()
+    a, b = net.to_plan(precision=64), net.to_plan(precision=64)
+    step = torch.zeros((), dtype=torch.int64, device="cuda")
+    status = torch.full((), -99, dtype=torch.int32, device="cuda")
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    bufs = (C.c_void_p * 2)(step.data_ptr(), status.data_ptr())
+    op = struct.pack("<Qq", a._h.value, 40)
+    L.bspk_xla_run(st, bufs, op, len(op))
+    torch.cuda.synchronize()
+    assert int(step) == 40 and int(status) == 0
+    one = struct.pack("<Q", a._h.value)
+    for k in range(3):
+        L.bspk_xla_step(st, bufs, one, len(one))
+    torch.cuda.synchronize()
+    assert int(step) == 43 and int(status) == 0
+    b.run(43)
+    np.testing.assert_array_equal(a.get_state(0, "V_m"), b.get_state(0, "V_m"))
+    bad = struct.pack("<Qq", 0, 10)
+    L.bspk_xla_run(st, bufs, bad, len(bad))
+    torch.cuda.synchronize()
+    assert int(step) == -1 and int(status) == -1
