@@ -404,6 +404,21 @@ def sweep_numbers(args):
     r32, r64 = np.array(r32), np.array(r64)
     err = np.abs(r32 - r64) / np.maximum(r64, 1e-12)
     ms32 = out[32]["ms"]
+    # per-instance rate error of the FP32 batch against the float64 oracle on
+    # the same instance (connectivity, drive stream and V_m), for instances
+    # spread over the size range (the oracle cannot run all 256 in minutes)
+    from oracle import sweep_net
+    order = np.argsort([s["NE"] for s in specs])
+    pick = order[np.linspace(0, len(specs) - 1, 8).astype(int)]
+    orc = []
+    for k in pick:
+        osim, _ = sweep_net.build(specs[k], threads=_host_threads())
+        ref = osim.run(steps, cap=1 << 23)[0].size
+        n = specs[k]["NE"] + specs[k]["NI"]
+        orc.append({"instance": int(k), "N": int(n), "rate_hz_fp32": round(float(r32[k]), 4),
+                    "rate_hz_oracle": round(ref / n, 4),
+                    "rel_err": round(abs(float(r32[k]) * n - ref) / max(ref, 1), 5)})
+    orc_err = np.array([o["rel_err"] for o in orc])
     return {"workload": "256 Brunel instances, NE~U[500,8000], NI=NE/4, eps=0.1, g~U[3,8], "
                         "eta~U[0.9,4], delay 1.5 ms, 1000 ms each, one persistent launch",
             "neurons": int(N), "edges": int(edges),
@@ -414,7 +429,13 @@ def sweep_numbers(args):
             "rate_hz_median": round(float(np.median(r64)), 3),
             "rate_rel_err_median": round(float(np.median(err)), 5),
             "rate_rel_err_max": round(float(err.max()), 5),
-            "within_1pct": int((err <= 0.01).sum()), "within_5pct": int((err <= 0.05).sum())}
+            "within_1pct": int((err <= 0.01).sum()), "within_5pct": int((err <= 0.05).sum()),
+            "vs_oracle": {"instances": orc, "rel_err_median": round(float(np.median(orc_err)), 5),
+                          "rel_err_max": round(float(orc_err.max()), 5),
+                          "oracle": "float64 oracle, same instance realised independently, "
+                                    "1000 ms"},
+            "vs_fp64_note": "rate_rel_err_* compare the FP32 batch with the FP64 batch of the "
+                            "same 256 instances"}
 
 
 def sweep_sharded(rank, world):
@@ -458,15 +479,45 @@ def adex_numbers(args):
     wall = time.perf_counter() - t0
     kms, launches = sim._plan.kernel_time()
     spk = res.spikes(h["rec"])
+    par = adex_parity()
     return {"workload": "16000E+4000I aeif_cond_alpha, in-degree 1600 E + 400 I, lognormal "
                         "weights (ln 1 nS, 0.5), E->E stdp_synapse (25.6 M edges), 5 kHz drive "
                         "of 6 nS, RKF45 tol 1e-6, 2000 ms, FP32 stages / FP64 error control",
+            "parity": par,
             "ms_per_simulated_s": round(kms / 2.0, 2),
             "rtf": round(2000.0 / kms, 4),
             "rate_hz_sampled": round(float(spk.sum()) / spk.shape[1] / 2.0, 3),
             "rk_substeps_per_neuron_step": round(
                 sim._plan.rk_substeps() / float((h["NE"] + h["NI"]) * 20000), 3),
             "build_and_run_wall_s": round(wall, 2)}
+
+
+def adex_parity(scale=0.1, seconds=1):
+    """The same AdEx + STDP network at `scale` (NE = 16000 scale, in-degrees
+    10 %), FP32 on the GPU against the float64 oracle on the same realised
+    network (oracle/mirror.py): population rate over `seconds` s and the mean
+    E->E weight at the end."""
+    from brainpy.state_b200 import adex_net
+    from brainpy.state_b200.units import ms
+    from oracle import mirror
+    sim, h = adex_net.build(scale=scale, precision=32)
+    sim.simulate(0.0 * ms)
+    osim, pids = mirror.from_simulator(sim, threads=_host_threads())
+    n = h["NE"] + h["NI"]
+    res = sim.cont(seconds * 1000.0 * ms)
+    count = float(res.spikes(h["rec"]).sum())
+    w_gpu = sim._plan.weights(h["ee"].proj_id)
+    t0 = time.perf_counter()
+    ref = 0
+    for _ in range(seconds):
+        ref += osim.run(10000, cap=1 << 22)[0].size
+    wall = time.perf_counter() - t0
+    w_ref = osim.weights(pids[0], w_gpu.size)
+    return {"scale": scale, "neurons": n, "seconds": seconds,
+            "rate_hz": round(count / n / seconds, 4), "oracle_rate_hz": round(ref / n / seconds, 4),
+            "rate_rel_err": round(abs(count - ref) / max(ref, 1), 5),
+            "mean_ee_weight_nS": float(w_gpu.mean()),
+            "oracle_mean_ee_weight_nS": float(w_ref.mean()), "oracle_wall_s": round(wall, 2)}
 
 
 def bptt_numbers(args):

@@ -31,3 +31,24 @@ def test_full_size_adex_stdp_network_runs_and_keeps_weights_bounded():
     # facilitation stops at Wmax, depression at 0: a changed weight never
     # leaves [0, max(w0, Wmax)]
     assert np.all(w[changed] <= np.maximum(w0[changed], h["Wmax"]) + 1e-12)
+
+
+def test_scaled_adex_stdp_network_fp32_rate_close_to_oracle(oracle):
+    """The same network at scale 0.05 (800 E + 200 I, in-degrees 80 + 20),
+    FP32 stages with FP64 error control and FP64 plastic weights, against the
+    float64 oracle on the identical realised network (oracle/mirror.py), 500 ms:
+    population rates within 5 % (the network is chaotic: trajectories separate,
+    the rate does not) and mean plastic weight within 2 %."""
+    import os
+    from oracle import mirror
+    sim, h = adex_net.build(scale=0.05, precision=32)
+    sim.simulate(0.0 * ms)
+    osim, pids = mirror.from_simulator(sim, threads=os.cpu_count() or 1)
+    res = sim.cont(500.0 * ms)
+    count = float(res.spikes(h["rec"]).sum())
+    ref = osim.run(5000, cap=1 << 22)[0].size
+    assert ref > 100
+    assert abs(count - ref) / ref < 0.05, (count, ref)
+    w = sim._plan.weights(h["ee"].proj_id)
+    w_ref = osim.weights(pids[0], w.size)
+    assert abs(w.mean() - w_ref.mean()) / w_ref.mean() < 0.02

@@ -331,3 +331,28 @@ def test_headline_network_fp32_rate_within_1pct_of_fp64_oracle(oracle):
     assert 20.0 < ref / (NE + NI) / (steps * 1e-4) < 60.0   # Hz
     assert abs(counts[32] - ref) / ref < 0.01
     assert abs(counts[64] - ref) / ref < 0.01
+
+
+def test_fixed_point_ring_with_large_weight_sums(oracle):
+    """The tiled kernel rounds weights to rint(w * 2^k) with k set by the
+    largest per-neuron sum of |w|: in-degree 400 of +-2500 pA gives a sum of
+    1e6 pA, k = 10 for the int32 ring (resolution 2^-10 pA, 4e-7 relative to a
+    weight) and k = 41 for the int64 ring.  FP64: identical spikes and V_m
+    within 1e-9 relative over 100 steps; FP32: V_m within 2e-6 relative
+    (a few float32 ulps) plus 2e-3 mV over 30 steps."""
+    net = Net(NE=800, NI=200, CE=320, CI=80, J=2500.0, g=1.0, rate=9000.0, delay=15, seed=31)
+    net.drives = [(0, 9000.0, 400.0, 15, 101), (1, 9000.0, 400.0, 15, 102)]
+    rec = np.arange(0, 1000, 11)
+    pl64 = net.to_plan(precision=64, semantics=1, rec=rec)
+    pl32 = net.to_plan(precision=32, semantics=1, rec=rec)
+    assert pl64.engine == "tiled" and pl32.engine == "tiled"
+    assert pl32.ring_fraction_bits == 10 and pl64.ring_fraction_bits == 41
+    sim = net.to_oracle(oracle, semantics=1, rec=rec)
+    pl64.run(100)
+    pl32.run(30)
+    st, g = pl64.spikes()
+    ost, og, ov = sim.run(100)
+    assert len(ost) > 0
+    assert _raster(st, g) == _raster(ost, og)
+    np.testing.assert_allclose(pl64.v_trace(), ov, rtol=1e-9, atol=1e-9)
+    np.testing.assert_allclose(pl32.v_trace(), ov[:30], rtol=2e-6, atol=2e-3)
