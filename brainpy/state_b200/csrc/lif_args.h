@@ -44,7 +44,7 @@ struct LifArgs {
 // c a CSR over all pre neurons of the edges that target c's tile,
 // ptr[c * (N + 1) + pre] .. ptr[c * (N + 1) + pre + 1] into `edges` (edge
 // word = post_in_tile | lag << 16 | projection << 24); per-window spike
-// records list[kRecBufs][G][kRecWords] (tagged count word + kRecInline
+// records list[kRecBufs][rec_rep][G][kRecWords] (tagged count word + kRecInline
 // tagged entries) with an overflow area ovf[kRecBufs][G][list_cap];
 // (with separate receptor ports, bit 15 of the edge word is the port);
 // per-CTA spike-record counts rec_count[G] (running across the launches of
@@ -53,6 +53,7 @@ struct LifArgs {
 constexpr int kRecWords = 16;
 constexpr int kRecInline = kRecWords - 1;
 constexpr int kRecBufs = 4;
+constexpr int kRecRepMax = 16;
 
 // The tiled kernel accumulates arrivals in fixed point: weights are
 // rint(w * 2^k) in int32 (FP32 plans) or int64 (FP64 plans), k chosen per plan
@@ -93,6 +94,13 @@ struct TiledArgs {
     // 1: the receptor ports 'ex' and 'in_' have rings of their own (edge
     // word bit 15 = port; drives feed 'ex'); 0: one ring, sum split by sign
     int ports;
+    // copies of every record (1..kRecRepMax): CTA c polls copy c % rec_rep,
+    // so each record line is read by G / rec_rep CTAs instead of all G
+    int rec_rep;
+    // pause (ns) before the first poll of a window's records, about one
+    // write latency: a poll issued right after this CTA's own publish mostly
+    // finds the other records not yet written
+    int poll_pause;
 };
 
 struct TiledLayout {
@@ -117,10 +125,11 @@ __host__ __device__ inline TiledLayout tiled_layout(size_t coef_sz, size_t proj_
 template <typename Real>
 cudaError_t launch_lif_tiled(const LifArgs<Real> &a, const TiledArgs<Real> &t2, int grid,
                              cudaStream_t st);
-// Poisson drive of steps [m0, m0 + n) for every neuron into out[(m - m0) * N + g].
+// Poisson drive of steps [m0, m0 + n) for every neuron into out[(m - m0) * N + g];
+// `beside`: blocks of 128 threads sized to run next to the persistent kernel.
 template <typename Real>
 cudaError_t launch_drive_fill(const LifArgs<Real> &a, int64_t m0, int n, Real *out,
-                              cudaStream_t st);
+                              cudaStream_t st, bool beside = false);
 // ports: two rings ('ex', 'in_') instead of one
 size_t lif_tiled_smem(int tile, int L, int W, int N, int npop, int nproj, bool dbl, bool smem_ptr,
                       bool ports = false);

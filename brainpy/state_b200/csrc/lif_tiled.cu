@@ -42,8 +42,7 @@
 namespace bspk {
 
 namespace {
-constexpr int kThreads = 256;  // one CTA per SM: the whole register file is
-                                // the kernel's (launch bounds (256, 1))
+constexpr int kThreads = 256;  // one CTA per SM
 constexpr int kHalfWarps = kThreads / 16;     // 16 record readers of 16 words each
 constexpr int kRecPerHalf = 10;               // G <= kHalfWarps * kRecPerHalf = 160
 constexpr int kListCap = 2048;                // spikes gathered per window and CTA
@@ -242,8 +241,10 @@ __global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64
 // ring_s[(port * L + slot) * tile + t] (the kernel models' ports,
 // _kernel/models/iaf_psc_alpha.py 'ex' / 'in_'); otherwise one ring whose
 // sum is split by sign (_base.py:312-382).
+// 224 registers per thread (no spills) leave 8 K of the SM's 64 K registers
+// free, room for a 128-thread block of the drive pass running beside it.
 template <typename Real, int MODEL, bool PORTS>
-__global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a, const TiledArgs<Real> t2) {
+__global__ void __maxnreg__(224) k_lif_tiled(const LifArgs<Real> a, const TiledArgs<Real> t2) {
     using Fix = typename FixOf<Real>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int W = a.W;
@@ -337,7 +338,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
     };
     // first loads of a poll of window e's records (word w of record hw + 16 i)
     auto poll_issue = [&](int e, uint32_t (&word)[kRecPerHalf]) {
-        const uint32_t *recs = t2.list + static_cast<size_t>(e & (kRecBufs - 1)) * G * kRecWords;
+        const uint32_t *recs =
+            t2.list + (static_cast<size_t>(e & (kRecBufs - 1)) * t2.rec_rep + c % t2.rec_rep) * G * kRecWords;
 #pragma unroll
         for (int i = 0; i < kRecPerHalf; ++i) {
             const int j = hw + kHalfWarps * i;
@@ -409,7 +411,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
         const uint32_t tag = tag_of(e);
         const int64_t e0 = a.step0 + static_cast<int64_t>(e) * W;
         const int slot0 = static_cast<int>(e0 % L);
-        const uint32_t *recs = t2.list + static_cast<size_t>(buf) * G * kRecWords;
+        const uint32_t *recs =
+            t2.list + (static_cast<size_t>(buf) * t2.rec_rep + c % t2.rec_rep) * G * kRecWords;
         // a gathered spike: its entry and the bounds of its edge bucket
         auto put = [&](int pos, int src, uint32_t word_) {
             const int pre = src * tile + static_cast<int>((word_ & kPayMask) >> 5);
@@ -437,7 +440,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
         // the other records not yet written and only adds to the L2 traffic
         // of the lines being written; waiting about one write latency first
         // saves a polling round
-        if (!have) __nanosleep(700);
+        if (!have && t2.poll_pause > 0) __nanosleep(t2.poll_pause);
         const uint64_t t_start = gtimer();
         bool first = true;
         while (__any_sync(0xffffffffu, pend != 0u)) {
@@ -552,7 +555,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
         const int slot0 = static_cast<int>(n0 % L);
         const int buf = j & (kRecBufs - 1);
         const uint32_t tag = tag_of(j);
-        uint32_t *rec = t2.list + (static_cast<size_t>(buf) * G + c) * kRecWords;
+        // this CTA's record in every replica (stride G * kRecWords words)
+        uint32_t *rec = t2.list + (static_cast<size_t>(buf) * t2.rec_rep * G + c) * kRecWords;
+        const size_t rstride = static_cast<size_t>(G) * kRecWords;
         uint32_t *ovf = t2.ovf + (static_cast<size_t>(buf) * G + c) * t2.list_cap;
         const bool pre = a.pipe && j >= 1;
         if (pre) poll_issue(j - 1, word);
@@ -579,7 +584,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
                     const int pos = atomicAdd(&s_nsp[j & 1], 1);
                     const uint32_t ent = (static_cast<uint32_t>(tid) << 5) | static_cast<uint32_t>(k);
                     s_spk[pos] = ent;
-                    if (pos < kRecInline) rec[1 + pos] = tag | ent;
+                    if (pos < kRecInline)
+                        for (int q = 0; q < t2.rec_rep; ++q) rec[q * rstride + 1 + pos] = tag | ent;
                     else if (pos - kRecInline < t2.list_cap) ovf[pos - kRecInline] = tag | ent;
                 }
                 if (rslot >= 0)
@@ -591,10 +597,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_lif_tiled(const LifArgs<Real> a
         const int nsp = s_nsp[j & 1];
         // the other parity's counter was last read before this barrier
         if (tid == 0) s_nsp[(j + 1) & 1] = 0;
-        if (tid == 0) {
-            if (c != t2.hold_cta || j != t2.hold_win) rec[0] = tag | static_cast<uint32_t>(nsp);
+        {
+            // thread 16 q + w writes word w of replica q: the count word, or
+            // the window's tag into the unused entry slots
+            const int q = tid >> 4, wd = tid & 15;
+            if (q < t2.rec_rep) {
+                if (wd == 0) {
+                    if (c != t2.hold_cta || j != t2.hold_win)
+                        rec[q * rstride] = tag | static_cast<uint32_t>(nsp);
+                } else if (wd - 1 >= nsp) {
+                    rec[q * rstride + wd] = tag | kPayMask;
+                }
+            }
         }
-        else if (tid <= kRecInline && tid - 1 >= nsp) rec[tid] = tag | kPayMask;  // unused slots
 
         // ---- spike record into this CTA's region (holes for unrecorded neurons)
         for (int i = tid; i < nsp; i += B) {
@@ -661,13 +676,14 @@ cudaError_t launch_lif_tiled(const LifArgs<Real> &a, const TiledArgs<Real> &t2, 
 
 template <typename Real>
 cudaError_t launch_drive_fill(const LifArgs<Real> &a, int64_t m0, int n, Real *out,
-                              cudaStream_t st) {
+                              cudaStream_t st, bool beside) {
     if (n <= 0 || a.N <= 0) return cudaSuccess;
-    const int gx = (a.N + 255) / 256;
+    const int threads = beside ? 128 : 256;
+    const int gx = (a.N + threads - 1) / threads;
     const int gy = static_cast<int>(std::min<int64_t>(std::max<int64_t>(1, (148 * 16 + gx - 1) / gx),
                                                       std::min(n, 65535)));
     const int spb = (n + gy - 1) / gy;
-    k_drive_fill<Real><<<dim3(gx, (n + spb - 1) / spb), 256, 0, st>>>(a, m0, n, spb, out);
+    k_drive_fill<Real><<<dim3(gx, (n + spb - 1) / spb), threads, 0, st>>>(a, m0, n, spb, out);
     return cudaGetLastError();
 }
 
@@ -700,8 +716,8 @@ template cudaError_t launch_lif_tiled<float>(const LifArgs<float> &, const Tiled
 template cudaError_t launch_lif_tiled<double>(const LifArgs<double> &, const TiledArgs<double> &,
                                               int, cudaStream_t);
 template cudaError_t launch_drive_fill<float>(const LifArgs<float> &, int64_t, int, float *,
-                                              cudaStream_t);
+                                              cudaStream_t, bool);
 template cudaError_t launch_drive_fill<double>(const LifArgs<double> &, int64_t, int, double *,
-                                               cudaStream_t);
+                                               cudaStream_t, bool);
 
 }  // namespace bspk

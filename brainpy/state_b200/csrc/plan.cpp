@@ -387,6 +387,9 @@ int bspk_plan_destroy(bspk_plan *p) {
     if (p->h_stage) cudaFreeHost(p->h_stage);
     if (p->ev0) cudaEventDestroy(p->ev0);
     if (p->ev1) cudaEventDestroy(p->ev1);
+    if (p->ev_side) cudaEventDestroy(p->ev_side);
+    if (p->ev_main) cudaEventDestroy(p->ev_main);
+    if (p->side) cudaStreamDestroy(p->side);
     cudaSetDevice(dev);
     delete p;
     return BSPK_OK;
@@ -955,7 +958,7 @@ int build_tiled(bspk_plan *p) {
         if (rc) return rc;
     }
     p->list_cap = tile * p->tW;
-    rc = dalloc(p, &p->d_tlist, static_cast<size_t>(kRecBufs) * G * kRecWords);
+    rc = dalloc(p, &p->d_tlist, static_cast<size_t>(kRecBufs) * kRecRepMax * G * kRecWords);
     if (!rc) rc = dalloc(p, &p->d_tovf, static_cast<size_t>(kRecBufs) * G * p->list_cap);
     if (!rc) rc = dalloc(p, &p->d_trec, static_cast<size_t>(G));
     if (rc) return rc;
@@ -1249,15 +1252,27 @@ int run_tiled(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
     const size_t per_step = sizeof(Real) * static_cast<size_t>(p->N);
     const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(n_steps, kDriveBudget / per_step));
     if (p->tdrive_steps < chunk) {
-        if (p->d_tdrive) {
-            cudaFree(p->d_tdrive);
-            p->allocs.erase(std::remove(p->allocs.begin(), p->allocs.end(), p->d_tdrive), p->allocs.end());
-            p->d_tdrive = nullptr;
+        for (void **b : {&p->d_tdrive, &p->d_tdrive2}) {
+            if (*b) {
+                cudaFree(*b);
+                p->allocs.erase(std::remove(p->allocs.begin(), p->allocs.end(), *b), p->allocs.end());
+                *b = nullptr;
+            }
+            int rc = dalloc_bytes(p, b, per_step * chunk);
+            if (rc) return rc;
         }
-        int rc = dalloc_bytes(p, &p->d_tdrive, per_step * chunk);
-        if (rc) return rc;
         p->tdrive_steps = chunk;
+        p->pref_step0 = -1;
     }
+    if (p->drive_overlap && !p->side) {
+        BSPK_CUDA(cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking));
+        BSPK_CUDA(cudaEventCreateWithFlags(&p->ev_side, cudaEventDisableTiming));
+        BSPK_CUDA(cudaEventCreateWithFlags(&p->ev_main, cudaEventDisableTiming));
+    }
+    void *bufs[2] = {p->d_tdrive, p->d_tdrive2};
+    // a prefill issued by the previous run may still be writing a buffer if
+    // this run comes on another stream
+    if (p->side) BSPK_CUDA(cudaStreamWaitEvent(st, p->ev_side, 0));
     const int64_t run0 = p->step;
     int64_t launches = 0;
     for (int64_t done = 0; done < n_steps; done += chunk) {
@@ -1267,23 +1282,59 @@ int run_tiled(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
         a.run_step0 = run0;
         a.W = p->tW;
         a.pipe = p->tpipe;
-        BSPK_CUDA(cudaMemsetAsync(p->d_tlist, 0, sizeof(uint32_t) * kRecBufs * p->grid * kRecWords, st));
+        // this launch's drive: prefilled beside the previous launch, or now
+        int cur = 0;
+        if (p->drive_overlap && p->pref_step0 == a.step0 && p->pref_n >= n) {
+            cur = p->pref_buf;
+            BSPK_CUDA(cudaStreamWaitEvent(st, p->ev_side, 0));
+        } else {
+            cudaError_t e = launch_drive_fill<Real>(a, a.step0, static_cast<int>(n),
+                                                    static_cast<Real *>(bufs[cur]), st);
+            if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("drive launch: ") + cudaGetErrorString(e));
+            ++launches;
+        }
+        p->pref_step0 = -1;
+        BSPK_CUDA(cudaMemsetAsync(p->d_tlist, 0,
+                                  sizeof(uint32_t) * kRecBufs * p->rec_rep * p->grid * kRecWords, st));
         BSPK_CUDA(cudaMemsetAsync(p->d_tovf, 0,
                                   sizeof(uint32_t) * kRecBufs * static_cast<size_t>(p->grid) * p->list_cap, st));
-        cudaError_t e = launch_drive_fill<Real>(a, a.step0, static_cast<int>(n),
-                                                static_cast<Real *>(p->d_tdrive), st);
-        if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("drive launch: ") + cudaGetErrorString(e));
         using Fix = typename FixOf<Real>::type;
         TiledArgs<Real> t2{p->d_tptr, p->d_tedges, static_cast<const Fix *>(p->d_tw),
                            static_cast<const Fix *>(p->d_twproj), static_cast<Real>(p->tinv_scale),
                            p->d_tlist, p->d_tovf, p->d_trec, p->list_cap, p->smem_ptr ? 1 : 0,
-                           static_cast<const Real *>(p->d_tdrive), a.step0,
+                           static_cast<const Real *>(bufs[cur]), a.step0,
                            done == 0 ? p->hold_cta : -1, done == 0 ? p->hold_win : -1,
-                           p->ports_tiled};
-        e = launch_lif_tiled<Real>(a, t2, p->grid, st);
+                           p->ports_tiled, p->rec_rep, p->poll_pause};
+        // ev_main marks the end of everything before this launch (the last
+        // reader of the other buffer); the persistent kernel is submitted
+        // first so that its CTAs take their SMs before the side blocks do
+        if (p->drive_overlap) BSPK_CUDA(cudaEventRecord(p->ev_main, st));
+        cudaError_t e = launch_lif_tiled<Real>(a, t2, p->grid, st);
         if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
-        launches += 2;
+        ++launches;
+        if (p->drive_overlap) {
+            // the drive of the steps after this launch (the next launch, or as
+            // many steps after the run), into the other buffer, once every
+            // launch enqueued so far (the last reader of that buffer) is done
+            const int64_t next0 = a.step0 + n;
+            const int64_t nn = done + n < n_steps ? std::min<int64_t>(chunk, n_steps - done - n) : n;
+            if (next0 + nn < (int64_t(1) << 32)) {
+                BSPK_CUDA(cudaStreamWaitEvent(p->side, p->ev_main, 0));
+                LifArgs<Real> b = lif_args<Real>(p, nn);
+                cudaError_t e = launch_drive_fill<Real>(b, next0, static_cast<int>(nn),
+                                                        static_cast<Real *>(bufs[cur ^ 1]), p->side,
+                                                        true);
+                if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("drive launch: ") + cudaGetErrorString(e));
+                BSPK_CUDA(cudaEventRecord(p->ev_side, p->side));
+                p->pref_step0 = next0;
+                p->pref_n = nn;
+                p->pref_buf = cur ^ 1;
+                ++launches;
+            }
+        }
     }
+    // the side stream's last prefill completes within this run's stream order
+    if (p->drive_overlap && p->pref_step0 >= 0) BSPK_CUDA(cudaStreamWaitEvent(st, p->ev_side, 0));
     p->hold_cta = p->hold_win = -1;  // the test hook covers one run
     p->last_launches = launches;
     return BSPK_OK;
@@ -1570,6 +1621,29 @@ int bspk_state_set(bspk_plan *p, int pop, const char *name, const double *values
 int64_t bspk_step_count(bspk_plan *p) { return p ? p->step : -1; }
 
 int bspk_step_fused(bspk_plan *p, void *stream) { return bspk_run(p, 1, stream); }
+
+int bspk_plan_set_tiled_options(bspk_plan *p, int record_copies, int poll_pause_ns,
+                                int drive_overlap) {
+    if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    if (record_copies < 1 || record_copies > kRecRepMax)
+        return fail(BSPK_ERR_ARG, "record copies must be in 1.." + std::to_string(kRecRepMax));
+    if (poll_pause_ns < 0 || poll_pause_ns > 100000)
+        return fail(BSPK_ERR_ARG, "poll pause must be in 0..100000 ns");
+    p->rec_rep = record_copies;
+    p->poll_pause = poll_pause_ns;
+    p->drive_overlap = drive_overlap != 0;
+    p->pref_step0 = -1;
+    return BSPK_OK;
+}
+
+int bspk_plan_get_tiled_options(bspk_plan *p, int *record_copies, int *poll_pause_ns,
+                                int *drive_overlap) {
+    if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    if (record_copies) *record_copies = p->rec_rep;
+    if (poll_pause_ns) *poll_pause_ns = p->poll_pause;
+    if (drive_overlap) *drive_overlap = p->drive_overlap ? 1 : 0;
+    return BSPK_OK;
+}
 
 int bspk_record_weights(bspk_plan *p, int proj_id, int on) {
     if (!p || proj_id < 0 || proj_id >= static_cast<int>(p->projs.size()))

@@ -155,6 +155,18 @@ struct bspk_plan {
     bool cspk_valid = false;
     int64_t cspk_n = 0;
     int64_t tdrive_steps = 0;      // its capacity in steps
+    // Drive double buffer.  Beside each persistent launch, the drive pass of
+    // the steps that follow it (the next launch of the run, or the same
+    // number of steps after the run) runs on a side stream into the other
+    // buffer; a run that starts where the prefill starts uses it as is.
+    void *d_tdrive2 = nullptr;
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_side = nullptr, ev_main = nullptr;
+    int64_t pref_step0 = -1, pref_n = 0;  // prefilled steps [pref_step0, +pref_n)
+    int pref_buf = 0;                     // in buffer 0 (d_tdrive) or 1 (d_tdrive2)
+    bool drive_overlap = true;
+    int rec_rep = 1;                      // copies of every spike record (tiled kernel)
+    int poll_pause = 700;                 // ns before a window's first record poll
 };
 
 namespace bspk {

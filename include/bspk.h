@@ -253,6 +253,20 @@ int bspk_run(bspk_plan *plan, int64_t n_steps, void *stream);
 /* One step of the network (the single-step target a jax.ffi program calls
  * inside its own loop; bspk_run(plan, 1, stream)). */
 int bspk_step_fused(bspk_plan *plan, void *stream);
+/* Options of the tiled path (none changes a result):
+ *  record_copies (1..16, default 1): each CTA's per-window spike record is
+ *    written that many times and CTA c polls copy c % record_copies, so each
+ *    record line is read by G / record_copies CTAs;
+ *  poll_pause_ns (default 700): pause before a window's first record poll;
+ *  drive_overlap (default 1): the Poisson drive of the steps after each
+ *    persistent launch is computed on a side stream beside it (double
+ *    buffer; a run that continues where the previous one ended finds its
+ *    first drive ready); 0 runs every drive pass before its launch on the
+ *    caller's stream. */
+int bspk_plan_set_tiled_options(bspk_plan *plan, int record_copies, int poll_pause_ns,
+                                int drive_overlap);
+int bspk_plan_get_tiled_options(bspk_plan *plan, int *record_copies, int *poll_pause_ns,
+                                int *drive_overlap);
 
 /* Synchronise and copy out what the last bspk_run recorded.
  * spikes: (step, gid) pairs in no particular order, *n_out = count. */

@@ -3,7 +3,8 @@ realised network (kernel timing, separate ex / in_ receptor ports with
 different synaptic time constants, Poisson devices, keyed fixed_indegree).
 
 Tolerances: FP64 spike counts per interval identical and V_m within 1e-9
-(per-step engine, floating-point atomics in delivery); FP32 rate within 5 %.
+(the tiled kernel with one ring per port; the Poisson units on the kernel's
+block-key stream); FP32 rate within 5 %.
 """
 import numpy as np
 import pytest
@@ -42,8 +43,8 @@ def _oracle_twin(oracle, prog, model_name):
     for p in prog.net.populations:
         if not p.is_device:
             sim.add_pop(p.n, p.params)
-    for post, rate, w, d, seed, t_min, t_max, port in prog.drives:
-        sim.add_drive(post, rate, w, d, seed, t_min, t_max, receptor=port)
+    for post, rate, w, d, okey, unit0, t_min, t_max, port in prog.drives:
+        sim.add_drive_keyed(post, rate, w, d, okey, unit0, t_min, t_max, receptor=port)
     for a, b, indptr, idx, w, d, port in prog.realised:
         sim.add_proj(a, b, indptr, idx, w, d, port)
     for p in prog.net.populations:

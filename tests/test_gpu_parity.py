@@ -356,3 +356,42 @@ def test_fixed_point_ring_with_large_weight_sums(oracle):
     assert _raster(st, g) == _raster(ost, og)
     np.testing.assert_allclose(pl64.v_trace(), ov, rtol=1e-9, atol=1e-9)
     np.testing.assert_allclose(pl32.v_trace(), ov[:30], rtol=2e-6, atol=2e-3)
+
+
+def test_tiled_options_do_not_change_results(oracle):
+    """Record copies, the poll pause and the drive pass beside the launch
+    (with prefills consumed across runs, and a restore that discards one)
+    change scheduling only: FP32 runs give identical spikes and V_m under
+    every setting, and the FP64 run under the non-default one matches the
+    oracle."""
+    net = Net(per_edge_delay=(10, 30), delay=10, seed=17)
+    rec = np.arange(0, 250, 3)
+    out = []
+    for copies, pause, overlap in ((1, 700, False), (1, 700, True), (4, 0, True), (16, 300, True)):
+        pl = net.to_plan(precision=32, semantics=1, rec=rec)
+        pl.set_tiled_options(copies, pause, overlap)
+        ck = pl.checkpoint()
+        pl.run(70)
+        pl.restore(ck)                      # the prefilled drive no longer fits
+        runs = []
+        for n in (150, 150, 37):            # the 2nd run starts at the prefill
+            pl.run(n)
+            runs.append((pl.spikes(), pl.v_trace().copy()))
+        out.append(runs)
+    for other in out[1:]:
+        for (s0, v0), (s1, v1) in zip(out[0], other):
+            np.testing.assert_array_equal(np.sort(s0[0] * 1000 + s0[1]), np.sort(s1[0] * 1000 + s1[1]))
+            np.testing.assert_array_equal(v0, v1)
+    pl = net.to_plan(precision=64, semantics=1, rec=rec)
+    pl.set_tiled_options(4, 0, True)
+    sim = net.to_oracle(oracle, semantics=1, rec=rec)
+    sts, gs, vs = [], [], []
+    for n in (100, 100):
+        pl.run(n)
+        st, g = pl.spikes()
+        sts.append(st)
+        gs.append(g)
+        vs.append(pl.v_trace())
+    ost, og, ov = sim.run(200)
+    assert _raster(np.concatenate(sts), np.concatenate(gs)) == _raster(ost, og)
+    np.testing.assert_allclose(np.concatenate(vs), ov, rtol=0, atol=1e-9)
