@@ -47,6 +47,7 @@ constexpr int kHalfWarps = kThreads / 16;     // 16 record readers of 16 words e
 constexpr int kRecPerHalf = 10;               // G <= kHalfWarps * kRecPerHalf = 160
 constexpr int kListCap = 2048;                // spikes gathered per window and CTA
 constexpr int kEdgeUnroll = 8;                // edge loads in flight per thread
+constexpr int kUpd = 16;                      // window steps whose inputs sit in registers
 constexpr int kEdgeCap = 4096;                // flattened edges mapped per pass
 constexpr int kTagShift = 14;                 // word = tag (18 bits) << 14 | payload
 constexpr uint32_t kPayMask = (1u << kTagShift) - 1u;
@@ -563,34 +564,61 @@ __global__ void __maxnreg__(224) k_lif_tiled(const LifArgs<Real> a, const TiledA
         if (pre) poll_issue(j - 1, word);
         __pipeline_wait_prior(0);  // this thread's drive entries of window j have landed
 
-        // ---- update (rolled loop over the window)
+        // ---- update.  The window's inputs are read from shared memory into
+        // registers first (kUpd steps at a time), so the steps' dependency
+        // chain runs on registers only; spikes are collected in a bit mask
+        // and written to the record after the loop.
         if (own) {
             const Real *drv = drv_s + static_cast<size_t>(j & 1) * W * tile + tid;
+            const Real inv = t2.inv_scale;
+            uint32_t spmask = 0u;
             int slot = slot0;
-            for (int k = 0; k < Wk; ++k) {
-                const Real x = static_cast<Real>(ring_s[slot * tile + tid]) * t2.inv_scale + drv[k * tile];
-                ring_s[slot * tile + tid] = Fix(0);
-                bool sp;
-                if (PORTS) {
-                    const Real xi = static_cast<Real>(ring_s[(L + slot) * tile + tid]) * t2.inv_scale;
-                    ring_s[(L + slot) * tile + tid] = Fix(0);
-                    if (MODEL == 0) sp = iaf_alpha_step_ports<Real>(cf, st, r, x, xi);
-                    else sp = iaf_exp_step_ports<Real>(cf, st, r, x, xi);
-                } else {
-                    if (MODEL == 0) sp = iaf_alpha_step<Real>(cf, st, r, x);
-                    else sp = iaf_exp_step<Real>(cf, st, r, x);
+            for (int k0 = 0; k0 < Wk; k0 += kUpd) {
+                const int kn = min(kUpd, Wk - k0);
+                Real xe[kUpd], xi[kUpd];
+#pragma unroll
+                for (int u = 0; u < kUpd; ++u) {
+                    xe[u] = Real(0);
+                    xi[u] = Real(0);
+                    if (u < kn) {
+                        int sl = slot + u;  // slot + u < 2 L: kn <= W < L
+                        if (sl >= L) sl -= L;
+                        xe[u] = static_cast<Real>(ring_s[sl * tile + tid]) * inv + drv[(k0 + u) * tile];
+                        ring_s[sl * tile + tid] = Fix(0);
+                        if (PORTS) {
+                            xi[u] = static_cast<Real>(ring_s[(L + sl) * tile + tid]) * inv;
+                            ring_s[(L + sl) * tile + tid] = Fix(0);
+                        }
+                    }
                 }
-                if (sp) {
-                    const int pos = atomicAdd(&s_nsp[j & 1], 1);
-                    const uint32_t ent = (static_cast<uint32_t>(tid) << 5) | static_cast<uint32_t>(k);
-                    s_spk[pos] = ent;
-                    if (pos < kRecInline)
-                        for (int q = 0; q < t2.rec_rep; ++q) rec[q * rstride + 1 + pos] = tag | ent;
-                    else if (pos - kRecInline < t2.list_cap) ovf[pos - kRecInline] = tag | ent;
+#pragma unroll
+                for (int u = 0; u < kUpd; ++u) {
+                    if (u < kn) {
+                        bool sp;
+                        if (PORTS) {
+                            if (MODEL == 0) sp = iaf_alpha_step_ports<Real>(cf, st, r, xe[u], xi[u]);
+                            else sp = iaf_exp_step_ports<Real>(cf, st, r, xe[u], xi[u]);
+                        } else {
+                            if (MODEL == 0) sp = iaf_alpha_step<Real>(cf, st, r, xe[u]);
+                            else sp = iaf_exp_step<Real>(cf, st, r, xe[u]);
+                        }
+                        spmask |= static_cast<uint32_t>(sp) << (k0 + u);
+                        if (rslot >= 0)
+                            a.v_out[static_cast<size_t>(n0 + k0 + u - a.run_step0) * a.n_rec + rslot] = st[0];
+                    }
                 }
-                if (rslot >= 0)
-                    a.v_out[static_cast<size_t>(n0 + k - a.run_step0) * a.n_rec + rslot] = st[0];
-                if (++slot == L) slot = 0;
+                slot += kn;
+                if (slot >= L) slot -= L;
+            }
+            while (spmask) {
+                const int k = __ffs(static_cast<int>(spmask)) - 1;
+                spmask &= spmask - 1u;
+                const int pos = atomicAdd(&s_nsp[j & 1], 1);
+                const uint32_t ent = (static_cast<uint32_t>(tid) << 5) | static_cast<uint32_t>(k);
+                s_spk[pos] = ent;
+                if (pos < kRecInline)
+                    for (int q = 0; q < t2.rec_rep; ++q) rec[q * rstride + 1 + pos] = tag | ent;
+                else if (pos - kRecInline < t2.list_cap) ovf[pos - kRecInline] = tag | ent;
             }
         }
         __syncthreads();
