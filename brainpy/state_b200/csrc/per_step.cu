@@ -447,8 +447,6 @@ __global__ void __launch_bounds__(256) k_deliver_static(const StepArgs<Real> a) 
     }
 }
 
-// STDP 1: traces decay-then-add (event_plastic.py:390-420); lists of pres
-// whose delayed spike arrives now and of posts that fired at n - 1.
 // Weights of a plastic projection after the step that just closed
 // (*step_ptr already advanced) into its row of the run's trajectory, the
 // counterpart of the reference's per-step weight tap
@@ -462,6 +460,8 @@ __global__ void k_weight_tap(const double *w, int64_t n_edges, double *wtrace,
         dst[e] = w[e];
 }
 
+// STDP 1: traces decay-then-add (event_plastic.py:390-420); lists of pres
+// whose delayed spike arrives now and of posts that fired at n - 1.
 __global__ void k_stdp_traces(StdpDev s, const uint64_t *hist, const int64_t *step_ptr) {
     const int64_t n = *step_ptr;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
