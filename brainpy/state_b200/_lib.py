@@ -111,6 +111,8 @@ def lib():
             "bspk_checkpoint_size": (C.c_int, [vp, C.POINTER(i64)]),
             "bspk_checkpoint_save": (C.c_int, [vp, vp, i64]),
             "bspk_checkpoint_restore": (C.c_int, [vp, vp, i64]),
+            "bspk_host_alloc": (C.c_int, [i64, C.POINTER(vp)]),
+            "bspk_host_free": (C.c_int, [vp]),
             "bspk_gen_fixed_indegree": (C.c_int, [C.c_int, i64, C.c_int, C.c_int, C.c_int,
                                                   C.c_int, C.c_int, C.c_int, vp, vp]),
             "bspk_batch_create": (C.c_int, [C.POINTER(Config), C.POINTER(vp)]),
@@ -219,6 +221,31 @@ def kernel_poisson_table(rate_hz, dt_ms):
     check(lib().bspk_kernel_poisson_table(float(rate_hz), float(dt_ms), n.value, ptr(out),
                                           C.byref(n)))
     return out
+
+
+class _Pinned:
+    """Owner of a page-locked host allocation (freed with the object)."""
+
+    def __init__(self, nbytes):
+        self.ptr = C.c_void_p()
+        check(lib().bspk_host_alloc(int(nbytes), C.byref(self.ptr)))
+        self.nbytes = int(nbytes)
+
+    def __del__(self):
+        if getattr(self, "ptr", None) and self.ptr.value:
+            lib().bspk_host_free(self.ptr)
+            self.ptr = None
+
+
+def pinned_bytes(nbytes):
+    """A uint8 numpy array over page-locked host memory; the allocation is
+    freed when the array (and every view of it) is gone."""
+    if nbytes == 0:
+        return np.zeros(0, np.uint8)
+    owner = _Pinned(nbytes)
+    buf = (C.c_uint8 * int(nbytes)).from_address(owner.ptr.value)
+    buf._owner = owner  # the ctypes array keeps the allocation alive
+    return np.frombuffer(buf, dtype=np.uint8)
 
 
 def check(rc):
@@ -462,10 +489,12 @@ class Plan:
         check(self._L.bspk_rk_substeps(self._h, C.byref(n)))
         return n.value
 
-    def checkpoint(self):
+    def checkpoint(self, pinned=False):
+        """Host copy of every evolving device buffer; ``pinned`` puts it in
+        page-locked memory (a restore from it needs no staging copy)."""
         n = C.c_int64()
         check(self._L.bspk_checkpoint_size(self._h, C.byref(n)))
-        buf = np.zeros(n.value, np.uint8)
+        buf = pinned_bytes(n.value) if pinned else np.zeros(n.value, np.uint8)
         check(self._L.bspk_checkpoint_save(self._h, ptr(buf), n.value))
         return buf
 

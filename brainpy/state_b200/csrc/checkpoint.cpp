@@ -84,18 +84,39 @@ int bspk_checkpoint_restore(bspk_plan *p, const void *host_buf, int64_t bytes) {
     BSPK_CUDA(cudaSetDevice(p->cfg.device));
     BSPK_CUDA(cudaDeviceSynchronize());
     b += sizeof(hdr);
-    // through the plan's pinned staging buffer: one host copy, then
-    // host-to-device copies at link speed
+    // a pinned source is copied from directly; a pageable one through the
+    // plan's pinned staging buffer (one host copy, then host-to-device copies
+    // at link speed)
     const size_t body = static_cast<size_t>(need) - sizeof(hdr);
-    rc = plan_stage(p, body);
-    if (rc) return rc;
-    memcpy(p->h_stage, b, body);
-    const char *st = static_cast<const char *>(p->h_stage);
+    cudaPointerAttributes attr{};
+    const bool pinned = cudaPointerGetAttributes(&attr, host_buf) == cudaSuccess &&
+                        attr.type == cudaMemoryTypeHost;
+    cudaGetLastError();  // a pageable pointer may leave an error behind
+    const char *st = b;
+    if (!pinned) {
+        rc = plan_stage(p, body);
+        if (rc) return rc;
+        memcpy(p->h_stage, b, body);
+        st = static_cast<const char *>(p->h_stage);
+    }
     for (auto &s : sections(p)) {
         BSPK_CUDA(cudaMemcpy(s.ptr, st, s.bytes, cudaMemcpyHostToDevice));
         st += s.bytes;
     }
     p->step = hdr[1];
+    return BSPK_OK;
+}
+
+int bspk_host_alloc(int64_t bytes, void **ptr) {
+    if (!ptr || bytes < 0) return fail(BSPK_ERR_ARG, "bad arguments");
+    *ptr = nullptr;
+    if (bytes == 0) return BSPK_OK;
+    BSPK_CUDA(cudaHostAlloc(ptr, static_cast<size_t>(bytes), cudaHostAllocDefault));
+    return BSPK_OK;
+}
+
+int bspk_host_free(void *ptr) {
+    if (ptr) BSPK_CUDA(cudaFreeHost(ptr));
     return BSPK_OK;
 }
 

@@ -431,7 +431,12 @@ class Program:
         pl.upload()
         for p in neurons:
             pl.set_state(p.lib_pop, "V_m", self.initial_v(p))
-        self._ck0 = pl.checkpoint()
+        # the initial state in page-locked memory: simulate() restores it with
+        # one host-to-device copy per buffer
+        self._ck0 = pl.checkpoint(pinned=True)
+        # library columns of every observer, in view order
+        self.obs_cols = {o.name: np.array([self._lib_gid(x) for x in o.view.gids], np.int64)
+                         for o in net.observers}
 
     @property
     def bits(self):
@@ -591,7 +596,7 @@ class Runner:
         recs = {}
         for o in prog.net.observers:
             k, ns = o.interval, o.n_samples(n_steps)
-            cols = np.array([prog._lib_gid(x) for x in o.view.gids], np.int64)
+            cols = prog.obs_cols[o.name]
             rec = Recording()
             if "spike" in o.recordables:
                 counts = np.zeros((ns, cols.size), np.float64)

@@ -672,25 +672,28 @@ class Simulator:
         if syn is not None:
             syn.attach(pl, j)
 
+    def initial_v(self, pop_id):
+        """Initial V_m of population ``pop_id`` (mV) as ``simulate`` sets it."""
+        p = self._pops[pop_id]
+        init = p.v_init
+        if init is None and p.spec.v_init_const is not None:
+            return np.full(p.n, p.spec.v_init_const)
+        if init is None:
+            return np.full(p.n, p.params[p.spec.order.index(p.spec.v_default)])
+        if isinstance(init, _DISTS):
+            # the reference draws V_initializer from brainstate's global
+            # random state, which no Simulator seed sets; the facade draws
+            # it from fold(fold(key(0), INIT_STREAM), population ordinal)
+            k = _streams.fold_in(_streams.fold_in(_streams.root_key(0), _INIT_STREAM), p.pop_id)
+            return init.sample_in(k, p.n, mV, self._bits)
+        if callable(init):
+            return np.broadcast_to(np.asarray(init(p.n), np.float64), (p.n,))
+        return np.broadcast_to(mantissa(init, mV), (p.n,))
+
     def _init_state(self):
         pl = self._plan
         for p in self._pops:
-            init = p.v_init
-            if init is None and p.spec.v_init_const is not None:
-                v = np.full(p.n, p.spec.v_init_const)
-            elif init is None:
-                v = np.full(p.n, p.params[p.spec.order.index(p.spec.v_default)])
-            elif isinstance(init, _DISTS):
-                # the reference draws V_initializer from brainstate's global
-                # random state, which no Simulator seed sets; the facade draws
-                # it from fold(fold(key(0), INIT_STREAM), population ordinal)
-                k = _streams.fold_in(_streams.fold_in(_streams.root_key(0), _INIT_STREAM),
-                                     p.pop_id)
-                v = init.sample_in(k, p.n, mV, self._bits)
-            elif callable(init):
-                v = np.broadcast_to(np.asarray(init(p.n), np.float64), (p.n,))
-            else:
-                v = np.broadcast_to(mantissa(init, mV), (p.n,))
+            v = self.initial_v(p.pop_id)
             pl.set_state(p.pop_id, "V_m", v)
             for name in pl_state_names(self._model):
                 pl.set_state(p.pop_id, name, np.zeros(p.n))

@@ -317,6 +317,10 @@ int bspk_rk_substeps(bspk_plan *plan, int64_t *total);
 int bspk_checkpoint_size(bspk_plan *plan, int64_t *bytes);
 int bspk_checkpoint_save(bspk_plan *plan, void *host_buf, int64_t bytes);
 int bspk_checkpoint_restore(bspk_plan *plan, const void *host_buf, int64_t bytes);
+/* Page-locked host memory for checkpoints and read-backs: a restore from it
+ * is one host-to-device copy per section (no staging copy). */
+int bspk_host_alloc(int64_t bytes, void **ptr);
+int bspk_host_free(void *ptr);
 
 /* fixed_indegree connectivity drawn on the GPU (one thread per edge, the
  * same key derivation and bits as bspk_proj_add_fixed_indegree) and sorted

@@ -72,5 +72,4 @@ def test_simulator_exact_fp64_matches_oracle(oracle):
 
 
 def _init_v(sim, pop_id):
-    p = sim._pops[pop_id]
-    return p.v_init.sample(p.n, np.random.default_rng(1_000_003 + p.pop_id), mV)
+    return sim.initial_v(pop_id)
