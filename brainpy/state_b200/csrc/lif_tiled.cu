@@ -111,22 +111,6 @@ __device__ __forceinline__ void fix_add(long long *p, long long v) {
     atomicAdd(reinterpret_cast<unsigned long long *>(p), static_cast<unsigned long long>(v));
 }
 
-// The drive buffer streams through L2 once per launch (hundreds of MB for
-// long launches); it is written and read with evict-first hints so that it
-// does not push the tiles' edge arrays out of L2.
-__device__ __forceinline__ uint64_t evict_first_policy() {
-    uint64_t pol;
-    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
-template <typename Real>
-__device__ __forceinline__ void cp_async_evict_first(Real *dst, const Real *src, uint64_t pol) {
-    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], %2, %3;" ::"r"(d), "l"(src),
-                 "n"(static_cast<int>(sizeof(Real))), "l"(pol)
-                 : "memory");
-}
-
 __device__ __forceinline__ uint32_t tag_of(int64_t window) {
     return (static_cast<uint32_t>(window + 1) & 0x3FFFFu) << kTagShift;
 }
@@ -202,7 +186,7 @@ __global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64
                         }
                         add += static_cast<Real>(cnt) * wd;
                     }
-                    if (valid) __stcs(out + static_cast<int64_t>(kc + j) * a.N + g, add);
+                    if (valid) out[static_cast<int64_t>(kc + j) * a.N + g] = add;
                 }
             }
             return;
@@ -234,7 +218,7 @@ __global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64
                 }
                 add += static_cast<Real>(cnt) * wd;  // as the general path: 0 + count * weight
             }
-            __stcs(out + static_cast<int64_t>(k) * a.N + g, add);
+            out[static_cast<int64_t>(k) * a.N + g] = add;
         }
         return;
     }
@@ -250,7 +234,7 @@ __global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64
                 add += static_cast<Real>(cnt) * static_cast<Real>(d.weight);
             }
         }
-        __stcs(out + static_cast<int64_t>(k) * a.N + g, add);
+        out[static_cast<int64_t>(k) * a.N + g] = add;
     }
 }
 
@@ -342,7 +326,6 @@ __global__ void __maxnreg__(224) k_lif_tiled(const LifArgs<Real> a, const TiledA
     const int lane = tid & 31, hw = tid >> 4, w = lane & 15;
 
     // drive of window j into drv_s[j & 1] (own neuron's entries, asynchronous)
-    const uint64_t pol = evict_first_policy();
     auto drive_prefetch = [&](int j) {
         if (j < nwin && own) {
             const int64_t m0 = a.step0 + static_cast<int64_t>(j) * W;
@@ -350,7 +333,7 @@ __global__ void __maxnreg__(224) k_lif_tiled(const LifArgs<Real> a, const TiledA
             Real *dst = drv_s + static_cast<size_t>(j & 1) * W * tile + tid;
             const Real *src = t2.drive + (m0 - t2.drive_step0) * N + g;
             for (int k = 0; k < Wk; ++k)
-                cp_async_evict_first(dst + k * tile, src + static_cast<int64_t>(k) * N, pol);
+                __pipeline_memcpy_async(dst + k * tile, src + static_cast<int64_t>(k) * N, sizeof(Real));
         }
         __pipeline_commit();
     };
