@@ -1250,7 +1250,8 @@ constexpr size_t kDriveBudget = size_t(512) << 20;
 template <typename Real>
 int run_tiled(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
     const size_t per_step = sizeof(Real) * static_cast<size_t>(p->N);
-    const int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(n_steps, kDriveBudget / per_step));
+    int64_t chunk = std::max<int64_t>(1, std::min<int64_t>(n_steps, kDriveBudget / per_step));
+    if (p->drive_chunk > 0) chunk = std::min<int64_t>(chunk, p->drive_chunk);
     if (p->tdrive_steps < chunk) {
         for (void **b : {&p->d_tdrive, &p->d_tdrive2}) {
             if (*b) {
@@ -1623,8 +1624,9 @@ int64_t bspk_step_count(bspk_plan *p) { return p ? p->step : -1; }
 int bspk_step_fused(bspk_plan *p, void *stream) { return bspk_run(p, 1, stream); }
 
 int bspk_plan_set_tiled_options(bspk_plan *p, int record_copies, int poll_pause_ns,
-                                int drive_overlap) {
+                                int drive_overlap, int drive_chunk_steps) {
     if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    if (drive_chunk_steps < 0) return fail(BSPK_ERR_ARG, "drive chunk must be >= 0 steps");
     if (record_copies < 1 || record_copies > kRecRepMax)
         return fail(BSPK_ERR_ARG, "record copies must be in 1.." + std::to_string(kRecRepMax));
     if (poll_pause_ns < 0 || poll_pause_ns > 100000)
@@ -1632,13 +1634,15 @@ int bspk_plan_set_tiled_options(bspk_plan *p, int record_copies, int poll_pause_
     p->rec_rep = record_copies;
     p->poll_pause = poll_pause_ns;
     p->drive_overlap = drive_overlap != 0;
+    p->drive_chunk = drive_chunk_steps;
     p->pref_step0 = -1;
     return BSPK_OK;
 }
 
 int bspk_plan_get_tiled_options(bspk_plan *p, int *record_copies, int *poll_pause_ns,
-                                int *drive_overlap) {
+                                int *drive_overlap, int *drive_chunk_steps) {
     if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    if (drive_chunk_steps) *drive_chunk_steps = p->drive_chunk;
     if (record_copies) *record_copies = p->rec_rep;
     if (poll_pause_ns) *poll_pause_ns = p->poll_pause;
     if (drive_overlap) *drive_overlap = p->drive_overlap ? 1 : 0;

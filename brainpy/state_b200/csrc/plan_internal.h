@@ -167,6 +167,7 @@ struct bspk_plan {
     bool drive_overlap = true;
     int rec_rep = 1;                      // copies of every spike record (tiled kernel)
     int poll_pause = 700;                 // ns before a window's first record poll
+    int drive_chunk = 0;                  // steps per persistent launch (0: drive budget)
 };
 
 namespace bspk {

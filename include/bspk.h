@@ -262,11 +262,14 @@ int bspk_step_fused(bspk_plan *plan, void *stream);
  *    persistent launch is computed on a side stream beside it (double
  *    buffer; a run that continues where the previous one ended finds its
  *    first drive ready); 0 runs every drive pass before its launch on the
- *    caller's stream. */
+ *    caller's stream;
+ *  drive_chunk_steps (default 0 = up to 512 MB of drive per launch): the
+ *    steps of one persistent launch; small chunks keep the two drive buffers
+ *    resident in L2 beside the edge arrays, at one launch per chunk. */
 int bspk_plan_set_tiled_options(bspk_plan *plan, int record_copies, int poll_pause_ns,
-                                int drive_overlap);
+                                int drive_overlap, int drive_chunk_steps);
 int bspk_plan_get_tiled_options(bspk_plan *plan, int *record_copies, int *poll_pause_ns,
-                                int *drive_overlap);
+                                int *drive_overlap, int *drive_chunk_steps);
 
 /* Synchronise and copy out what the last bspk_run recorded.
  * spikes: (step, gid) pairs in no particular order, *n_out = count. */

@@ -359,17 +359,18 @@ def test_fixed_point_ring_with_large_weight_sums(oracle):
 
 
 def test_tiled_options_do_not_change_results(oracle):
-    """Record copies, the poll pause and the drive pass beside the launch
-    (with prefills consumed across runs, and a restore that discards one)
-    change scheduling only: FP32 runs give identical spikes and V_m under
+    """Record copies, the poll pause, the drive pass beside the launch (with
+    prefills consumed across runs, and a restore that discards one) and the
+    steps per launch change scheduling only: FP32 runs give identical spikes and V_m under
     every setting, and the FP64 run under the non-default one matches the
     oracle."""
     net = Net(per_edge_delay=(10, 30), delay=10, seed=17)
     rec = np.arange(0, 250, 3)
     out = []
-    for copies, pause, overlap in ((1, 700, False), (1, 700, True), (4, 0, True), (16, 300, True)):
+    for copies, pause, overlap, chunk in ((1, 700, False, 0), (1, 700, True, 0), (4, 0, True, 64),
+                                          (16, 300, True, 0), (2, 700, False, 37)):
         pl = net.to_plan(precision=32, semantics=1, rec=rec)
-        pl.set_tiled_options(copies, pause, overlap)
+        pl.set_tiled_options(copies, pause, overlap, chunk)
         ck = pl.checkpoint()
         pl.run(70)
         pl.restore(ck)                      # the prefilled drive no longer fits
@@ -383,7 +384,7 @@ def test_tiled_options_do_not_change_results(oracle):
             np.testing.assert_array_equal(np.sort(s0[0] * 1000 + s0[1]), np.sort(s1[0] * 1000 + s1[1]))
             np.testing.assert_array_equal(v0, v1)
     pl = net.to_plan(precision=64, semantics=1, rec=rec)
-    pl.set_tiled_options(4, 0, True)
+    pl.set_tiled_options(4, 0, True, 64)
     sim = net.to_oracle(oracle, semantics=1, rec=rec)
     sts, gs, vs = [], [], []
     for n in (100, 100):
