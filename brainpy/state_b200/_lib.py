@@ -149,9 +149,9 @@ def lib():
             "bspk_xla_run": (None, [vp, vp, C.c_char_p, C.c_size_t]),
             "bspk_xla_step": (None, [vp, vp, C.c_char_p, C.c_size_t]),
             "bspk_step_fused": (C.c_int, [vp, vp]),
-            "bspk_plan_set_tiled_options": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int]),
-            "bspk_plan_get_tiled_options": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int),
-                                                      C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+            "bspk_plan_set_tiled_options": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                      C.c_int]),
+            "bspk_plan_get_tiled_options": (C.c_int, [vp] + [C.POINTER(C.c_int)] * 5),
             "bspk_adjoint_sizes": (C.c_int, [vp, C.POINTER(i64), C.POINTER(i64),
                                              C.POINTER(C.c_int)]),
             "bspk_xla_batch_run": (None, [vp, vp, C.c_char_p, C.c_size_t]),
@@ -466,18 +466,18 @@ class Plan:
         return ms.value, n.value
 
     def set_tiled_options(self, record_copies=1, poll_pause_ns=700, drive_overlap=True,
-                          drive_chunk_steps=0):
+                          drive_chunk_steps=0, record_stride_bytes=64):
         """Options of the tiled path (results do not depend on them)."""
         check(self._L.bspk_plan_set_tiled_options(self._h, int(record_copies), int(poll_pause_ns),
                                                   int(bool(drive_overlap)),
-                                                  int(drive_chunk_steps)))
+                                                  int(drive_chunk_steps), int(record_stride_bytes)))
 
     def tiled_options(self):
-        a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_int()
-        check(self._L.bspk_plan_get_tiled_options(self._h, C.byref(a), C.byref(b), C.byref(c),
-                                                  C.byref(d)))
-        return dict(record_copies=a.value, poll_pause_ns=b.value, drive_overlap=bool(c.value),
-                    drive_chunk_steps=d.value)
+        v = [C.c_int() for _ in range(5)]
+        check(self._L.bspk_plan_get_tiled_options(self._h, *[C.byref(x) for x in v]))
+        return dict(record_copies=v[0].value, poll_pause_ns=v[1].value,
+                    drive_overlap=bool(v[2].value), drive_chunk_steps=v[3].value,
+                    record_stride_bytes=v[4].value)
 
     @property
     def ring_fraction_bits(self):

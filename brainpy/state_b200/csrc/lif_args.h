@@ -44,7 +44,7 @@ struct LifArgs {
 // c a CSR over all pre neurons of the edges that target c's tile,
 // ptr[c * (N + 1) + pre] .. ptr[c * (N + 1) + pre + 1] into `edges` (edge
 // word = post_in_tile | lag << 16 | projection << 24); per-window spike
-// records list[kRecBufs][rec_rep][G][kRecWords] (tagged count word + kRecInline
+// records list[kRecBufs][rec_rep][G][rec_stride] (tagged count word + kRecInline
 // tagged entries) with an overflow area ovf[kRecBufs][G][list_cap];
 // (with separate receptor ports, bit 15 of the edge word is the port);
 // per-CTA spike-record counts rec_count[G] (running across the launches of
@@ -97,6 +97,9 @@ struct TiledArgs {
     // copies of every record (1..kRecRepMax): CTA c polls copy c % rec_rep,
     // so each record line is read by G / rec_rep CTAs instead of all G
     int rec_rep;
+    // words from one CTA's record to the next (>= kRecWords): records on
+    // separate lines, or spread further over L2
+    int rec_stride;
     // pause (ns) before the first poll of a window's records, about one
     // write latency: a poll issued right after this CTA's own publish mostly
     // finds the other records not yet written

@@ -272,6 +272,7 @@ __global__ void __maxnreg__(224) k_lif_tiled(const LifArgs<Real> a, const TiledA
     const int tid = threadIdx.x, B = blockDim.x;
     const int G = gridDim.x, c = blockIdx.x;
     const int N = a.N, L = a.L, tile = a.tile;
+    const size_t RS = static_cast<size_t>(t2.rec_stride);  // words from one record to the next
     const int cta0 = c * tile;
     const int nloc = max(0, min(tile, N - cta0));
     const int *gptr = t2.ptr + static_cast<size_t>(c) * (N + 1);  // this tile's bounds in HBM
@@ -340,11 +341,11 @@ __global__ void __maxnreg__(224) k_lif_tiled(const LifArgs<Real> a, const TiledA
     // first loads of a poll of window e's records (word w of record hw + 16 i)
     auto poll_issue = [&](int e, uint32_t (&word)[kRecPerHalf]) {
         const uint32_t *recs =
-            t2.list + (static_cast<size_t>(e & (kRecBufs - 1)) * t2.rec_rep + c % t2.rec_rep) * G * kRecWords;
+            t2.list + (static_cast<size_t>(e & (kRecBufs - 1)) * t2.rec_rep + c % t2.rec_rep) * G * RS;
 #pragma unroll
         for (int i = 0; i < kRecPerHalf; ++i) {
             const int j = hw + kHalfWarps * i;
-            word[i] = j < G ? __ldcg(recs + j * kRecWords + w) : 0u;
+            word[i] = j < G ? __ldcg(recs + j * RS + w) : 0u;
         }
     };
     // scatter the S gathered spikes in s_list / s_ibeg / s_ioff into the
@@ -413,7 +414,7 @@ __global__ void __maxnreg__(224) k_lif_tiled(const LifArgs<Real> a, const TiledA
         const int64_t e0 = a.step0 + static_cast<int64_t>(e) * W;
         const int slot0 = static_cast<int>(e0 % L);
         const uint32_t *recs =
-            t2.list + (static_cast<size_t>(buf) * t2.rec_rep + c % t2.rec_rep) * G * kRecWords;
+            t2.list + (static_cast<size_t>(buf) * t2.rec_rep + c % t2.rec_rep) * G * RS;
         // a gathered spike: its entry and the bounds of its edge bucket
         auto put = [&](int pos, int src, uint32_t word_) {
             const int pre = src * tile + static_cast<int>((word_ & kPayMask) >> 5);
@@ -449,7 +450,7 @@ __global__ void __maxnreg__(224) k_lif_tiled(const LifArgs<Real> a, const TiledA
 #pragma unroll
                 for (int i = 0; i < kRecPerHalf; ++i) {
                     const int j = hw + kHalfWarps * i;
-                    word[i] = (pend >> i) & 1u ? __ldcg(recs + j * kRecWords + w) : 0u;
+                    word[i] = (pend >> i) & 1u ? __ldcg(recs + j * RS + w) : 0u;
                 }
             }
             first = false;
@@ -519,16 +520,16 @@ __global__ void __maxnreg__(224) k_lif_tiled(const LifArgs<Real> a, const TiledA
                 int part = 0;
                 if (j < G)
                     for (int k = w; k < j; k += 16)
-                        part += static_cast<int>(__ldcg(recs + k * kRecWords) & kPayMask);
+                        part += static_cast<int>(__ldcg(recs + k * RS) & kPayMask);
 #pragma unroll
                 for (int o = 8; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o, 16);
                 if (j >= G) continue;
-                const uint32_t head = __ldcg(recs + j * kRecWords);
+                const uint32_t head = __ldcg(recs + j * RS);
                 const int cnt = static_cast<int>(head & kPayMask);
                 const uint32_t *ovs = t2.ovf + (static_cast<size_t>(buf) * G + j) * t2.list_cap;
                 const int q1 = min(cnt, ce - part);
                 for (int q = max(0, cb - part) + w; q < q1; q += 16) {
-                    const uint32_t wq = q < kRecInline ? __ldcg(recs + j * kRecWords + 1 + q)
+                    const uint32_t wq = q < kRecInline ? __ldcg(recs + j * RS + 1 + q)
                                                        : __ldcg(ovs + (q - kRecInline));
                     const int pos = part + q - cb;
                     if ((wq & kTagMask) == tag) {
@@ -556,9 +557,9 @@ __global__ void __maxnreg__(224) k_lif_tiled(const LifArgs<Real> a, const TiledA
         const int slot0 = static_cast<int>(n0 % L);
         const int buf = j & (kRecBufs - 1);
         const uint32_t tag = tag_of(j);
-        // this CTA's record in every replica (stride G * kRecWords words)
-        uint32_t *rec = t2.list + (static_cast<size_t>(buf) * t2.rec_rep * G + c) * kRecWords;
-        const size_t rstride = static_cast<size_t>(G) * kRecWords;
+        // this CTA's record in every replica (stride G * RS words)
+        uint32_t *rec = t2.list + (static_cast<size_t>(buf) * t2.rec_rep * G + c) * RS;
+        const size_t rstride = static_cast<size_t>(G) * RS;
         uint32_t *ovf = t2.ovf + (static_cast<size_t>(buf) * G + c) * t2.list_cap;
         const bool pre = a.pipe && j >= 1;
         if (pre) poll_issue(j - 1, word);

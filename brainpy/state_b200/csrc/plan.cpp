@@ -958,7 +958,8 @@ int build_tiled(bspk_plan *p) {
         if (rc) return rc;
     }
     p->list_cap = tile * p->tW;
-    rc = dalloc(p, &p->d_tlist, static_cast<size_t>(kRecBufs) * kRecRepMax * G * kRecWords);
+    p->tlist_words = static_cast<size_t>(kRecBufs) * G * kRecWords;
+    rc = dalloc(p, &p->d_tlist, p->tlist_words);
     if (!rc) rc = dalloc(p, &p->d_tovf, static_cast<size_t>(kRecBufs) * G * p->list_cap);
     if (!rc) rc = dalloc(p, &p->d_trec, static_cast<size_t>(G));
     if (rc) return rc;
@@ -1270,6 +1271,16 @@ int run_tiled(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
         BSPK_CUDA(cudaEventCreateWithFlags(&p->ev_side, cudaEventDisableTiming));
         BSPK_CUDA(cudaEventCreateWithFlags(&p->ev_main, cudaEventDisableTiming));
     }
+    // the record area for the chosen copies and stride
+    const size_t rec_words = static_cast<size_t>(kRecBufs) * p->rec_rep * p->grid * p->rec_stride;
+    if (rec_words > p->tlist_words) {
+        cudaFree(p->d_tlist);
+        p->allocs.erase(std::remove(p->allocs.begin(), p->allocs.end(), p->d_tlist), p->allocs.end());
+        p->d_tlist = nullptr;
+        int rc = dalloc(p, &p->d_tlist, rec_words);
+        if (rc) return rc;
+        p->tlist_words = rec_words;
+    }
     void *bufs[2] = {p->d_tdrive, p->d_tdrive2};
     // a prefill issued by the previous run may still be writing a buffer if
     // this run comes on another stream
@@ -1295,8 +1306,7 @@ int run_tiled(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
             ++launches;
         }
         p->pref_step0 = -1;
-        BSPK_CUDA(cudaMemsetAsync(p->d_tlist, 0,
-                                  sizeof(uint32_t) * kRecBufs * p->rec_rep * p->grid * kRecWords, st));
+        BSPK_CUDA(cudaMemsetAsync(p->d_tlist, 0, sizeof(uint32_t) * rec_words, st));
         BSPK_CUDA(cudaMemsetAsync(p->d_tovf, 0,
                                   sizeof(uint32_t) * kRecBufs * static_cast<size_t>(p->grid) * p->list_cap, st));
         using Fix = typename FixOf<Real>::type;
@@ -1305,7 +1315,7 @@ int run_tiled(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
                            p->d_tlist, p->d_tovf, p->d_trec, p->list_cap, p->smem_ptr ? 1 : 0,
                            static_cast<const Real *>(bufs[cur]), a.step0,
                            done == 0 ? p->hold_cta : -1, done == 0 ? p->hold_win : -1,
-                           p->ports_tiled, p->rec_rep, p->poll_pause};
+                           p->ports_tiled, p->rec_rep, p->rec_stride, p->poll_pause};
         // ev_main marks the end of everything before this launch (the last
         // reader of the other buffer); the persistent kernel is submitted
         // first so that its CTAs take their SMs before the side blocks do
@@ -1624,8 +1634,10 @@ int64_t bspk_step_count(bspk_plan *p) { return p ? p->step : -1; }
 int bspk_step_fused(bspk_plan *p, void *stream) { return bspk_run(p, 1, stream); }
 
 int bspk_plan_set_tiled_options(bspk_plan *p, int record_copies, int poll_pause_ns,
-                                int drive_overlap, int drive_chunk_steps) {
+                                int drive_overlap, int drive_chunk_steps, int record_stride_bytes) {
     if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    if (record_stride_bytes < 64 || record_stride_bytes > 65536 || record_stride_bytes % 64)
+        return fail(BSPK_ERR_ARG, "record stride must be a multiple of 64 bytes in 64..65536");
     if (drive_chunk_steps < 0) return fail(BSPK_ERR_ARG, "drive chunk must be >= 0 steps");
     if (record_copies < 1 || record_copies > kRecRepMax)
         return fail(BSPK_ERR_ARG, "record copies must be in 1.." + std::to_string(kRecRepMax));
@@ -1635,13 +1647,16 @@ int bspk_plan_set_tiled_options(bspk_plan *p, int record_copies, int poll_pause_
     p->poll_pause = poll_pause_ns;
     p->drive_overlap = drive_overlap != 0;
     p->drive_chunk = drive_chunk_steps;
+    p->rec_stride = record_stride_bytes / 4;
     p->pref_step0 = -1;
     return BSPK_OK;
 }
 
 int bspk_plan_get_tiled_options(bspk_plan *p, int *record_copies, int *poll_pause_ns,
-                                int *drive_overlap, int *drive_chunk_steps) {
+                                int *drive_overlap, int *drive_chunk_steps,
+                                int *record_stride_bytes) {
     if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    if (record_stride_bytes) *record_stride_bytes = p->rec_stride * 4;
     if (drive_chunk_steps) *drive_chunk_steps = p->drive_chunk;
     if (record_copies) *record_copies = p->rec_rep;
     if (poll_pause_ns) *poll_pause_ns = p->poll_pause;

@@ -168,6 +168,8 @@ struct bspk_plan {
     int rec_rep = 1;                      // copies of every spike record (tiled kernel)
     int poll_pause = 700;                 // ns before a window's first record poll
     int drive_chunk = 0;                  // steps per persistent launch (0: drive budget)
+    int rec_stride = 16;                  // words per record slot (kRecWords or more)
+    size_t tlist_words = 0;               // allocated words of d_tlist
 };
 
 namespace bspk {

@@ -265,11 +265,15 @@ int bspk_step_fused(bspk_plan *plan, void *stream);
  *    caller's stream;
  *  drive_chunk_steps (default 0 = up to 512 MB of drive per launch): the
  *    steps of one persistent launch; small chunks keep the two drive buffers
- *    resident in L2 beside the edge arrays, at one launch per chunk. */
+ *    resident in L2 beside the edge arrays, at one launch per chunk;
+ *  record_stride_bytes (64..65536, multiple of 64; default 64): distance
+ *    between two CTAs' records, which spreads the polled lines over L2. */
 int bspk_plan_set_tiled_options(bspk_plan *plan, int record_copies, int poll_pause_ns,
-                                int drive_overlap, int drive_chunk_steps);
+                                int drive_overlap, int drive_chunk_steps,
+                                int record_stride_bytes);
 int bspk_plan_get_tiled_options(bspk_plan *plan, int *record_copies, int *poll_pause_ns,
-                                int *drive_overlap, int *drive_chunk_steps);
+                                int *drive_overlap, int *drive_chunk_steps,
+                                int *record_stride_bytes);
 
 /* Synchronise and copy out what the last bspk_run recorded.
  * spikes: (step, gid) pairs in no particular order, *n_out = count. */
