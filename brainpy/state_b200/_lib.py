@@ -230,10 +230,13 @@ class _Pinned:
         self.ptr = C.c_void_p()
         check(lib().bspk_host_alloc(int(nbytes), C.byref(self.ptr)))
         self.nbytes = int(nbytes)
+        # held by the object: module globals may already be gone when the
+        # last reference dies at interpreter exit
+        self._free = lib().bspk_host_free
 
     def __del__(self):
-        if getattr(self, "ptr", None) and self.ptr.value:
-            lib().bspk_host_free(self.ptr)
+        if getattr(self, "ptr", None) and self.ptr.value and getattr(self, "_free", None):
+            self._free(self.ptr)
             self.ptr = None
 
 
