@@ -468,7 +468,7 @@ class Plan:
         check(self._L.bspk_last_kernel_time(self._h, C.byref(ms), C.byref(n)))
         return ms.value, n.value
 
-    def set_tiled_options(self, record_copies=1, poll_pause_ns=700, drive_overlap=True,
+    def set_tiled_options(self, record_copies=1, poll_pause_ns=400, drive_overlap=True,
                           drive_chunk_steps=0, record_stride_bytes=64):
         """Options of the tiled path (results do not depend on them)."""
         check(self._L.bspk_plan_set_tiled_options(self._h, int(record_copies), int(poll_pause_ns),

@@ -1,7 +1,7 @@
 // lif_tiled.cu -- persistent windowed kernel for iaf networks with
 // target-partitioned delivery and record-based synchronisation (FP32/FP64).
 //
-// One cooperative launch runs a stretch of steps, one 256-thread CTA per SM.
+// One cooperative launch runs a stretch of steps, one 512-thread CTA per SM.
 // CTA c owns the neurons [c*tile, (c+1)*tile): their state lives in
 // registers for the whole launch, their arrival ring in shared memory
 // (ring_s[slot][t], L slots), and so does the CSR index of every edge that
@@ -42,9 +42,7 @@
 namespace bspk {
 
 namespace {
-constexpr int kThreads = 256;  // one CTA per SM
-constexpr int kHalfWarps = kThreads / 16;     // 16 record readers of 16 words each
-constexpr int kRecPerHalf = 10;               // G <= kHalfWarps * kRecPerHalf = 160
+constexpr int kMaxCtas = 160;                 // G <= 160 CTAs, one per SM
 constexpr int kListCap = 2048;                // spikes gathered per window and CTA
 constexpr int kEdgeUnroll = 8;                // edge loads in flight per thread
 constexpr int kUpd = 16;                      // window steps whose inputs sit in registers
@@ -242,10 +240,24 @@ __global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64
 // ring_s[(port * L + slot) * tile + t] (the kernel models' ports,
 // _kernel/models/iaf_psc_alpha.py 'ex' / 'in_'); otherwise one ring whose
 // sum is split by sign (_base.py:312-382).
-// 224 registers per thread (no spills) leave 8 K of the SM's 64 K registers
-// free, room for a 128-thread block of the drive pass running beside it.
-template <typename Real, int MODEL, bool PORTS>
-__global__ void __maxnreg__(224) k_lif_tiled(const LifArgs<Real> a, const TiledArgs<Real> t2) {
+// NT threads per CTA: the update needs only one thread per neuron of the
+// tile, but the delivery phases (record validation, bucket lookups, edge
+// loads) are chains of dependent latencies, and more warps per SM hide them:
+// NT x REGS stays at 56 K of the SM's 64 K registers, which leaves room for a
+// 128-thread block of the drive pass running beside it.
+// (measured on the 12 500-neuron network: 256 threads 11.9 ms per simulated
+// second in FP32, 384 10.4, 512 9.65, 640 10.2, 768 10.4, 1024 11.2; FP64
+// 14.2 at 256, 13.2 at 512)
+template <typename Real>
+struct TiledBlock {
+    static constexpr int threads = 512, regs = 112;
+};
+
+template <typename Real, int MODEL, bool PORTS, int NT, int REGS>
+__global__ void __maxnreg__(REGS) k_lif_tiled(const LifArgs<Real> a, const TiledArgs<Real> t2) {
+    // half-warp hw reads records hw + kHalfWarps i, i < kRecPerHalf
+    constexpr int kHalfWarps = NT / 16;
+    constexpr int kRecPerHalf = (kMaxCtas + kHalfWarps - 1) / kHalfWarps;
     using Fix = typename FixOf<Real>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int W = a.W;
@@ -692,15 +704,16 @@ cudaError_t launch_lif_tiled(const LifArgs<Real> &a, const TiledArgs<Real> &t2, 
     const size_t smem = lif_tiled_smem(a.tile, a.L, a.W, a.N, a.npop, a.nproj, sizeof(Real) == 8,
                                        t2.smem_ptr != 0, t2.ports != 0);
     void *args[] = {const_cast<LifArgs<Real> *>(&a), const_cast<TiledArgs<Real> *>(&t2)};
+    constexpr int NT = TiledBlock<Real>::threads, RG = TiledBlock<Real>::regs;
     const void *fn =
-        t2.ports ? (a.model == 0 ? reinterpret_cast<const void *>(&k_lif_tiled<Real, 0, true>)
-                                 : reinterpret_cast<const void *>(&k_lif_tiled<Real, 1, true>))
-                 : (a.model == 0 ? reinterpret_cast<const void *>(&k_lif_tiled<Real, 0, false>)
-                                 : reinterpret_cast<const void *>(&k_lif_tiled<Real, 1, false>));
+        t2.ports ? (a.model == 0 ? reinterpret_cast<const void *>(&k_lif_tiled<Real, 0, true, NT, RG>)
+                                 : reinterpret_cast<const void *>(&k_lif_tiled<Real, 1, true, NT, RG>))
+                 : (a.model == 0 ? reinterpret_cast<const void *>(&k_lif_tiled<Real, 0, false, NT, RG>)
+                                 : reinterpret_cast<const void *>(&k_lif_tiled<Real, 1, false, NT, RG>));
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return e;
-    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, smem, st);
+    return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(NT), args, smem, st);
 }
 
 template <typename Real>

@@ -166,7 +166,7 @@ struct bspk_plan {
     int pref_buf = 0;                     // in buffer 0 (d_tdrive) or 1 (d_tdrive2)
     bool drive_overlap = true;
     int rec_rep = 1;                      // copies of every spike record (tiled kernel)
-    int poll_pause = 700;                 // ns before a window's first record poll
+    int poll_pause = 400;                 // ns before a window's first record poll
     int drive_chunk = 0;                  // steps per persistent launch (0: drive budget)
     int rec_stride = 16;                  // words per record slot (kRecWords or more)
     size_t tlist_words = 0;               // allocated words of d_tlist

@@ -257,7 +257,7 @@ int bspk_step_fused(bspk_plan *plan, void *stream);
  *  record_copies (1..16, default 1): each CTA's per-window spike record is
  *    written that many times and CTA c polls copy c % record_copies, so each
  *    record line is read by G / record_copies CTAs;
- *  poll_pause_ns (default 700): pause before a window's first record poll;
+ *  poll_pause_ns (default 400): pause before a window's first record poll;
  *  drive_overlap (default 1): the Poisson drive of the steps after each
  *    persistent launch is computed on a side stream beside it (double
  *    buffer; a run that continues where the previous one ended finds its
