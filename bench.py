@@ -539,26 +539,36 @@ def bptt_numbers(args):
         wi = torch.tensor(T["w_in"], dtype=dt, device="cuda")
         inp = torch.tensor(T["inputs"], dtype=torch.uint8, device="cuda")
         tg = torch.tensor(T["targets"], dtype=dt, device="cuda")
-        for _ in range(2):
-            adj.forward(w, wi, inp, tg)
-            adj.backward()
-        torch.cuda.synchronize()
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        k = 3
-        fw = bw = 0.0
-        for _ in range(k):
-            ev[0].record()
-            adj.forward(w, wi, inp, tg)
-            ev[1].record()
-            adj.backward()
-            ev[2].record()
+        def timed():
+            for _ in range(2):
+                adj.forward(w, wi, inp, tg)
+                adj.backward()
             torch.cuda.synchronize()
-            fw += ev[0].elapsed_time(ev[1])
-            bw += ev[1].elapsed_time(ev[2])
-        fw, bw = fw / k, bw / k
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            k = 3
+            fw = bw = 0.0
+            for _ in range(k):
+                ev[0].record()
+                adj.forward(w, wi, inp, tg)
+                ev[1].record()
+                adj.backward()
+                ev[2].record()
+                torch.cuda.synchronize()
+                fw += ev[0].elapsed_time(ev[1])
+                bw += ev[1].elapsed_time(ev[2])
+            return fw / k, bw / k
+
+        fw, bw = timed()
         res[f"fp{prec}"] = {"forward_ms": round(fw, 3), "backward_ms": round(bw, 3),
                             "grads_per_s": round(1000.0 / (fw + bw), 3),
-                            "trial_steps_per_s": round(64 * 1000 * 1000.0 / (fw + bw), 1)}
+                            "trial_steps_per_s": round(64 * 1000 * 1000.0 / (fw + bw), 1),
+                            "weight_gradients": "contraction" if adj.contraction
+                            else "read-modify-write"}
+        if adj.contraction:
+            # the same backward with per-trial read-modify-writes of the gradients
+            adj.contraction = False
+            res[f"fp{prec}"]["backward_ms_read_modify_write"] = round(timed()[1], 3)
+            adj.contraction = True
         adj.close()
     # finite differences on 64 random weights (32 recurrent, 32 input) at the
     # configured 1000 steps, FP64, relaxed forward with t_ref = 0 (smooth in

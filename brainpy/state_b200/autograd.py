@@ -47,6 +47,16 @@ class LifAdjoint:
         """1, or 2 when each trial runs on a two-CTA cluster."""
         return int(self._L.bspk_adjoint_ctas_per_trial(self._h))
 
+    @property
+    def contraction(self):
+        """True when the weight gradients are dense contractions over (step,
+        trial) (FP32 default); False: per-trial read-modify-writes."""
+        return bool(self._L.bspk_adjoint_contraction(self._h))
+
+    @contraction.setter
+    def contraction(self, on):
+        _lib.check(self._L.bspk_adjoint_set_contraction(self._h, int(bool(on))))
+
     def close(self):
         if getattr(self, "_h", None):
             self._L.bspk_adjoint_destroy(self._h)

@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <cmath>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../../include/bspk.h"
@@ -71,6 +72,13 @@ struct AdjArgs {
     unsigned long long *nspk;
     int64_t din_stride;      // din_max * N
     int split;               // CTAs per trial: 1, or 2 as a thread-block cluster
+    // contraction mode (gemm = 1): the backward stores the input adjoint
+    // gD[t][b][i] and the recompute the previous step's spikes
+    // gS[t][b][p] = s_{t-1}[b][p] (row 0 stays zero); the weight gradients
+    // are then two dense contractions over (t, b) instead of per-trial
+    // read-modify-writes
+    Real *gD, *gS;
+    int gemm;
 };
 
 // A trial's CTA (1 or 2 per trial).  With split = 2 the two CTAs of a
@@ -221,6 +229,7 @@ __device__ void forward_step(const AdjArgs<Real> &a, const Smem<Real> &s, int t,
             ++nsp;
         }
         s.sc[i] = sv;
+        if (trace && a.gemm && t + 1 < a.T) a.gS[(static_cast<size_t>(t + 1) * a.B + b) * N + i] = sv;
         if (trace) {
             const size_t o = (static_cast<size_t>(b) * a.K + row) * N + i;
             a.tr_x[o] = x;
@@ -401,7 +410,9 @@ __global__ void __launch_bounds__(1024) k_adj_backward(const AdjArgs<Real> a) {
                 s.lIi[i] = s.lIi[i] * a.eP11in + (nr ? lVt * a.eP21in : Real(0));
                 s.lV[i] = nr ? lVt * a.eP22 : lVt;
                 s.lxc[i] = lx;
-                if (t > 0) {
+                if (a.gemm) {
+                    a.gD[(static_cast<size_t>(t) * a.B + b) * N + i] = lx;
+                } else if (t > 0) {
                     const int d = a.deg_in[i];
                     for (int k0 = 0; k0 < d; k0 += kAdjUnroll) {
                         int col[kAdjUnroll];
@@ -428,7 +439,7 @@ __global__ void __launch_bounds__(1024) k_adj_backward(const AdjArgs<Real> a) {
                                 dwb[static_cast<size_t>(k0 + u) * N + i] = old[u] + lx * spre[u];
                     }
                 }
-                for (int q0 = 0; q0 < nact; q0 += kAdjUnroll) {
+                for (int q0 = 0; q0 < (a.gemm ? 0 : nact); q0 += kAdjUnroll) {
                     Real old[kAdjUnroll];
 #pragma unroll
                     for (int u = 0; u < kAdjUnroll; ++u)
@@ -471,6 +482,107 @@ __global__ void k_adj_reduce_in(const Real *part, int N, int NI, int B, Real *ou
         Real acc = Real(0);
         for (int b = 0; b < B; ++b) acc = acc + part[(static_cast<size_t>(b) * NI + k) * N + i];
         out[e] = acc;
+    }
+}
+
+// Weight-gradient contraction (FP32 plans): C = A^T B over the rows r = (t, b)
+// shared by two row-major operands, A [K][M] (the input adjoints gD) and
+// B [K][Nc] (the shifted spikes gS, or the input counts as uint8), C [M][Nc].
+// A 256-thread CTA computes a 128 x 128 tile of C, each thread an 8 x 8
+// block (two 4-row by two 4-column quarters, so its shared-memory reads are
+// conflict-free 16-byte loads), over the rows [z kc, (z + 1) kc), double
+// buffering 8-row slices of both operands; it writes its partial sum to
+// part[z][M][Nc].  The partials are added in z order afterwards, so the
+// result does not depend on scheduling.
+constexpr int kGBM = 128, kGBN = 128, kGBK = 8;
+template <typename TB>
+__global__ void __launch_bounds__(256) k_gemm_tn(const float *A, const TB *Bm, int M, int Nc, int64_t K,
+                                                 int64_t kc, float *part) {
+    __shared__ __align__(16) float As[2][kGBK][kGBM];
+    __shared__ __align__(16) float Bs[2][kGBK][kGBN];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int m0 = blockIdx.y * kGBM, n0 = blockIdx.x * kGBN;
+    const int64_t k0 = static_cast<int64_t>(blockIdx.z) * kc;
+    const int64_t k1 = k0 + kc < K ? k0 + kc : K;
+    // loader: k-row lr of the slice, columns lc .. lc + 3 of both tiles
+    const int lr = tid >> 5, lc = (tid & 31) * 4;
+    float ra[4], rb[4];
+    auto load = [&](int64_t kk) {
+        const int64_t r = kk + lr;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int m = m0 + lc + u, n = n0 + lc + u;
+            ra[u] = (r < k1 && m < M) ? A[r * M + m] : 0.f;
+            rb[u] = (r < k1 && n < Nc) ? static_cast<float>(Bm[r * Nc + n]) : 0.f;
+        }
+    };
+    auto store = [&](int buf) {
+        *reinterpret_cast<float4 *>(&As[buf][lr][lc]) = make_float4(ra[0], ra[1], ra[2], ra[3]);
+        *reinterpret_cast<float4 *>(&Bs[buf][lr][lc]) = make_float4(rb[0], rb[1], rb[2], rb[3]);
+    };
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+    if (k0 < k1) {
+        load(k0);
+        store(0);
+    }
+    __syncthreads();
+    int buf = 0;
+    for (int64_t kk = k0; kk < k1; kk += kGBK) {
+        const bool more = kk + kGBK < k1;
+        if (more) load(kk + kGBK);  // in flight during this slice's products
+#pragma unroll
+        for (int k = 0; k < kGBK; ++k) {
+            const float4 a0 = *reinterpret_cast<const float4 *>(&As[buf][k][ty * 4]);
+            const float4 a1 = *reinterpret_cast<const float4 *>(&As[buf][k][64 + ty * 4]);
+            const float4 b0 = *reinterpret_cast<const float4 *>(&Bs[buf][k][tx * 4]);
+            const float4 b1 = *reinterpret_cast<const float4 *>(&Bs[buf][k][64 + tx * 4]);
+            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        }
+        if (more) store(buf ^ 1);
+        __syncthreads();
+        buf ^= 1;
+    }
+    float *P = part + static_cast<size_t>(blockIdx.z) * M * Nc;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int m = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
+        if (m >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int n = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + j - 4);
+            if (n < Nc) P[static_cast<size_t>(m) * Nc + n] = acc[i][j];
+        }
+    }
+}
+
+// out[e] = sum over z in order of part[z][post(e)][pre(e)], the caller's CSR edges
+__global__ void k_gemm_gather(const float *part, int S, int Nc, size_t MN, const int32_t *e_post,
+                              const int32_t *e_pre, int64_t nnz, float *out) {
+    for (int64_t e = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < nnz;
+         e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const size_t q = static_cast<size_t>(e_post[e]) * Nc + e_pre[e];
+        float acc = 0.f;
+        for (int z = 0; z < S; ++z) acc = acc + part[z * MN + q];
+        out[e] = acc;
+    }
+}
+
+// out[q] = sum over z in order of part[z][q]
+__global__ void k_gemm_sum(const float *part, int S, size_t n, float *out) {
+    for (size_t q = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; q < n;
+         q += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        float acc = 0.f;
+        for (int z = 0; z < S; ++z) acc = acc + part[z * n + q];
+        out[q] = acc;
     }
 }
 
@@ -527,6 +639,11 @@ struct bspk_adjoint {
     const void *targets = nullptr;  // operands of the last forward (borrowed)
     const uint8_t *inputs = nullptr;
     bool have_forward = false;
+    // FP32 weight-gradient contraction: buffers allocated (can), selected (gemm)
+    int can_gemm = 0, gemm = 0, sms = 0;
+    void *gD = nullptr, *gS = nullptr;   // [n_steps][batch][n]
+    float *gpart = nullptr;              // split-K partial sums
+    int32_t *e_post = nullptr, *e_pre = nullptr;  // the CSR edges' (post, pre)
 };
 
 extern "C" int bspk_adjoint_sizes(const bspk_adjoint *adj, int64_t *nnz, int64_t *n_w_in,
@@ -593,6 +710,9 @@ AdjArgs<Real> make_args(const bspk_adjoint *h) {
     a.nspk = h->nspk;
     a.din_stride = static_cast<int64_t>(h->din_max) * c.n;
     a.split = h->split;
+    a.gD = static_cast<Real *>(h->gD);
+    a.gS = static_cast<Real *>(h->gS);
+    a.gemm = h->gemm;
     return a;
 }
 
@@ -647,10 +767,53 @@ int run_forward(bspk_adjoint *h, const void *w, const void *w_in, double *loss, 
     return BSPK_OK;
 }
 
+// Row splits of a contraction with an M x Nc result: enough CTAs for two per
+// SM, at most 64 partials, and at least 64 rows per split.
+int gemm_splits(int sms, int M, int Nc, int64_t K) {
+    const int64_t tiles = static_cast<int64_t>((M + kGBM - 1) / kGBM) * ((Nc + kGBN - 1) / kGBN);
+    int64_t S = (2 * static_cast<int64_t>(std::max(sms, 1)) + tiles - 1) / tiles;
+    S = std::min<int64_t>(S, std::max<int64_t>(1, K / 64));
+    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(S, 64)));
+}
+
+// dL/dw and dL/dw_in of an FP32 handle by contraction over (step, trial)
+int run_contractions(bspk_adjoint *h, float *dw, float *dw_in, cudaStream_t st) {
+    const bspk_adjoint_config &c = h->cfg;
+    const int N = c.n, NI = c.n_in;
+    const int64_t K = static_cast<int64_t>(c.n_steps) * c.batch;
+    const float *D = static_cast<const float *>(h->gD);
+    if (h->nnz > 0) {
+        const int S = gemm_splits(h->sms, N, N, K);
+        const int64_t kc = (K + S - 1) / S;
+        k_gemm_tn<float><<<dim3((N + kGBN - 1) / kGBN, (N + kGBM - 1) / kGBM, S), 256, 0, st>>>(
+            D, static_cast<const float *>(h->gS), N, N, K, kc, h->gpart);
+        k_gemm_gather<<<grid_of(h->nnz), 256, 0, st>>>(h->gpart, S, N, static_cast<size_t>(N) * N,
+                                                       h->e_post, h->e_pre, h->nnz, dw);
+    }
+    if (NI > 0 && dw_in) {
+        const int S = gemm_splits(h->sms, N, NI, K);
+        const int64_t kc = (K + S - 1) / S;
+        k_gemm_tn<uint8_t><<<dim3((NI + kGBN - 1) / kGBN, (N + kGBM - 1) / kGBM, S), 256, 0, st>>>(
+            D, h->inputs, N, NI, K, kc, h->gpart);
+        const size_t n = static_cast<size_t>(N) * NI;
+        k_gemm_sum<<<grid_of(static_cast<int64_t>(n)), 256, 0, st>>>(h->gpart, S, n, dw_in);
+    }
+    BSPK_CUDA(cudaGetLastError());
+    return BSPK_OK;
+}
+
 template <typename Real>
 int run_backward(bspk_adjoint *h, void *dw, void *dw_in, cudaStream_t st) {
     const AdjArgs<Real> a = make_args<Real>(h);
     const bspk_adjoint_config &c = h->cfg;
+    if (a.gemm) {
+        // step 0's row of the shifted spikes stays zero
+        BSPK_CUDA(cudaMemsetAsync(h->gS, 0, sizeof(Real) * static_cast<size_t>(c.batch) * c.n, st));
+        BSPK_CUDA(launch_trials<Real>(k_adj_backward<Real>, a, h, st));
+        if constexpr (std::is_same<Real, float>::value)
+            return run_contractions(h, static_cast<float *>(dw), static_cast<float *>(dw_in), st);
+        return fail(BSPK_ERR_UNSUPPORTED, "contraction mode is FP32 only");
+    }
     const size_t nw = static_cast<size_t>(c.batch) * a.din_stride;
     const size_t nwi = static_cast<size_t>(c.batch) * c.n * c.n_in;
     BSPK_CUDA(cudaMemsetAsync(h->dwb, 0, sizeof(Real) * std::max<size_t>(nw, 1), st));
@@ -673,6 +836,16 @@ int run_backward(bspk_adjoint *h, void *dw, void *dw_in, cudaStream_t st) {
 extern "C" {
 
 int bspk_adjoint_ctas_per_trial(const bspk_adjoint *h) { return h ? h->split : 0; }
+
+int bspk_adjoint_set_contraction(bspk_adjoint *h, int on) {
+    if (!h) return fail(BSPK_ERR_ARG, "null handle");
+    if (on && !h->can_gemm)
+        return fail(BSPK_ERR_UNSUPPORTED, "weight-gradient contraction needs an FP32 handle with its buffers");
+    h->gemm = on ? 1 : 0;
+    return BSPK_OK;
+}
+
+int bspk_adjoint_contraction(const bspk_adjoint *h) { return h ? h->gemm : 0; }
 
 int bspk_adjoint_create(const bspk_adjoint_config *cfg, const int64_t *row_ptr, const int32_t *col,
                         int64_t nnz, bspk_adjoint **out) {
@@ -714,6 +887,7 @@ int bspk_adjoint_create(const bspk_adjoint_config *cfg, const int64_t *row_ptr, 
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device) != cudaSuccess)
             sms = 0;
         h->split = (2 * c.batch <= sms && c.n >= 64 && c.n_readout <= c.n / 2) ? 2 : 1;
+        h->sms = sms;
     }
     const int per_cta = (c.n + h->split - 1) / h->split;
     h->threads = std::min(1024, std::max(32, (per_cta + 31) / 32 * 32));
@@ -791,6 +965,41 @@ int bspk_adjoint_create(const bspk_adjoint_config *cfg, const int64_t *row_ptr, 
         cudaMemcpy(h->oe_eid, oe_eid.data(), 8 * n_oe, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(h->in_pos, in_pos.data(), 8 * in_pos.size(), cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(fail(BSPK_ERR_CUDA, "upload of the structure failed"));
+    // FP32: the buffers of the weight-gradient contraction, when they fit in
+    // 16 GB (otherwise the read-modify-write mode only)
+    if (c.precision == 32) {
+        const int64_t Kr = static_cast<int64_t>(c.n_steps) * c.batch;
+        const size_t S1 = gemm_splits(h->sms, N, N, Kr), S2 = gemm_splits(h->sms, N, c.n_in, Kr);
+        const size_t part = std::max(S1 * NN * NN, S2 * NN * static_cast<size_t>(c.n_in));
+        const size_t op = 4 * static_cast<size_t>(Kr) * NN;
+        const size_t ne = static_cast<size_t>(std::max<int64_t>(nnz, 1));
+        if (2 * op + 4 * part + 8 * ne <= (size_t(16) << 30)) {
+            void *p[5] = {};
+            const size_t by[5] = {op, op, 4 * std::max<size_t>(part, 1), 4 * ne, 4 * ne};
+            bool ok = true;
+            for (int k = 0; k < 5 && ok; ++k) {
+                ok = cudaMalloc(&p[k], by[k]) == cudaSuccess;
+                if (ok) h->allocs.push_back(p[k]);
+            }
+            if (ok) {
+                std::vector<int32_t> ep(ne, 0);
+                for (int i = 0; i < N; ++i)
+                    for (int64_t e = row_ptr[i]; e < row_ptr[i + 1]; ++e) ep[e] = i;
+                ok = cudaMemcpy(p[3], ep.data(), 4 * ne, cudaMemcpyHostToDevice) == cudaSuccess &&
+                     (nnz == 0 || cudaMemcpy(p[4], col, 4 * static_cast<size_t>(nnz),
+                                             cudaMemcpyHostToDevice) == cudaSuccess);
+                if (!ok) return bail(fail(BSPK_ERR_CUDA, "upload of the edge list failed"));
+                h->gD = p[0];
+                h->gS = p[1];
+                h->gpart = static_cast<float *>(p[2]);
+                h->e_post = static_cast<int32_t *>(p[3]);
+                h->e_pre = static_cast<int32_t *>(p[4]);
+                h->can_gemm = h->gemm = 1;
+            } else {
+                cudaGetLastError();  // an allocation that failed leaves the mode off
+            }
+        }
+    }
     rc = h->elt == 8 ? set_smem<double>(h) : set_smem<float>(h);
     if (rc) return bail(rc);
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(BSPK_ERR_CUDA, "upload failed"));

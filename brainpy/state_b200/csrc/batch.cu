@@ -33,7 +33,7 @@ namespace bspk {
 namespace {
 constexpr int kBMaxT = 512;
 constexpr int kBListCap = 1024;   // gathered spikes per delivery chunk
-constexpr int kBEdgeUnroll = 16;  // edge loads in flight per thread
+constexpr int kBEdgeUnroll = 8;   // edge loads in flight per thread
 constexpr uint64_t kBPollNs = 2000000000ull;
 constexpr uint32_t kCompleteBit = 0x80000000u;
 
@@ -91,8 +91,17 @@ __device__ int block_scan_excl(int *s, int n, int *s_warp) {
 }
 }  // namespace
 
+// FP32: 80 registers per thread let three 256-neuron tiles (CTAs) share an
+// SM, whose independent tile-window chains overlap (514 against 548 ms per
+// simulated second for the 256-instance sweep with 128 registers, where
+// one 512-neuron tile per SM was the best shape); FP64 keeps 128 (80 spills).
+template <typename Real>
+constexpr int batch_regs() {
+    return sizeof(Real) == 4 ? 80 : 128;
+}
+
 template <typename Real, int MODEL>
-__global__ void __launch_bounds__(kBMaxT) k_lif_batch(const BatchArgs<Real> a) {
+__global__ void __maxnreg__(batch_regs<Real>()) k_lif_batch(const BatchArgs<Real> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using Fix = typename FixOf<Real>::type;
     Fix *acc = reinterpret_cast<Fix *>(smem_raw);  // [Wmax][T], fixed point

@@ -432,6 +432,17 @@ int bspk_adjoint_backward(bspk_adjoint *adj, void *dw, void *dw_in, void *stream
 /* Element counts of the gradient operands (nnz recurrent weights, n * n_in
  * input weights) and the precision (32 / 64) of a handle. */
 int bspk_adjoint_sizes(const bspk_adjoint *adj, int64_t *nnz, int64_t *n_w_in, int *precision);
+/* How an FP32 handle forms the weight gradients.  1 (the default when the
+ * buffers fit): the backward stores the input adjoint of every (step, trial,
+ * neuron) and the recompute the previous step's spikes, and dL/dw, dL/dw_in
+ * are dense contractions over (step, trial) followed by a gather of the
+ * edges (partial sums added in a fixed order: deterministic).  0: per-trial
+ * read-modify-writes in time order, summed over trials in trial order (the
+ * only mode of FP64 handles, bit-exact with the float64 restatement).
+ * Setting 1 on an FP64 handle, or on one whose buffers could not be
+ * allocated, is BSPK_ERR_UNSUPPORTED. */
+int bspk_adjoint_set_contraction(bspk_adjoint *adj, int on);
+int bspk_adjoint_contraction(const bspk_adjoint *adj);
 
 /* No-allocation entry point (no counterpart in the reference).  For callers
  * that cannot call cudaMalloc -- code running inside another framework's

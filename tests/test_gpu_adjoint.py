@@ -5,6 +5,8 @@
     kernels are compiled without FMA contraction and follow its order);
   * checkpoint spacing does not change the result (bitwise);
   * FP32: gradients within 1e-3 relative of the FP64 ones on a short episode;
+    the FP32 contraction mode (dense products over (step, trial), the
+    default) against the FP32 read-modify-write mode within 1e-4 relative;
   * central finite differences (h = 1e-3) on 64 random weights of the
     gradient-training network (800 + 200 neurons, batch 64) over 200 steps in
     the relaxed forward with refractoriness off (the loss is then smooth in
@@ -30,12 +32,16 @@ def _small(relaxed=False, detach=False, t_ref=2.0, seed=3, n_steps=120):
                      detach_reset=detach, params=params, w_in_scale=900.0, seed=seed)
 
 
-def _gpu(T, precision=64, ckpt=50, split=None):
+def _gpu(T, precision=64, ckpt=50, split=None, contraction=None):
     from brainpy.state_b200.autograd import LifAdjoint
     dt = torch.float64 if precision == 64 else torch.float32
     adj = LifAdjoint(T["cfg"], T["row_ptr"], T["col"], precision=precision, ckpt_every=ckpt)
     if split is not None:
         assert adj.ctas_per_trial == split
+    # FP32 handles contract by default, FP64 handles never do
+    assert adj.contraction == (precision == 32)
+    if contraction is not None:
+        adj.contraction = contraction
     w = torch.tensor(T["w"], dtype=dt, device="cuda")
     wi = torch.tensor(T["w_in"], dtype=dt, device="cuda")
     inp = torch.tensor(T["inputs"], dtype=torch.uint8, device="cuda")
@@ -98,6 +104,28 @@ def test_fp32_gradient_tracks_fp64():
     assert abs(L32 - L64) <= 1e-4 * abs(L64)
     for a, b in ((dw32, dw64), (dwi32, dwi64)):
         np.testing.assert_allclose(a, b, rtol=1e-3, atol=1e-3 * np.abs(b).max())
+
+
+@pytest.mark.parametrize("relaxed", [False, True])
+def test_fp32_contraction_matches_read_modify_write(relaxed):
+    # the two FP32 ways of forming dL/dw, dL/dw_in differ only in the order
+    # of the FP32 additions
+    T = _small(relaxed=relaxed, n_steps=150)
+    L1, dw1, dwi1, n1 = _gpu(T, precision=32, contraction=True)
+    L0, dw0, dwi0, n0 = _gpu(T, precision=32, contraction=False)
+    assert (L1, n1) == (L0, n0)
+    assert np.abs(dw0).max() > 0 and np.abs(dwi0).max() > 0
+    for a, b in ((dw1, dw0), (dwi1, dwi0)):
+        np.testing.assert_allclose(a, b, rtol=1e-4, atol=1e-5 * np.abs(b).max())
+
+
+def test_fp64_handle_refuses_contraction():
+    from brainpy.state_b200.autograd import LifAdjoint
+    T = _small(n_steps=20)
+    adj = LifAdjoint(T["cfg"], T["row_ptr"], T["col"], precision=64)
+    with pytest.raises(NotImplementedError):
+        adj.contraction = True
+    adj.close()
 
 
 def test_finite_differences_full_workload():
