@@ -31,7 +31,6 @@
 namespace bspk {
 
 namespace {
-constexpr int kBMaxT = 512;
 constexpr int kBListCap = 1024;   // gathered spikes per delivery chunk
 constexpr int kBEdgeUnroll = 8;   // edge loads in flight per thread
 constexpr uint64_t kBPollNs = 2000000000ull;
