@@ -103,6 +103,7 @@ def lib():
             "bspk_state_set": (C.c_int, [vp, C.c_int, C.c_char_p, vp]),
             "bspk_step_count": (i64, [vp]),
             "bspk_plan_engine": (C.c_char_p, [vp]),
+            "bspk_plan_set_windowed": (C.c_int, [vp, C.c_int]),
             "bspk_record_weights": (C.c_int, [vp, C.c_int, C.c_int]),
             "bspk_weight_trace_get": (C.c_int, [vp, C.c_int, C.POINTER(i64), vp]),
             "bspk_plan_ring_fraction_bits": (C.c_int, [vp, C.POINTER(C.c_int)]),
@@ -461,9 +462,14 @@ class Plan:
 
     @property
     def engine(self):
-        """Kernel family of the uploaded plan: 'tiled', 'global_ring', 'exact'
-        or 'per_step'."""
+        """Kernel family of the uploaded plan: 'tiled', 'global_ring', 'exact',
+        'per_step' or 'windowed'."""
         return self._L.bspk_plan_engine(self._h).decode()
+
+    def set_windowed(self, on):
+        """Run a plan that can run windowed in the windowed (True) or the
+        per-step (False) form."""
+        check(self._L.bspk_plan_set_windowed(self._h, int(bool(on))))
 
     def kernel_time(self):
         ms, n = C.c_double(), C.c_int64()

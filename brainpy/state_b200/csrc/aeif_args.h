@@ -70,6 +70,24 @@ struct StdpDev {
     int64_t n_edges, run_step0;
 };
 
+// Windowed engine: the neuron kernel advances W steps per launch (all lags
+// >= W, so no spike of a window arrives inside it) and the plastic
+// projection's weights are brought up to date per edge at each arrival.
+struct WinDev {
+    int on;                // a plastic pair-rule projection is handled (s)
+    StdpDev s;
+    int W, cap;            // window; arrivals held per (step, post)
+    double *kp;            // [W][n_pre] pre trace at step n0 + k without that step's arrival
+    long long *upto;       // [edges] last step whose facilitation reached the edge
+    uint2 *arr;            // [W][cap][n_post] (CSR edge, pre) arriving at n0 + k
+    int *cnt;              // [W][n_post] arrivals per (step, post), cleared by their reader
+    uint32_t *spk;         // spikes of the window: gid << 5 | step in window
+    uint32_t *pre_list;    // pres with arrivals in the window, then their step masks
+    uint32_t *post_list;   // plastic posts that fired in the window, then their masks
+    int *ctr;              // [0] window spikes, [1] arriving pres, [2] posts that fired
+    int *err;
+};
+
 int run_per_step(bspk_plan *p, int64_t n_steps, cudaStream_t st);
 
 }  // namespace bspk

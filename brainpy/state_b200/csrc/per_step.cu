@@ -311,20 +311,23 @@ __device__ __forceinline__ bool iaf_ms_step(const PopCoef<Real> &c, Real *s, int
 
 // ------------------------------------------------------------- kernels
 
-template <typename Real, int MODEL>
-__global__ void __launch_bounds__(128) k_neuron_step(const StepArgs<Real> a, double dt) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= a.N) return;
-    const int64_t n = *a.step_ptr;
-    const int p = find_pop_t(a.coef, a.npop, g);
-    const PopCoef<Real> c = a.coef[p];
+// The pieces of one neuron-step, shared by the per-step and the windowed
+// engines.  Inputs of step n: the ring slot (read and cleared) plus the
+// Poisson drives of the neuron's population.
+template <typename Real>
+__device__ __forceinline__ void step_inputs(const StepArgs<Real> &a, int g, int p,
+                                            const PopCoef<Real> &c, int64_t n, Real (&in)[kMaxReceptors]) {
     const int slot = static_cast<int>(n % a.L);
-    Real in[kMaxReceptors] = {Real(0), Real(0), Real(0), Real(0)};
+    for (int ch = 0; ch < kMaxReceptors; ++ch) in[ch] = Real(0);
     for (int ch = 0; ch < a.R; ++ch) {
         Real *cell = a.ring + (static_cast<size_t>(slot) * a.R + ch) * a.N + g;
         in[ch] = *cell;
         *cell = Real(0);
     }
+}
+template <typename Real>
+__device__ __forceinline__ void step_drives(const StepArgs<Real> &a, int g, int p,
+                                            const PopCoef<Real> &c, int64_t n, Real (&in)[kMaxReceptors]) {
     for (int q = a.pop_drive_ptr[p]; q < a.pop_drive_ptr[p + 1]; ++q) {
         const DriveDev d = a.drives[a.pop_drive_list[q]];
         const int64_t se = n - d.lag;
@@ -335,11 +338,11 @@ __global__ void __launch_bounds__(128) k_neuron_step(const StepArgs<Real> a, dou
             in[d.receptor < a.R ? d.receptor : 0] += static_cast<Real>(cnt) * static_cast<Real>(d.weight);
         }
     }
-    constexpr int kSlots = model_n_slots(MODEL);
-    Real st[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) st[i] = i < kSlots ? a.s[i][g] : Real(0);
-    int r = a.r[g];
+}
+// the model's update of one step; returns the spike flag
+template <typename Real, int MODEL>
+__device__ __forceinline__ bool step_update(const StepArgs<Real> &a, const PopCoef<Real> &c, Real (&st)[8],
+                                            int &r, Real (&in)[kMaxReceptors], double dt) {
     bool sp;
     if constexpr (MODEL == 0) {
         Real s6[6];
@@ -362,6 +365,43 @@ __global__ void __launch_bounds__(128) k_neuron_step(const StepArgs<Real> a, dou
     } else {
         sp = cond_step<Real, MODEL>(c, st, r, in[0], in[1], dt, a.err, a.rk_iters);
     }
+    return sp;
+}
+// a spike of neuron g at step n into the recorder (when g is recorded)
+template <typename Real>
+__device__ __forceinline__ void step_record_spike(const StepArgs<Real> &a, int g, int64_t n) {
+    if (a.spk_flag == nullptr || a.spk_flag[g]) {
+        const unsigned long long at = atomicAdd(a.spk_count, 1ull);
+        if (at < static_cast<unsigned long long>(a.spk_cap)) {
+            a.spk_step[at] = n;
+            a.spk_gid[at] = g;
+        }
+    }
+}
+template <typename Real>
+__device__ __forceinline__ void step_record_v(const StepArgs<Real> &a, int g, int64_t n, Real v) {
+    if (a.rec_slot) {
+        const int rs = a.rec_slot[g];
+        if (rs >= 0) a.v_out[static_cast<size_t>(n - a.run_step0) * a.n_rec + rs] = v;
+    }
+}
+
+template <typename Real, int MODEL>
+__global__ void __launch_bounds__(128) k_neuron_step(const StepArgs<Real> a, double dt) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= a.N) return;
+    const int64_t n = *a.step_ptr;
+    const int p = find_pop_t(a.coef, a.npop, g);
+    const PopCoef<Real> c = a.coef[p];
+    Real in[kMaxReceptors];
+    step_inputs<Real>(a, g, p, c, n, in);
+    step_drives<Real>(a, g, p, c, n, in);
+    constexpr int kSlots = model_n_slots(MODEL);
+    Real st[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) st[i] = i < kSlots ? a.s[i][g] : Real(0);
+    int r = a.r[g];
+    const bool sp = step_update<Real, MODEL>(a, c, st, r, in, dt);
 #pragma unroll
     for (int i = 0; i < 8; ++i)
         if (i < kSlots) a.s[i][g] = st[i];
@@ -371,18 +411,9 @@ __global__ void __launch_bounds__(128) k_neuron_step(const StepArgs<Real> a, dou
     if (sp) {
         const int pos = atomicAdd(a.step_nspk, 1);
         a.step_spk[pos] = static_cast<uint32_t>(g);
-        if (a.spk_flag == nullptr || a.spk_flag[g]) {
-            const unsigned long long at = atomicAdd(a.spk_count, 1ull);
-            if (at < static_cast<unsigned long long>(a.spk_cap)) {
-                a.spk_step[at] = n;
-                a.spk_gid[at] = g;
-            }
-        }
+        step_record_spike<Real>(a, g, n);
     }
-    if (a.rec_slot) {
-        const int rs = a.rec_slot[g];
-        if (rs >= 0) a.v_out[static_cast<size_t>(n - a.run_step0) * a.n_rec + rs] = st[0];
-    }
+    step_record_v<Real>(a, g, n, st[0]);
 }
 
 // Static delivery of this step's spikes.  A work item is one chunk of
@@ -603,6 +634,264 @@ __global__ void __launch_bounds__(256) k_stdp_depress(StdpDev s, const StepArgs<
     }
 }
 
+// ------------------------------------------------------ windowed engine
+// A window covers the steps [n0, n0 + Wk), Wk <= W <= every lag, so a spike
+// of the window arrives after it and the steps' inputs are known at its
+// start, except the plastic weights, whose facilitation by the post's own
+// spikes of the window must precede each arrival on the edge.  Per window:
+//   pretrace: per pre of the plastic projection, the pre trace of every
+//     step of the window without that step's arrival (kp, the K+ that a
+//     facilitation at that step reads), and the pres whose spikes arrive;
+//   arrivals: the out-edges of those pres into per-(step, post) lists;
+//   neuron: each thread advances its neuron through the window; at step n
+//     a plastic post updates its post trace, then for each edge arriving at
+//     n applies the facilitations its own spikes of the window still owe
+//     the edge (steps after the edge's last update, up to n) and the
+//     depression, and adds the new weight to the step's input; the step's
+//     static input comes from the ring as in the per-step engine;
+//   deliver: the window's spikes into the ring slots n + lag;
+//   facilitate: the facilitations owed by each post that fired in the
+//     window on all its in-edges (those after each edge's last update).
+// Every weight goes through the same operations in the same order as in
+// the per-step engine (_nest_plasticity/stdp_synapse.py:163-169 per step).
+
+__global__ void k_win_pretrace(WinDev w, const uint64_t *hist, int64_t n0, int Wk) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= w.s.n_pre) return;
+    double tr = w.s.pre_trace[i];
+    uint32_t am = 0u;
+    for (int k = 0; k < Wk; ++k) {
+        const bool x = fired(hist, w.s.pre_off + i, n0 + k - w.s.lag);
+        const double xv = x ? 1.0 : 0.0;
+        const double t = tr * w.s.dec_pre + xv;
+        w.kp[static_cast<size_t>(k) * w.s.n_pre + i] = t - xv;
+        tr = t;
+        am |= static_cast<uint32_t>(x) << k;
+    }
+    w.s.pre_trace[i] = tr;
+    if (am) {
+        const int q = atomicAdd(&w.ctr[1], 1);
+        w.pre_list[q] = static_cast<uint32_t>(i);
+        w.pre_list[w.s.n_pre + q] = am;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_win_arrivals(WinDev w) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int C = w.s.out_chunks, np = w.s.n_post;
+    const int64_t nitems = static_cast<int64_t>(w.ctr[1]) * C;
+    for (int64_t it = warp; it < nitems; it += nwarps) {
+        const int q = static_cast<int>(it / C);
+        const uint32_t i = w.pre_list[q], am = w.pre_list[w.s.n_pre + q];
+        const int64_t beg = w.s.indptr[i] + (it % C) * kChunkEdges, end = w.s.indptr[i + 1];
+        if (beg >= end) continue;
+        int post[kEdgeU];
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            const int64_t e = beg + u * 32 + lane;
+            post[u] = e < end ? static_cast<int>(w.s.edges[e] & kEdgePostMask) : -1;
+        }
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            if (post[u] < 0) continue;
+            const int64_t e = beg + u * 32 + lane;
+            for (uint32_t m = am; m; m &= m - 1u) {
+                const int k = __ffs(static_cast<int>(m)) - 1;
+                const int pos = atomicAdd(&w.cnt[static_cast<size_t>(k) * np + post[u]], 1);
+                if (pos < w.cap)
+                    w.arr[(static_cast<size_t>(k) * w.cap + pos) * np + post[u]] =
+                        make_uint2(static_cast<uint32_t>(e), i);
+                else
+                    atomicExch(w.err, BSPK_DEV_ERR_OVERFLOW);
+            }
+        }
+    }
+}
+
+template <typename Real, int MODEL>
+__global__ void __launch_bounds__(128) k_win_neuron(const StepArgs<Real> a, WinDev w, int64_t n0, int Wk,
+                                                    double dt) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= a.N) return;
+    const int p = find_pop_t(a.coef, a.npop, g);
+    const PopCoef<Real> c = a.coef[p];
+    constexpr int kSlots = model_n_slots(MODEL);
+    Real st[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) st[i] = i < kSlots ? a.s[i][g] : Real(0);
+    int r = a.r[g];
+    const int np = w.s.n_post;
+    const int j = g - w.s.post_off;
+    const bool pp = w.on && j >= 0 && j < np;  // a post of the plastic projection
+    double post_tr = pp ? w.s.post_trace[j] : 0.0;
+    const int rec = w.s.receptor < a.R ? w.s.receptor : 0;
+    uint64_t hw = a.hist[g];
+    uint32_t spmask = 0u;
+    for (int k = 0; k < Wk; ++k) {
+        const int64_t n = n0 + k;
+        Real in[kMaxReceptors];
+        step_inputs<Real>(a, g, p, c, n, in);
+        if (pp) {
+            // post trace of step n (decay, then the spike of n - 1) and the
+            // K- of a depression at n (without that spike)
+            const bool yb = k == 0 ? (n >= 1 && ((hw >> ((n - 1) & 63)) & 1ull) != 0)
+                                   : ((spmask >> (k - 1)) & 1u) != 0;
+            const double y = yb ? 1.0 : 0.0;
+            const double t = post_tr * w.s.dec_post + y;
+            const double kminus = t - y;
+            post_tr = t;
+            const size_t ci = static_cast<size_t>(k) * np + j;
+            int na = w.cnt[ci];
+            w.cnt[ci] = 0;  // cleared for the next window
+            if (na > w.cap) na = w.cap;
+            for (int q = 0; q < na; ++q) {
+                const uint2 en = w.arr[(static_cast<size_t>(k) * w.cap + q) * np + j];
+                const int64_t e = en.x;
+                const int pre = static_cast<int>(en.y);
+                double wv = w.s.w[e];
+                // facilitations at steps f in (fdone, n] for the spikes at
+                // f - 1 of this window: bits [fdone - n0, k) of the mask
+                const long long u = w.upto[e];
+                const int lo = u > n0 ? static_cast<int>(u - n0) : 0;
+                uint32_t due = spmask & ((1u << k) - 1u) & ~((1u << lo) - 1u);
+                for (; due; due &= due - 1u) {
+                    const int kk = __ffs(static_cast<int>(due)) - 1;
+                    wv = stdp_facilitate(w.s, wv, w.kp[static_cast<size_t>(kk + 1) * w.s.n_pre + pre]);
+                }
+                wv = stdp_depress(w.s, wv, kminus);
+                w.s.w[e] = wv;
+                w.upto[e] = n;
+                in[rec] += static_cast<Real>(wv);
+            }
+        }
+        step_drives<Real>(a, g, p, c, n, in);
+        const bool sp = step_update<Real, MODEL>(a, c, st, r, in, dt);
+        spmask |= static_cast<uint32_t>(sp) << k;
+        const int bit = static_cast<int>(n & 63);
+        hw = (hw & ~(1ull << bit)) | (static_cast<uint64_t>(sp) << bit);
+        if (sp) {
+            const int pos = atomicAdd(&w.ctr[0], 1);
+            w.spk[pos] = (static_cast<uint32_t>(g) << 5) | static_cast<uint32_t>(k);
+            step_record_spike<Real>(a, g, n);
+        }
+        step_record_v<Real>(a, g, n, st[0]);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        if (i < kSlots) a.s[i][g] = st[i];
+    a.r[g] = r;
+    a.hist[g] = hw;
+    if (pp) {
+        w.s.post_trace[j] = post_tr;
+        if (spmask) {
+            const int q = atomicAdd(&w.ctr[2], 1);
+            w.post_list[q] = static_cast<uint32_t>(j);
+            w.post_list[np + q] = spmask;
+        }
+    }
+}
+
+// Static delivery of the window's spikes (as k_deliver_static, a spike of
+// step n0 + k into the slots n0 + k + lag).
+template <typename Real>
+__global__ void __launch_bounds__(256) k_win_deliver(const StepArgs<Real> a, WinDev w, int64_t n0) {
+    const int nspk = w.ctr[0];
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int C = a.static_chunks;
+    const int64_t per_spike = static_cast<int64_t>(a.nproj) * C;
+    for (int64_t item = warp; item < nspk * per_spike; item += nwarps) {
+        const int i = static_cast<int>(item / per_spike);
+        const int rem = static_cast<int>(item % per_spike);
+        const int q = rem / C, chunk = rem % C;
+        if (a.proj_plastic[q]) continue;
+        const ProjDev<Real> &P = a.projs[q];
+        const uint32_t ent = w.spk[i];
+        const int g = static_cast<int>(ent >> 5);
+        const int pre_off = a.coef[P.pre_pop].off;
+        if (g < pre_off || g >= pre_off + a.coef[P.pre_pop].n) continue;
+        const int slot_n = static_cast<int>((n0 + static_cast<int64_t>(ent & 31u)) % a.L);
+        const int gl = g - pre_off;
+        const int64_t beg = P.indptr[gl] + static_cast<int64_t>(chunk) * kChunkEdges;
+        const int64_t end = P.indptr[gl + 1];
+        if (beg >= end) continue;
+        uint32_t ed[kEdgeU];
+        Real wv[kEdgeU];
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            const int64_t e = beg + u * 32 + lane;
+            ed[u] = e < end ? __ldg(P.edges + e) : 0xFFFFFFFFu;
+            wv[u] = (e < end && !P.homogeneous) ? __ldg(P.w + e) : P.w0;
+        }
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            if (ed[u] == 0xFFFFFFFFu) continue;
+            const int slot = (slot_n + static_cast<int>(ed[u] >> kEdgeDelayShift)) % a.L;
+            atomicAdd(a.ring + (static_cast<size_t>(slot) * a.R + P.receptor) * a.N + P.post_off +
+                          (ed[u] & kEdgePostMask),
+                      wv[u]);
+        }
+    }
+}
+
+// The facilitations owed by the posts that fired in the window on all their
+// in-edges: for a spike at n0 + kk, the facilitation at step n0 + kk + 1,
+// unless the edge's last update (an arrival) already covered it.  The last
+// step's K+ (step n0 + Wk, the next window's first) is formed here from the
+// carried pre trace and that step's arrival, as the next pretrace will.
+__global__ void __launch_bounds__(256) k_win_facilitate(WinDev w, const uint64_t *hist, int64_t n0, int Wk) {
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int C = w.s.in_chunks, np = w.s.n_post;
+    const int64_t nitems = static_cast<int64_t>(w.ctr[2]) * C;
+    for (int64_t it = warp; it < nitems; it += nwarps) {
+        const int q = static_cast<int>(it / C);
+        const int j = static_cast<int>(w.post_list[q]);
+        const uint32_t mask = w.post_list[np + q];
+        const int64_t beg = w.s.cindptr[j] + (it % C) * kChunkEdges, end = w.s.cindptr[j + 1];
+        if (beg >= end) continue;
+        int pre[kEdgeU];
+        int64_t eid[kEdgeU];
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            const int64_t cpos = beg + u * 32 + lane;
+            pre[u] = cpos < end ? static_cast<int>(w.s.cedges[cpos] & kEdgePostMask) : -1;
+            eid[u] = cpos < end ? w.s.cperm[cpos] : 0;
+        }
+        double wv[kEdgeU];
+        long long up[kEdgeU];
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            if (pre[u] < 0) continue;
+            wv[u] = w.s.w[eid[u]];
+            up[u] = w.upto[eid[u]];
+        }
+#pragma unroll
+        for (int u = 0; u < kEdgeU; ++u) {
+            if (pre[u] < 0) continue;
+            const int lo = up[u] > n0 ? static_cast<int>(up[u] - n0) : 0;
+            uint32_t due = mask & ~((1u << lo) - 1u);
+            double x = wv[u];
+            for (; due; due &= due - 1u) {
+                const int kk = __ffs(static_cast<int>(due)) - 1;
+                double kplus;
+                if (kk + 1 < Wk) {
+                    kplus = w.kp[static_cast<size_t>(kk + 1) * w.s.n_pre + pre[u]];
+                } else {
+                    const double xv = fired(hist, w.s.pre_off + pre[u], n0 + Wk - w.s.lag) ? 1.0 : 0.0;
+                    kplus = (w.s.pre_trace[pre[u]] * w.s.dec_pre + xv) - xv;
+                }
+                x = stdp_facilitate(w.s, x, kplus);
+            }
+            w.s.w[eid[u]] = x;
+        }
+    }
+}
+
 // work items per row for rows of at most max_deg edges (at least one)
 int chunks_of(int64_t max_deg) {
     const int64_t c = (max_deg + kChunkEdges - 1) / kChunkEdges;
@@ -781,9 +1070,74 @@ int run_typed(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
     return BSPK_OK;
 }
 
+WinDev win_desc(bspk_plan *p, const std::vector<StdpDev> &sd) {
+    WinDev w{};
+    w.on = sd.empty() ? 0 : 1;
+    if (w.on) w.s = sd[0];
+    w.W = p->W;
+    w.cap = p->win_cap;
+    w.kp = p->d_win_kp;
+    w.upto = p->d_win_upto;
+    w.arr = p->d_win_arr;
+    w.cnt = p->d_win_cnt;
+    w.spk = p->d_win_spk;
+    w.pre_list = p->d_win_pre;
+    w.post_list = p->d_win_post;
+    w.ctr = p->d_win_ctr;
+    w.err = p->d_err;
+    return w;
+}
+
+// The run in windows of W steps (the last one shorter), five launches each
+// with a plastic projection, three without.
+template <typename Real>
+int run_windowed(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
+    const StepArgs<Real> a = step_args<Real>(p, p->d_step_ptr);
+    const std::vector<StdpDev> sd = stdp_descs(p);
+    const WinDev w = win_desc(p, sd);
+    const double dt = p->cfg.dt;
+    const int nb = (a.N + 127) / 128, eg = p->sm_count * 4;
+    int64_t launches = 0;
+    for (int64_t done = 0; done < n_steps;) {
+        const int Wk = static_cast<int>(std::min<int64_t>(p->W, n_steps - done));
+        const int64_t n0 = p->step + done;
+        BSPK_CUDA(cudaMemsetAsync(w.ctr, 0, 4 * sizeof(int), st));
+        if (w.on) {
+            k_win_pretrace<<<(w.s.n_pre + 255) / 256, 256, 0, st>>>(w, a.hist, n0, Wk);
+            k_win_arrivals<<<eg, 256, 0, st>>>(w);
+            launches += 2;
+        }
+        switch (a.model) {
+            case 0: k_win_neuron<Real, 0><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
+            case 1: k_win_neuron<Real, 1><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
+            case 2: k_win_neuron<Real, 2><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
+            case 3: k_win_neuron<Real, 3><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
+            case 4: k_win_neuron<Real, 4><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
+            default: k_win_neuron<Real, 5><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
+        }
+        k_win_deliver<Real><<<eg, 256, 0, st>>>(a, w, n0);
+        launches += 2;
+        if (w.on) {
+            k_win_facilitate<<<eg, 256, 0, st>>>(w, a.hist, n0, Wk);
+            ++launches;
+        }
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return fail(BSPK_ERR_CUDA, std::string("window launch: ") + cudaGetErrorString(e));
+        done += Wk;
+    }
+    p->last_launches = launches;
+    return BSPK_OK;
+}
+
 }  // namespace
 
 int run_per_step(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
+    // weight recording taps every step: the per-step form
+    bool taps = false;
+    for (const auto &J : p->projs) taps = taps || (J.plastic && J.rec_w);
+    if (p->win && !taps)
+        return p->cfg.precision == 64 ? run_windowed<double>(p, n_steps, st)
+                                      : run_windowed<float>(p, n_steps, st);
     return p->cfg.precision == 64 ? run_typed<double>(p, n_steps, st)
                                   : run_typed<float>(p, n_steps, st);
 }

@@ -969,6 +969,30 @@ int build_tiled(bspk_plan *p) {
 
 }  // namespace
 
+// Buffers of the windowed engine (see WinDev).
+static int alloc_window(bspk_plan *p) {
+    const Proj *J = nullptr;
+    for (const auto &q : p->projs)
+        if (q.plastic) J = &q;
+    const size_t W = p->W;
+    const size_t npre = J ? p->pops[J->pre].n : 1, npost = J ? p->pops[J->post].n : 1;
+    const size_t E = J ? std::max<size_t>(J->post_local.size(), 1) : 1;
+    const size_t cap = J ? p->win_cap : 1;
+    int rc = dalloc(p, &p->d_win_kp, W * npre);
+    if (!rc) rc = dalloc(p, &p->d_win_upto, E);
+    if (!rc) rc = dalloc(p, &p->d_win_arr, W * cap * npost);
+    if (!rc) rc = dalloc(p, &p->d_win_cnt, W * npost);
+    if (!rc) rc = dalloc(p, &p->d_win_spk, W * static_cast<size_t>(p->N));
+    if (!rc) rc = dalloc(p, &p->d_win_pre, 2 * npre);
+    if (!rc) rc = dalloc(p, &p->d_win_post, 2 * npost);
+    if (!rc) rc = dalloc(p, &p->d_win_ctr, 4);
+    if (rc) return rc;
+    // no edge has been brought up to date by an arrival yet (step -1)
+    BSPK_CUDA(cudaMemset(p->d_win_upto, 0xFF, sizeof(long long) * E));
+    BSPK_CUDA(cudaMemset(p->d_win_cnt, 0, sizeof(int) * W * npost));
+    return BSPK_OK;
+}
+
 extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
     (void)stream;
     if (!p) return fail(BSPK_ERR_ARG, "null plan");
@@ -1018,7 +1042,31 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
             p->ports_tiled = 0;
     }
     const bool aeif = plan_per_step(p);  // per-step engine (RKF45, multisynapse, ports)
-    if (aeif || plastic) p->W = 1;
+    p->win = false;
+    if (aeif || plastic) {
+        // windowed form when every lag allows W >= 2 steps per launch, the
+        // window and the lags fit in the 64-step spike history, and at most
+        // one pair-rule projection with one lag is plastic; its arrival
+        // lists (W x max in-degree x posts) must stay within 16 GB
+        int n_pl = 0;
+        bool pl_ok = true;
+        size_t arr_bytes = 0;
+        const int Ww = std::min({min_lag, 32, 64 - max_lag});
+        for (auto &J : p->projs) {
+            if (!J.plastic) continue;
+            ++n_pl;
+            pl_ok = pl_ok && J.rule == 0 && J.post_local.size() < (size_t(1) << 32);
+            for (int32_t d : J.delay) pl_ok = pl_ok && d == J.delay[0];
+            std::vector<int64_t> indeg(p->pops[J.post].n, 0);
+            for (int32_t q : J.post_local) indeg[q]++;
+            const int64_t mx = indeg.empty() ? 0 : *std::max_element(indeg.begin(), indeg.end());
+            arr_bytes = static_cast<size_t>(std::max(Ww, 1)) * std::max<int64_t>(mx, 1) *
+                        p->pops[J.post].n * sizeof(uint2);
+            p->win_cap = static_cast<int>(std::max<int64_t>(mx, 1));
+        }
+        p->win = p->win_ok = Ww >= 2 && n_pl <= 1 && pl_ok && arr_bytes <= (size_t(16) << 30);
+        p->W = p->win ? Ww : 1;
+    }
     p->L = p->W + max_lag + 1;
 
     // state
@@ -1065,6 +1113,7 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
 
     rc = dbl ? upload_coef<double>(p) : upload_coef<float>(p);
     if (!rc) rc = dbl ? upload_projs<double>(p) : upload_projs<float>(p);
+    if (!rc && p->win) rc = alloc_window(p);
     if (rc) return rc;
 
     // drives and CDF tables
@@ -1164,7 +1213,8 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
         p->block = 256;
         p->grid = std::max(1, std::min(p->sm_count, (p->N + 31) / 32));
         p->tile = (p->N + p->grid - 1) / p->grid;
-        if (static_cast<size_t>(p->tile) * p->W * 4 > 160 * 1024)
+        // (the per-step engine, windowed or not, keeps no tile in shared memory)
+        if (!(aeif || plastic) && static_cast<size_t>(p->tile) * p->W * 4 > 160 * 1024)
             return fail(BSPK_ERR_UNSUPPORTED, "network too large for the persistent kernel tile");
     }
     for (auto &J : p->projs)
@@ -1695,11 +1745,18 @@ int bspk_plan_ring_fraction_bits(bspk_plan *p, int *bits) {
     return BSPK_OK;
 }
 
+int bspk_plan_set_windowed(bspk_plan *p, int on) {
+    if (!p || !p->uploaded) return fail(BSPK_ERR_STATE, "plan not uploaded");
+    if (on && !p->win_ok) return fail(BSPK_ERR_UNSUPPORTED, "this plan cannot run windowed");
+    p->win = on != 0;
+    return BSPK_OK;
+}
+
 const char *bspk_plan_engine(bspk_plan *p) {
     if (!p || !p->uploaded) return "";
     bool per_step = plan_per_step(p);
     for (auto &J : p->projs) per_step |= J.plastic;
-    if (per_step) return "per_step";
+    if (per_step) return p->win ? "windowed" : "per_step";
     if (p->cfg.deterministic) return "exact";
     if (p->tiled) return "tiled";
     return "global_ring";

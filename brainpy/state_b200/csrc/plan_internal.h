@@ -119,6 +119,20 @@ struct bspk_plan {
     int *d_step_counters = nullptr;   // [0] spikes of the step, then 2 per plastic projection
     int n_step_counters = 0;
     int64_t *d_step_ptr = nullptr;    // device step counter of the per-step engine
+    // windowed form of the per-step engine (WinDev): the neuron kernel
+    // advances W steps per launch when every lag is >= W >= 2 and at most one
+    // projection is plastic (pair rule, one lag); weight recording runs the
+    // per-step form
+    bool win = false, win_ok = false;  // selected, possible
+    double *d_win_kp = nullptr;
+    long long *d_win_upto = nullptr;
+    uint2 *d_win_arr = nullptr;
+    int *d_win_cnt = nullptr;
+    int win_cap = 0;
+    uint32_t *d_win_spk = nullptr;
+    uint32_t *d_win_pre = nullptr;
+    uint32_t *d_win_post = nullptr;
+    int *d_win_ctr = nullptr;
     // timing
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;

@@ -301,8 +301,18 @@ int64_t bspk_step_count(bspk_plan *plan);
  * persistent kernel, ring in shared memory), "global_ring" (persistent
  * kernel with the ring in global memory, for tiles too large for shared
  * memory), "exact" (deterministic FP64 pull), "per_step" (conductance
- * models, separate ports or plasticity); "" before upload. */
+ * models, separate ports or plasticity, one launch sequence per time step),
+ * "windowed" (the same networks when every lag is >= 2 steps and at most
+ * one pair-rule projection with one lag is plastic: each launch sequence
+ * advances a window of W = min(lag, 32, 64 - max lag) steps, the neuron
+ * kernel running its W steps back to back); "" before upload. */
 const char *bspk_plan_engine(bspk_plan *plan);
+/* Switch an uploaded plan that can run windowed between the windowed (1)
+ * and the per-step (0) form; results agree up to the order of floating-point
+ * additions into the conductance inputs.  Runs with weight recording
+ * (bspk_record_weights) always take the per-step form.  Setting 1 on a plan
+ * that cannot run windowed is BSPK_ERR_UNSUPPORTED. */
+int bspk_plan_set_windowed(bspk_plan *plan, int on);
 /* The tiled kernel sums arrivals in fixed point: weights are rounded once to
  * rint(w * 2^k) (int32 for FP32 plans, int64 for FP64 plans) with k chosen so
  * that no ring slot can overflow; *bits = k of an uploaded tiled plan. */

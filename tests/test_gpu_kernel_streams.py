@@ -72,7 +72,7 @@ def test_per_step_engine_keyed_drive_matches_oracle(oracle):
     net.connect(A, A, fixed_indegree(20), port="ex", weight=15.0 * pA, delay=1.5 * ms, name="AA")
     obs = net.observe(A[::10], "V_m", name="v")
     prog = net.compile("float64")
-    assert prog.plan.engine == "per_step"
+    assert prog.plan.engine == "windowed"  # lags of 10 and 15 steps
     sim = oracle.OracleSim(0.1, "iaf_psc_alpha", semantics=oracle.RING)
     sim.set_ports(True)
     a = sim.add_pop(300, net.populations[0].params)
