@@ -220,7 +220,7 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peak,
                      "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic,
                      "traffic_source": traffic_source, "peak_kind": peak_kind,
-                     "kernel": "bspk::k_lif_tiled<float, 0, true>", "engine": engine},
+                     "kernel": "bspk::k_lif_tiled<float, 0, true, 512, 112>", "engine": engine},
         "clocks": clk.summary(),
     }
     pl.close()
