@@ -651,7 +651,9 @@ __global__ void __launch_bounds__(256) k_stdp_depress(StdpDev s, const StepArgs<
 //     static input comes from the ring as in the per-step engine;
 //   deliver: the window's spikes into the ring slots n + lag;
 //   facilitate: the facilitations owed by each post that fired in the
-//     window on all its in-edges (those after each edge's last update).
+//     window on all its in-edges (those after each edge's last update); a
+//     spike of the window's last step is facilitated in the next window, at
+//     its first step, as the per-step form does.
 // Every weight goes through the same operations in the same order as in
 // the per-step engine (_nest_plasticity/stdp_synapse.py:163-169 per step).
 
@@ -728,6 +730,8 @@ __global__ void __launch_bounds__(128) k_win_neuron(const StepArgs<Real> a, WinD
     double post_tr = pp ? w.s.post_trace[j] : 0.0;
     const int rec = w.s.receptor < a.R ? w.s.receptor : 0;
     uint64_t hw = a.hist[g];
+    // the spike of step n0 - 1, whose facilitation falls on step n0
+    const uint64_t prevbit = (n0 >= 1 && ((hw >> ((n0 - 1) & 63)) & 1ull) != 0) ? 1ull : 0ull;
     uint32_t spmask = 0u;
     for (int k = 0; k < Wk; ++k) {
         const int64_t n = n0 + k;
@@ -751,14 +755,18 @@ __global__ void __launch_bounds__(128) k_win_neuron(const StepArgs<Real> a, WinD
                 const int64_t e = en.x;
                 const int pre = static_cast<int>(en.y);
                 double wv = w.s.w[e];
-                // facilitations at steps f in (fdone, n] for the spikes at
-                // f - 1 of this window: bits [fdone - n0, k) of the mask
+                // facilitations at steps f in (fdone, n] for the post's
+                // spikes at f - 1 >= n0 - 1 (bit b of emask: a spike at
+                // n0 - 1 + b, facilitated at n0 + b with K+ kp[b]); fdone is
+                // the edge's last update, or n0 - 1 (the window before
+                // brought every edge to n0 - 1)
+                const uint64_t emask = (static_cast<uint64_t>(spmask) << 1) | prevbit;
                 const long long u = w.upto[e];
-                const int lo = u > n0 ? static_cast<int>(u - n0) : 0;
-                uint32_t due = spmask & ((1u << k) - 1u) & ~((1u << lo) - 1u);
-                for (; due; due &= due - 1u) {
-                    const int kk = __ffs(static_cast<int>(due)) - 1;
-                    wv = stdp_facilitate(w.s, wv, w.kp[static_cast<size_t>(kk + 1) * w.s.n_pre + pre]);
+                const int lo = u >= n0 - 1 ? static_cast<int>(u - n0 + 1) : 0;
+                uint64_t due = emask & ((2ull << k) - 1ull) & ~((1ull << lo) - 1ull);
+                for (; due; due &= due - 1ull) {
+                    const int b = __ffsll(static_cast<long long>(due)) - 1;
+                    wv = stdp_facilitate(w.s, wv, w.kp[static_cast<size_t>(b) * w.s.n_pre + pre]);
                 }
                 wv = stdp_depress(w.s, wv, kminus);
                 w.s.w[e] = wv;
@@ -785,10 +793,14 @@ __global__ void __launch_bounds__(128) k_win_neuron(const StepArgs<Real> a, WinD
     a.hist[g] = hw;
     if (pp) {
         w.s.post_trace[j] = post_tr;
-        if (spmask) {
+        // spikes at n0 - 1 .. n0 + Wk - 2: their facilitations fall in this
+        // window (the last step's falls on the next one)
+        const uint32_t em = static_cast<uint32_t>(((static_cast<uint64_t>(spmask) << 1) | prevbit) &
+                                                  ((1ull << Wk) - 1ull));
+        if (em) {
             const int q = atomicAdd(&w.ctr[2], 1);
             w.post_list[q] = static_cast<uint32_t>(j);
-            w.post_list[np + q] = spmask;
+            w.post_list[np + q] = em;
         }
     }
 }
@@ -837,12 +849,12 @@ __global__ void __launch_bounds__(256) k_win_deliver(const StepArgs<Real> a, Win
     }
 }
 
-// The facilitations owed by the posts that fired in the window on all their
-// in-edges: for a spike at n0 + kk, the facilitation at step n0 + kk + 1,
-// unless the edge's last update (an arrival) already covered it.  The last
-// step's K+ (step n0 + Wk, the next window's first) is formed here from the
-// carried pre trace and that step's arrival, as the next pretrace will.
-__global__ void __launch_bounds__(256) k_win_facilitate(WinDev w, const uint64_t *hist, int64_t n0, int Wk) {
+// The facilitations owed on all in-edges of the posts that fired at steps
+// n0 - 1 .. n0 + Wk - 2: for a spike at n0 - 1 + b, the facilitation at step
+// n0 + b (K+ kp[b]), unless the edge's last update (an arrival) already
+// covered it.  A spike of the window's last step is facilitated at the next
+// window's first step, as in the per-step form.
+__global__ void __launch_bounds__(256) k_win_facilitate(WinDev w, int64_t n0) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -851,7 +863,7 @@ __global__ void __launch_bounds__(256) k_win_facilitate(WinDev w, const uint64_t
     for (int64_t it = warp; it < nitems; it += nwarps) {
         const int q = static_cast<int>(it / C);
         const int j = static_cast<int>(w.post_list[q]);
-        const uint32_t mask = w.post_list[np + q];
+        const uint64_t mask = w.post_list[np + q];
         const int64_t beg = w.s.cindptr[j] + (it % C) * kChunkEdges, end = w.s.cindptr[j + 1];
         if (beg >= end) continue;
         int pre[kEdgeU];
@@ -873,19 +885,12 @@ __global__ void __launch_bounds__(256) k_win_facilitate(WinDev w, const uint64_t
 #pragma unroll
         for (int u = 0; u < kEdgeU; ++u) {
             if (pre[u] < 0) continue;
-            const int lo = up[u] > n0 ? static_cast<int>(up[u] - n0) : 0;
-            uint32_t due = mask & ~((1u << lo) - 1u);
+            const int lo = up[u] >= n0 - 1 ? static_cast<int>(up[u] - n0 + 1) : 0;
+            uint64_t due = mask & ~((1ull << lo) - 1ull);
             double x = wv[u];
-            for (; due; due &= due - 1u) {
-                const int kk = __ffs(static_cast<int>(due)) - 1;
-                double kplus;
-                if (kk + 1 < Wk) {
-                    kplus = w.kp[static_cast<size_t>(kk + 1) * w.s.n_pre + pre[u]];
-                } else {
-                    const double xv = fired(hist, w.s.pre_off + pre[u], n0 + Wk - w.s.lag) ? 1.0 : 0.0;
-                    kplus = (w.s.pre_trace[pre[u]] * w.s.dec_pre + xv) - xv;
-                }
-                x = stdp_facilitate(w.s, x, kplus);
+            for (; due; due &= due - 1ull) {
+                const int b = __ffsll(static_cast<long long>(due)) - 1;
+                x = stdp_facilitate(w.s, x, w.kp[static_cast<size_t>(b) * w.s.n_pre + pre[u]]);
             }
             w.s.w[eid[u]] = x;
         }
@@ -1118,7 +1123,7 @@ int run_windowed(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
         k_win_deliver<Real><<<eg, 256, 0, st>>>(a, w, n0);
         launches += 2;
         if (w.on) {
-            k_win_facilitate<<<eg, 256, 0, st>>>(w, a.hist, n0, Wk);
+            k_win_facilitate<<<eg, 256, 0, st>>>(w, n0);
             ++launches;
         }
         cudaError_t e = cudaGetLastError();
