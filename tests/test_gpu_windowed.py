@@ -23,7 +23,7 @@ IAF = [0.0, 250.0, 20.0, 2.0, 20.0, 10.0, 0.5, 0.5, 0.0, -math.inf]
 
 
 def _stdp_plan(NE=200, NI=50, KE=20, KI=5, J=20.68, seed=9, delay=15, windowed=True,
-               precision=64):
+               precision=64, semantics=_lib.LEGACY):
     rng = np.random.default_rng(seed)
     pieces = []
     for pre, K, w in ((0, KE, J), (1, KI, -5.0 * J)):
@@ -31,7 +31,7 @@ def _stdp_plan(NE=200, NI=50, KE=20, KI=5, J=20.68, seed=9, delay=15, windowed=T
             n_pre, n_post = (NE if pre == 0 else NI), (NE if post == 0 else NI)
             pieces.append((pre, post) + random_csr(rng, n_pre, n_post, K, w, delay))
     v0 = rng.uniform(0.0, 20.0, NE + NI)
-    pl = _lib.Plan(0.1, precision=precision)
+    pl = _lib.Plan(0.1, precision=precision, semantics=semantics)
     pl.add_pop(NE, IAF)
     pl.add_pop(NI, IAF)
     pl.add_poisson(0, 17789.0, 20.68, delay, 5)
@@ -99,7 +99,8 @@ def test_weight_recording_runs_per_step_forms_and_agrees():
 
 
 def test_short_lags_stay_per_step():
-    pl, _ = _stdp_plan(delay=1)
+    # kernel timing: a delay of one step is a lag of one step (W would be 1)
+    pl, _ = _stdp_plan(delay=1, semantics=_lib.RING)
     assert pl.engine == "per_step"
     with pytest.raises(NotImplementedError):
         pl.set_windowed(True)
