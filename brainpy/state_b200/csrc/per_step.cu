@@ -146,34 +146,57 @@ __device__ __forceinline__ double err_pow(double err, double q) {
 // iaf_cond_alpha.py:493-521) and the synaptic jumps after integration
 // (aeif_cond_alpha.py:709-728, iaf_cond_exp.py:594-614,
 // iaf_cond_alpha.py:602-624).  s: the NS ODE leaves, then h and I_stim.
-// Returns the spike flag.
+// The step is split into rk_begin, rk_substep (one trial step of the loop),
+// rk_done and rk_end, so that the windowed engine can let each lane walk
+// through its own steps (cond_step runs the four in sequence).
 template <typename Real, int MODEL>
-__device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Real w_in,
-                          double dt, int *err, unsigned long long *rk_iters) {
-    constexpr int NS = cond_n_ode(MODEL);
-    constexpr int kMaxIters = MODEL == 3 ? 10000 : 100000;  // the models' _MAX_ITERS
-    constexpr double min_h = 1e-8;
+struct RkState {
+    static constexpr int NS = cond_n_ode(MODEL);
     Real y[NS];
+    double h, t_loc;
+    Real i_stim;
+    int iters;
+    bool spiked, unstable;
+};
+template <int MODEL>
+__host__ __device__ constexpr int rk_max_iters() {
+    return MODEL == 3 ? 10000 : 100000;  // the models' _MAX_ITERS
+}
+constexpr double kRkMinH = 1e-8;
+
+template <typename Real, int MODEL>
+__device__ __forceinline__ void rk_begin(RkState<Real, MODEL> &q, const Real *s) {
+    constexpr int NS = RkState<Real, MODEL>::NS;
 #pragma unroll
-    for (int i = 0; i < NS; ++i) y[i] = s[i];
-    double h = static_cast<double>(s[NS]);
-    const Real i_stim = s[NS + 1];
+    for (int i = 0; i < NS; ++i) q.y[i] = s[i];
+    q.h = static_cast<double>(s[NS]);
+    q.i_stim = s[NS + 1];
+    q.spiked = false;
+    q.unstable = false;
+    q.t_loc = 0.0;
+    if (q.h < kRkMinH) q.h = kRkMinH;
+    q.iters = 0;
+}
+template <typename Real, int MODEL>
+__device__ __forceinline__ bool rk_done(const RkState<Real, MODEL> &q, double dt) {
+    return !(q.t_loc < dt && q.iters < rk_max_iters<MODEL>());
+}
+template <typename Real, int MODEL>
+__device__ __forceinline__ void rk_substep(const PopCoef<Real> &c, RkState<Real, MODEL> &q, int &r,
+                                           double dt) {
+    constexpr int NS = RkState<Real, MODEL>::NS;
     const double inv_atol = c.inv_atol;
-    bool spiked = false, unstable = false;
-    double t_loc = 0.0;
-    if (h < min_h) h = min_h;
-    int iters = 0;
     Real k[6][NS];
-    while (t_loc < dt && iters < kMaxIters) {
-        const double hh = h < dt - t_loc ? h : dt - t_loc;
-        h = hh > min_h ? hh : min_h;
-        const Real hR = static_cast<Real>(h);
+    {
+        const double hh = q.h < dt - q.t_loc ? q.h : dt - q.t_loc;
+        q.h = hh > kRkMinH ? hh : kRkMinH;
+        const Real hR = static_cast<Real>(q.h);
 #pragma unroll
         for (int st = 0; st < 6; ++st) {
             Real yi[NS];
             if (st == 0) {
 #pragma unroll
-                for (int i = 0; i < NS; ++i) yi[i] = y[i];
+                for (int i = 0; i < NS; ++i) yi[i] = q.y[i];
             } else {
 #pragma unroll
                 for (int i = 0; i < NS; ++i) {
@@ -187,11 +210,11 @@ __device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
                         acc = first ? term : acc + term;
                         first = false;
                     }
-                    yi[i] = y[i] + hR * acc;
+                    yi[i] = q.y[i] + hR * acc;
                 }
             }
-            if constexpr (MODEL == 2) aeif_vf<Real>(c, r, i_stim, yi, k[st]);
-            else iaf_cond_vf<Real, MODEL>(c, r, i_stim, yi, k[st]);
+            if constexpr (MODEL == 2) aeif_vf<Real>(c, r, q.i_stim, yi, k[st]);
+            else iaf_cond_vf<Real, MODEL>(c, r, q.i_stim, yi, k[st]);
         }
         Real yh[NS];
         double err = 0.0;
@@ -213,10 +236,10 @@ __device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
                     efirst = false;
                 }
             }
-            yh[i] = y[i] + hR * acc;
+            yh[i] = q.y[i] + hR * acc;
             const Real ye = hR * eacc;
-            const double ay = fabs(static_cast<double>(y[i])) > fabs(static_cast<double>(yh[i]))
-                                  ? fabs(static_cast<double>(y[i]))
+            const double ay = fabs(static_cast<double>(q.y[i])) > fabs(static_cast<double>(yh[i]))
+                                  ? fabs(static_cast<double>(q.y[i]))
                                   : fabs(static_cast<double>(yh[i]));
             // |err| / atol (rtol = 0); the 0 * |y| term carries a NaN or an
             // infinite state into the norm as the reference's scale does
@@ -224,21 +247,21 @@ __device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
             err = i == 0 ? e : ((err != err || e != e) ? NAN : (err > e ? err : e));
         }
         if (err != err) err = INFINITY;
-        const bool accept = (err <= 1.0) || (h <= min_h);
+        const bool accept = (err <= 1.0) || (q.h <= kRkMinH);
         if (accept) {
 #pragma unroll
-            for (int i = 0; i < NS; ++i) y[i] = yh[i];
-            t_loc = t_loc + h;
+            for (int i = 0; i < NS; ++i) q.y[i] = yh[i];
+            q.t_loc = q.t_loc + q.h;
             if constexpr (MODEL == 2) {
-                if (y[0] < Real(-1e3) || y[5] < Real(-1e6) || y[5] > Real(1e6)) unstable = true;
+                if (q.y[0] < Real(-1e3) || q.y[5] < Real(-1e6) || q.y[5] > Real(1e6)) q.unstable = true;
             } else if constexpr (MODEL == 3) {
-                if (y[0] < Real(-1e3)) unstable = true;
+                if (q.y[0] < Real(-1e3)) q.unstable = true;
             }
-            if (r > 0) y[0] = c.V_reset;
-            if (r <= 0 && y[0] >= c.v_peak_detect) {
-                spiked = true;
-                y[0] = c.V_reset;
-                if constexpr (MODEL == 2) y[5] = y[5] + c.b;
+            if (r > 0) q.y[0] = c.V_reset;
+            if (r <= 0 && q.y[0] >= c.v_peak_detect) {
+                q.spiked = true;
+                q.y[0] = c.V_reset;
+                if constexpr (MODEL == 2) q.y[5] = q.y[5] + c.b;
                 if (c.ref_count > 0) r = c.ref_count + 1;
             }
         }
@@ -251,32 +274,46 @@ __device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Re
             fac = 0.9 * err_pow<Real>(err_sg, 0.25);
             fac = fac < 0.2 ? 0.2 : (fac > 1.0 ? 1.0 : fac);
         }
-        const double hn = h * fac;
-        h = hn > min_h ? hn : min_h;
-        ++iters;
+        const double hn = q.h * fac;
+        q.h = hn > kRkMinH ? hn : kRkMinH;
+        ++q.iters;
     }
-    if (iters >= kMaxIters && t_loc < dt) atomicExch(err, BSPK_DEV_ERR_RKCAP);
-    if (unstable) atomicExch(err, BSPK_DEV_ERR_UNSTABLE);
+}
+template <typename Real, int MODEL>
+__device__ __forceinline__ bool rk_end(const PopCoef<Real> &c, RkState<Real, MODEL> &q, Real *s, int &r,
+                                       Real w_ex, Real w_in, double dt, int *err,
+                                       unsigned long long *rk_iters) {
+    constexpr int NS = RkState<Real, MODEL>::NS;
+    if (q.iters >= rk_max_iters<MODEL>() && q.t_loc < dt) atomicExch(err, BSPK_DEV_ERR_RKCAP);
+    if (q.unstable) atomicExch(err, BSPK_DEV_ERR_UNSTABLE);
     {
         // one atomic per group of converged lanes, not one per neuron
         const unsigned m = __activemask();
-        const unsigned sum = __reduce_add_sync(m, static_cast<unsigned>(iters));
+        const unsigned sum = __reduce_add_sync(m, static_cast<unsigned>(q.iters));
         if ((threadIdx.x & 31) == __ffs(m) - 1)
             atomicAdd(rk_iters, static_cast<unsigned long long>(sum));
     }
     if (r > 0) r = r - 1;
     if constexpr (MODEL == 3) {
-        y[1] = y[1] + w_ex;
-        y[2] = y[2] + w_in;
+        q.y[1] = q.y[1] + w_ex;
+        q.y[2] = q.y[2] + w_in;
     } else {
-        y[1] = y[1] + c.pscon_ex * w_ex;
-        y[3] = y[3] + c.pscon_in * w_in;
+        q.y[1] = q.y[1] + c.pscon_ex * w_ex;
+        q.y[3] = q.y[3] + c.pscon_in * w_in;
     }
 #pragma unroll
-    for (int i = 0; i < NS; ++i) s[i] = y[i];
-    s[NS] = static_cast<Real>(h);
+    for (int i = 0; i < NS; ++i) s[i] = q.y[i];
+    s[NS] = static_cast<Real>(q.h);
     s[NS + 1] = Real(0);  // no current input on this path: I_stim <- 0
-    return spiked;
+    return q.spiked;
+}
+template <typename Real, int MODEL>
+__device__ bool cond_step(const PopCoef<Real> &c, Real *s, int &r, Real w_ex, Real w_in,
+                          double dt, int *err, unsigned long long *rk_iters) {
+    RkState<Real, MODEL> q;
+    rk_begin<Real, MODEL>(q, s);
+    while (!rk_done<Real, MODEL>(q, dt)) rk_substep<Real, MODEL>(c, q, r, dt);
+    return rk_end<Real, MODEL>(c, q, s, r, w_ex, w_in, dt, err, rk_iters);
 }
 
 // iaf_psc_exp_multisynapse (_nest_neuron/iaf_psc_exp_multisynapse.py:716-790):
@@ -712,6 +749,97 @@ __global__ void __launch_bounds__(256) k_win_arrivals(WinDev w) {
     }
 }
 
+// Inputs of window step n = n0 + k of neuron g: the ring slot, then (a post
+// of the plastic projection) the post trace of step n and the arrivals of
+// step n -- each edge first receives the facilitations the post's spikes
+// still owe it, then the depression, and its new weight joins the input --
+// then the drives.
+template <typename Real>
+__device__ __forceinline__ void win_inputs(const StepArgs<Real> &a, const WinDev &w, int g, int p,
+                                           const PopCoef<Real> &c, int64_t n0, int k, bool pp,
+                                           int j, uint64_t prevbit, uint32_t spmask,
+                                           double &post_tr, Real (&in)[kMaxReceptors]) {
+    const int64_t n = n0 + k;
+    step_inputs<Real>(a, g, p, c, n, in);
+    if (pp) {
+        const int np = w.s.n_post;
+        // post trace of step n (decay, then the spike of n - 1) and the K- of
+        // a depression at n (without that spike)
+        const bool yb = k == 0 ? prevbit != 0 : ((spmask >> (k - 1)) & 1u) != 0;
+        const double y = yb ? 1.0 : 0.0;
+        const double t = post_tr * w.s.dec_post + y;
+        const double kminus = t - y;
+        post_tr = t;
+        const size_t ci = static_cast<size_t>(k) * np + j;
+        int na = w.cnt[ci];
+        w.cnt[ci] = 0;  // cleared for the next window
+        if (na > w.cap) na = w.cap;
+        // the post's spikes at n0 - 1 + b (bit b), facilitated at n0 + b
+        // with K+ kp[b]
+        const uint64_t emask = (static_cast<uint64_t>(spmask) << 1) | prevbit;
+        const int rec = w.s.receptor < a.R ? w.s.receptor : 0;
+        for (int q = 0; q < na; ++q) {
+            const uint2 en = w.arr[(static_cast<size_t>(k) * w.cap + q) * np + j];
+            const int64_t e = en.x;
+            const int pre = static_cast<int>(en.y);
+            double wv = w.s.w[e];
+            // facilitations at steps f in (fdone, n]: fdone is the edge's last
+            // update, or n0 - 1 (the window before brought every edge there)
+            const long long u = w.upto[e];
+            const int lo = u >= n0 - 1 ? static_cast<int>(u - n0 + 1) : 0;
+            uint64_t due = emask & ((2ull << k) - 1ull) & ~((1ull << lo) - 1ull);
+            for (; due; due &= due - 1ull) {
+                const int b = __ffsll(static_cast<long long>(due)) - 1;
+                wv = stdp_facilitate(w.s, wv, w.kp[static_cast<size_t>(b) * w.s.n_pre + pre]);
+            }
+            wv = stdp_depress(w.s, wv, kminus);
+            w.s.w[e] = wv;
+            w.upto[e] = n;
+            in[rec] += static_cast<Real>(wv);
+        }
+    }
+    step_drives<Real>(a, g, p, c, n, in);
+}
+
+// the bookkeeping after window step n0 + k of neuron g
+template <typename Real>
+__device__ __forceinline__ void win_after_step(const StepArgs<Real> &a, const WinDev &w, int g,
+                                               int64_t n0, int k, bool sp, Real v,
+                                               uint32_t &spmask, uint64_t &hw) {
+    const int64_t n = n0 + k;
+    spmask |= static_cast<uint32_t>(sp) << k;
+    const int bit = static_cast<int>(n & 63);
+    hw = (hw & ~(1ull << bit)) | (static_cast<uint64_t>(sp) << bit);
+    if (sp) {
+        const int pos = atomicAdd(&w.ctr[0], 1);
+        w.spk[pos] = (static_cast<uint32_t>(g) << 5) | static_cast<uint32_t>(k);
+        step_record_spike<Real>(a, g, n);
+    }
+    step_record_v<Real>(a, g, n, v);
+}
+
+// the end of a window for neuron g: its spike history, post trace and (a
+// post that fired at n0 - 1 .. n0 + Wk - 2) its entry in the post list
+template <typename Real>
+__device__ __forceinline__ void win_close(const StepArgs<Real> &a, const WinDev &w, int g, bool pp, int j,
+                                          int Wk, uint64_t prevbit, uint32_t spmask, uint64_t hw,
+                                          double post_tr) {
+    a.hist[g] = hw;
+    if (pp) {
+        w.s.post_trace[j] = post_tr;
+        // the last step's spike is facilitated in the next window
+        const uint32_t em = static_cast<uint32_t>(((static_cast<uint64_t>(spmask) << 1) | prevbit) &
+                                                  ((1ull << Wk) - 1ull));
+        if (em) {
+            const int q = atomicAdd(&w.ctr[2], 1);
+            w.post_list[q] = static_cast<uint32_t>(j);
+            w.post_list[w.s.n_post + q] = em;
+        }
+    }
+}
+
+// Neuron pass of a window for the exact-propagator models (and any model):
+// one thread per neuron, the window's steps in order.
 template <typename Real, int MODEL>
 __global__ void __launch_bounds__(128) k_win_neuron(const StepArgs<Real> a, WinDev w, int64_t n0, int Wk,
                                                     double dt) {
@@ -724,85 +852,69 @@ __global__ void __launch_bounds__(128) k_win_neuron(const StepArgs<Real> a, WinD
 #pragma unroll
     for (int i = 0; i < 8; ++i) st[i] = i < kSlots ? a.s[i][g] : Real(0);
     int r = a.r[g];
-    const int np = w.s.n_post;
     const int j = g - w.s.post_off;
-    const bool pp = w.on && j >= 0 && j < np;  // a post of the plastic projection
+    const bool pp = w.on && j >= 0 && j < w.s.n_post;  // a post of the plastic projection
     double post_tr = pp ? w.s.post_trace[j] : 0.0;
-    const int rec = w.s.receptor < a.R ? w.s.receptor : 0;
     uint64_t hw = a.hist[g];
     // the spike of step n0 - 1, whose facilitation falls on step n0
     const uint64_t prevbit = (n0 >= 1 && ((hw >> ((n0 - 1) & 63)) & 1ull) != 0) ? 1ull : 0ull;
     uint32_t spmask = 0u;
     for (int k = 0; k < Wk; ++k) {
-        const int64_t n = n0 + k;
         Real in[kMaxReceptors];
-        step_inputs<Real>(a, g, p, c, n, in);
-        if (pp) {
-            // post trace of step n (decay, then the spike of n - 1) and the
-            // K- of a depression at n (without that spike)
-            const bool yb = k == 0 ? (n >= 1 && ((hw >> ((n - 1) & 63)) & 1ull) != 0)
-                                   : ((spmask >> (k - 1)) & 1u) != 0;
-            const double y = yb ? 1.0 : 0.0;
-            const double t = post_tr * w.s.dec_post + y;
-            const double kminus = t - y;
-            post_tr = t;
-            const size_t ci = static_cast<size_t>(k) * np + j;
-            int na = w.cnt[ci];
-            w.cnt[ci] = 0;  // cleared for the next window
-            if (na > w.cap) na = w.cap;
-            for (int q = 0; q < na; ++q) {
-                const uint2 en = w.arr[(static_cast<size_t>(k) * w.cap + q) * np + j];
-                const int64_t e = en.x;
-                const int pre = static_cast<int>(en.y);
-                double wv = w.s.w[e];
-                // facilitations at steps f in (fdone, n] for the post's
-                // spikes at f - 1 >= n0 - 1 (bit b of emask: a spike at
-                // n0 - 1 + b, facilitated at n0 + b with K+ kp[b]); fdone is
-                // the edge's last update, or n0 - 1 (the window before
-                // brought every edge to n0 - 1)
-                const uint64_t emask = (static_cast<uint64_t>(spmask) << 1) | prevbit;
-                const long long u = w.upto[e];
-                const int lo = u >= n0 - 1 ? static_cast<int>(u - n0 + 1) : 0;
-                uint64_t due = emask & ((2ull << k) - 1ull) & ~((1ull << lo) - 1ull);
-                for (; due; due &= due - 1ull) {
-                    const int b = __ffsll(static_cast<long long>(due)) - 1;
-                    wv = stdp_facilitate(w.s, wv, w.kp[static_cast<size_t>(b) * w.s.n_pre + pre]);
-                }
-                wv = stdp_depress(w.s, wv, kminus);
-                w.s.w[e] = wv;
-                w.upto[e] = n;
-                in[rec] += static_cast<Real>(wv);
-            }
-        }
-        step_drives<Real>(a, g, p, c, n, in);
+        win_inputs<Real>(a, w, g, p, c, n0, k, pp, j, prevbit, spmask, post_tr, in);
         const bool sp = step_update<Real, MODEL>(a, c, st, r, in, dt);
-        spmask |= static_cast<uint32_t>(sp) << k;
-        const int bit = static_cast<int>(n & 63);
-        hw = (hw & ~(1ull << bit)) | (static_cast<uint64_t>(sp) << bit);
-        if (sp) {
-            const int pos = atomicAdd(&w.ctr[0], 1);
-            w.spk[pos] = (static_cast<uint32_t>(g) << 5) | static_cast<uint32_t>(k);
-            step_record_spike<Real>(a, g, n);
-        }
-        step_record_v<Real>(a, g, n, st[0]);
+        win_after_step<Real>(a, w, g, n0, k, sp, st[0], spmask, hw);
     }
 #pragma unroll
     for (int i = 0; i < 8; ++i)
         if (i < kSlots) a.s[i][g] = st[i];
     a.r[g] = r;
-    a.hist[g] = hw;
-    if (pp) {
-        w.s.post_trace[j] = post_tr;
-        // spikes at n0 - 1 .. n0 + Wk - 2: their facilitations fall in this
-        // window (the last step's falls on the next one)
-        const uint32_t em = static_cast<uint32_t>(((static_cast<uint64_t>(spmask) << 1) | prevbit) &
-                                                  ((1ull << Wk) - 1ull));
-        if (em) {
-            const int q = atomicAdd(&w.ctr[2], 1);
-            w.post_list[q] = static_cast<uint32_t>(j);
-            w.post_list[np + q] = em;
+    win_close<Real>(a, w, g, pp, j, Wk, prevbit, spmask, hw, post_tr);
+}
+
+// Neuron pass of a window for the RKF45 models: each lane walks through its
+// own steps -- a trial step of the adaptive loop, or, when its step's
+// interval is integrated, that step's inputs, jumps and spike -- so a warp
+// takes the largest per-lane sum of trial steps over the window instead of
+// the sum over steps of the largest per-lane count.
+template <typename Real, int MODEL>
+__global__ void __launch_bounds__(128) k_win_neuron_rk(const StepArgs<Real> a, WinDev w, int64_t n0,
+                                                       int Wk, double dt) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= a.N) return;
+    const int p = find_pop_t(a.coef, a.npop, g);
+    const PopCoef<Real> c = a.coef[p];
+    constexpr int kSlots = model_n_slots(MODEL);
+    Real st[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) st[i] = i < kSlots ? a.s[i][g] : Real(0);
+    int r = a.r[g];
+    const int j = g - w.s.post_off;
+    const bool pp = w.on && j >= 0 && j < w.s.n_post;
+    double post_tr = pp ? w.s.post_trace[j] : 0.0;
+    uint64_t hw = a.hist[g];
+    const uint64_t prevbit = (n0 >= 1 && ((hw >> ((n0 - 1) & 63)) & 1ull) != 0) ? 1ull : 0ull;
+    uint32_t spmask = 0u;
+    RkState<Real, MODEL> q;
+    rk_begin<Real, MODEL>(q, st);
+    int k = 0;
+    while (k < Wk) {
+        if (!rk_done<Real, MODEL>(q, dt)) {
+            rk_substep<Real, MODEL>(c, q, r, dt);
+            continue;
         }
+        Real in[kMaxReceptors];
+        win_inputs<Real>(a, w, g, p, c, n0, k, pp, j, prevbit, spmask, post_tr, in);
+        const bool sp = rk_end<Real, MODEL>(c, q, st, r, in[0], in[1], dt, a.err, a.rk_iters);
+        win_after_step<Real>(a, w, g, n0, k, sp, st[0], spmask, hw);
+        ++k;
+        if (k < Wk) rk_begin<Real, MODEL>(q, st);
     }
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        if (i < kSlots) a.s[i][g] = st[i];
+    a.r[g] = r;
+    win_close<Real>(a, w, g, pp, j, Wk, prevbit, spmask, hw, post_tr);
 }
 
 // Static delivery of the window's spikes (as k_deliver_static, a spike of
@@ -1115,9 +1227,9 @@ int run_windowed(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
         switch (a.model) {
             case 0: k_win_neuron<Real, 0><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
             case 1: k_win_neuron<Real, 1><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
-            case 2: k_win_neuron<Real, 2><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
-            case 3: k_win_neuron<Real, 3><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
-            case 4: k_win_neuron<Real, 4><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
+            case 2: k_win_neuron_rk<Real, 2><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
+            case 3: k_win_neuron_rk<Real, 3><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
+            case 4: k_win_neuron_rk<Real, 4><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
             default: k_win_neuron<Real, 5><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
         }
         k_win_deliver<Real><<<eg, 256, 0, st>>>(a, w, n0);
