@@ -79,7 +79,7 @@ struct WinDev {
     int W, cap;            // window; arrivals held per (step, post)
     double *kp;            // [W][n_pre] pre trace at step n0 + k without that step's arrival
     long long *upto;       // [edges] last step whose facilitation reached the edge
-    uint2 *arr;            // [W][cap][n_post] (CSR edge, pre) arriving at n0 + k
+    WinArrival *arr;       // [W][cap][n_post] arrivals at n0 + k
     int *cnt;              // [W][n_post] arrivals per (step, post), cleared by their reader
     uint32_t *spk;         // spikes of the window: gid << 5 | step in window
     uint32_t *pre_list;    // pres with arrivals in the window, then their step masks

@@ -1061,7 +1061,7 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
             for (int32_t q : J.post_local) indeg[q]++;
             const int64_t mx = indeg.empty() ? 0 : *std::max_element(indeg.begin(), indeg.end());
             arr_bytes = static_cast<size_t>(std::max(Ww, 1)) * std::max<int64_t>(mx, 1) *
-                        p->pops[J.post].n * sizeof(uint2);
+                        p->pops[J.post].n * sizeof(WinArrival);
             p->win_cap = static_cast<int>(std::max<int64_t>(mx, 1));
         }
         p->win = p->win_ok = Ww >= 2 && n_pl <= 1 && pl_ok && arr_bytes <= (size_t(16) << 30);

@@ -126,7 +126,7 @@ struct bspk_plan {
     bool win = false, win_ok = false;  // selected, possible
     double *d_win_kp = nullptr;
     long long *d_win_upto = nullptr;
-    uint2 *d_win_arr = nullptr;
+    bspk::WinArrival *d_win_arr = nullptr;
     int *d_win_cnt = nullptr;
     int win_cap = 0;
     uint32_t *d_win_spk = nullptr;
