@@ -44,6 +44,10 @@ constexpr int kEdgeU = 8;
 constexpr int kChunkEdges = 32 * kEdgeU;
 // longest window of the windowed engine (a step mask is 32 bits)
 constexpr int kMaxWin = 32;
+// an arrival's pre index takes the low 26 bits; the RKF45 window kernel
+// keeps the step of the edge's previous arrival in the window above them
+constexpr int kWinPreBits = 26;
+constexpr uint32_t kWinPreMask = (1u << kWinPreBits) - 1u;
 
 __device__ __forceinline__ bool fired(const uint64_t *hist, int gid, int64_t m) {
     if (m < 0) return false;
@@ -940,14 +944,19 @@ __global__ void __launch_bounds__(128) k_win_neuron_rk(const StepArgs<Real> a, W
             for (int q = 0; q < na; ++q) {
                 WinArrival &en = w.arr[(static_cast<size_t>(k) * w.cap + q) * np + j];
                 const int64_t e = en.e;
+                const uint32_t pre = en.pre;
                 double wv = w.s.w[e];
                 en.w_before = wv;
                 const long long u = w.upto[e];
+                // the step of the edge's previous arrival in this window (its
+                // last update, when inside the window), kept above the pre
+                // index: 0 none, else step + 1
+                const uint32_t prev = u >= n0 ? static_cast<uint32_t>(u - n0 + 1) : 0u;
+                en.pre = pre | (prev << kWinPreBits);
                 // of the facilitations owed (steps after the edge's last
                 // update, up to n), a silent post owes only that of its
                 // spike at n0 - 1, at step n0
-                if (prevbit && u < n0)
-                    wv = stdp_facilitate(w.s, wv, w.kp[static_cast<size_t>(en.pre)]);
+                if (prevbit && u < n0) wv = stdp_facilitate(w.s, wv, w.kp[static_cast<size_t>(pre)]);
                 wv = stdp_depress(w.s, wv, kminus);
                 w.s.w[e] = wv;
                 w.upto[e] = n;
@@ -984,14 +993,9 @@ __global__ void __launch_bounds__(128) k_win_neuron_rk(const StepArgs<Real> a, W
                 pl = Real(0);
                 for (int qq = 0; qq < nak[k]; ++qq) {
                     const WinArrival &en = w.arr[(static_cast<size_t>(k) * w.cap + qq) * np + j];
+                    const uint32_t pre = en.pre & kWinPreMask;
                     // the edge's previous arrival in this window, if any
-                    int kp_prev = -1;
-                    for (int kk = k - 1; kk >= 0 && kp_prev < 0; --kk)
-                        for (int q2 = 0; q2 < nak[kk]; ++q2)
-                            if (w.arr[(static_cast<size_t>(kk) * w.cap + q2) * np + j].e == en.e) {
-                                kp_prev = kk;
-                                break;
-                            }
+                    const int kp_prev = static_cast<int>(en.pre >> kWinPreBits) - 1;
                     // before it: the redone value of an arrival after s0,
                     // else the value kept (exact up to s0)
                     double wv = kp_prev > s0 ? w.s.w[en.e] : en.w_before;
@@ -999,7 +1003,7 @@ __global__ void __launch_bounds__(128) k_win_neuron_rk(const StepArgs<Real> a, W
                     uint64_t due = emask & ((2ull << k) - 1ull) & ~((1ull << lo) - 1ull);
                     for (; due; due &= due - 1ull) {
                         const int b = __ffsll(static_cast<long long>(due)) - 1;
-                        wv = stdp_facilitate(w.s, wv, w.kp[static_cast<size_t>(b) * w.s.n_pre + en.pre]);
+                        wv = stdp_facilitate(w.s, wv, w.kp[static_cast<size_t>(b) * w.s.n_pre + pre]);
                     }
                     wv = stdp_depress(w.s, wv, kminus);
                     w.s.w[en.e] = wv;
