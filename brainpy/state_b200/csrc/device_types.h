@@ -104,12 +104,9 @@ struct ProjDev {
     const double *cw;        // per in-edge weight (nullptr when homogeneous)
 };
 
-// An arrival of a window: CSR edge, pre, and the edge's weight before it
-// (kept by the RKF45 window kernel, which updates plastic weights ahead of
-// its integration and must be able to redo an update).
+// An arrival of a window: CSR edge and pre.
 struct WinArrival {
     uint32_t e, pre;
-    double w_before;
 };
 
 }  // namespace bspk

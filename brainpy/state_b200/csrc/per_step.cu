@@ -42,12 +42,6 @@ __device__ __forceinline__ int find_pop_t(const PopCoef<Real> *c, int npop, int 
 // kChunkEdges = 32 kEdgeU per warp-sized item.
 constexpr int kEdgeU = 8;
 constexpr int kChunkEdges = 32 * kEdgeU;
-// longest window of the windowed engine (a step mask is 32 bits)
-constexpr int kMaxWin = 32;
-// an arrival's pre index takes the low 26 bits; the RKF45 window kernel
-// keeps the step of the edge's previous arrival in the window above them
-constexpr int kWinPreBits = 26;
-constexpr uint32_t kWinPreMask = (1u << kWinPreBits) - 1u;
 
 __device__ __forceinline__ bool fired(const uint64_t *hist, int gid, int64_t m) {
     if (m < 0) return false;
@@ -153,8 +147,7 @@ __device__ __forceinline__ double err_pow(double err, double q) {
 // (aeif_cond_alpha.py:709-728, iaf_cond_exp.py:594-614,
 // iaf_cond_alpha.py:602-624).  s: the NS ODE leaves, then h and I_stim.
 // The step is split into rk_begin, rk_substep (one trial step of the loop),
-// rk_done and rk_end, so that the windowed engine can let each lane walk
-// through its own steps (cond_step runs the four in sequence).
+// rk_done and rk_end (cond_step runs the four in sequence).
 template <typename Real, int MODEL>
 struct RkState {
     static constexpr int NS = cond_n_ode(MODEL);
@@ -292,9 +285,8 @@ __device__ __forceinline__ bool rk_end(const PopCoef<Real> &c, RkState<Real, MOD
     constexpr int NS = RkState<Real, MODEL>::NS;
     if (q.iters >= rk_max_iters<MODEL>() && q.t_loc < dt) atomicExch(err, BSPK_DEV_ERR_RKCAP);
     if (q.unstable) atomicExch(err, BSPK_DEV_ERR_UNSTABLE);
-    if (rk_iters) {
-        // one atomic per group of converged lanes, not one per neuron (a
-        // caller passing nullptr counts the trial steps itself)
+    {
+        // one atomic per group of converged lanes, not one per neuron
         const unsigned m = __activemask();
         const unsigned sum = __reduce_add_sync(m, static_cast<unsigned>(q.iters));
         if ((threadIdx.x & 31) == __ffs(m) - 1)
@@ -768,10 +760,9 @@ template <typename Real>
 __device__ __forceinline__ void win_inputs(const StepArgs<Real> &a, const WinDev &w, int g, int p,
                                            const PopCoef<Real> &c, int64_t n0, int k, bool pp,
                                            int j, uint64_t prevbit, uint32_t spmask,
-                                           double &post_tr, Real (&in)[kMaxReceptors],
-                                           bool with_static = true) {
+                                           double &post_tr, Real (&in)[kMaxReceptors]) {
     const int64_t n = n0 + k;
-    if (with_static) step_inputs<Real>(a, g, p, c, n, in);
+    step_inputs<Real>(a, g, p, c, n, in);
     if (pp) {
         const int np = w.s.n_post;
         // post trace of step n (decay, then the spike of n - 1) and the K- of
@@ -809,7 +800,7 @@ __device__ __forceinline__ void win_inputs(const StepArgs<Real> &a, const WinDev
             in[rec] += static_cast<Real>(wv);
         }
     }
-    if (with_static) step_drives<Real>(a, g, p, c, n, in);
+    step_drives<Real>(a, g, p, c, n, in);
 }
 
 // the bookkeeping after window step n0 + k of neuron g
@@ -875,162 +866,6 @@ __global__ void __launch_bounds__(128) k_win_neuron(const StepArgs<Real> a, WinD
         win_inputs<Real>(a, w, g, p, c, n0, k, pp, j, prevbit, spmask, post_tr, in);
         const bool sp = step_update<Real, MODEL>(a, c, st, r, in, dt);
         win_after_step<Real>(a, w, g, n0, k, sp, st[0], spmask, hw);
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-        if (i < kSlots) a.s[i][g] = st[i];
-    a.r[g] = r;
-    win_close<Real>(a, w, g, pp, j, Wk, prevbit, spmask, hw, post_tr);
-}
-
-// Neuron pass of a window for the RKF45 models: each lane walks through its
-// own steps -- a trial step of the adaptive loop, or, when its step's
-// interval is integrated, that step's inputs, jumps and spike -- so a warp
-// takes the largest per-lane sum of trial steps over the window instead of
-// the sum over steps of the largest per-lane count.  So that a step's end
-// costs only register work, every input is formed beforehand with the warp
-// in step: the ring and drive inputs of each step, and for a plastic post
-// the plastic arrivals of each step as they are if the post does not fire
-// before them (its spike of n0 - 1 included): each weight is updated then,
-// in step order, with its previous value kept in the arrival.  If the post
-// fires at step s of the window, the arrivals after s are updated again at
-// their step's end from the kept values (or from the weight that an earlier
-// such redo left, for an edge with two arrivals after s), with the true
-// post trace and the facilitations of the spikes.
-template <typename Real, int MODEL>
-__global__ void __launch_bounds__(128) k_win_neuron_rk(const StepArgs<Real> a, WinDev w, int64_t n0,
-                                                       int Wk, double dt) {
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= a.N) return;
-    const int p = find_pop_t(a.coef, a.npop, g);
-    const PopCoef<Real> c = a.coef[p];
-    constexpr int kSlots = model_n_slots(MODEL);
-    Real st[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) st[i] = i < kSlots ? a.s[i][g] : Real(0);
-    int r = a.r[g];
-    const int np = w.s.n_post;
-    const int j = g - w.s.post_off;
-    const bool pp = w.on && j >= 0 && j < np;
-    const int rec = w.s.receptor < a.R ? w.s.receptor : 0;
-    double post_tr = pp ? w.s.post_trace[j] : 0.0;
-    uint64_t hw = a.hist[g];
-    const uint64_t prevbit = (n0 >= 1 && ((hw >> ((n0 - 1) & 63)) & 1ull) != 0) ? 1ull : 0ull;
-    // inputs of every step of the window
-    Real pin[kMaxWin][2];
-    Real pspec[kMaxWin];   // plastic input of the step if the post stays silent before it
-    int nak[kMaxWin];      // arrivals of the step
-    {
-        double tr = post_tr;
-        for (int k = 0; k < Wk; ++k) {
-            const int64_t n = n0 + k;
-            Real in[kMaxReceptors];
-            step_inputs<Real>(a, g, p, c, n, in);
-            step_drives<Real>(a, g, p, c, n, in);
-            pin[k][0] = in[0];
-            pin[k][1] = in[1];
-            pspec[k] = Real(0);
-            nak[k] = 0;
-            if (!pp) continue;
-            const double y = k == 0 ? static_cast<double>(prevbit) : 0.0;
-            const double t = tr * w.s.dec_post + y;
-            const double kminus = t - y;
-            tr = t;
-            const size_t ci = static_cast<size_t>(k) * np + j;
-            int na = w.cnt[ci];
-            w.cnt[ci] = 0;  // cleared for the next window
-            if (na > w.cap) na = w.cap;
-            nak[k] = na;
-            for (int q = 0; q < na; ++q) {
-                WinArrival &en = w.arr[(static_cast<size_t>(k) * w.cap + q) * np + j];
-                const int64_t e = en.e;
-                const uint32_t pre = en.pre;
-                double wv = w.s.w[e];
-                en.w_before = wv;
-                const long long u = w.upto[e];
-                // the step of the edge's previous arrival in this window (its
-                // last update, when inside the window), kept above the pre
-                // index: 0 none, else step + 1
-                const uint32_t prev = u >= n0 ? static_cast<uint32_t>(u - n0 + 1) : 0u;
-                en.pre = pre | (prev << kWinPreBits);
-                // of the facilitations owed (steps after the edge's last
-                // update, up to n), a silent post owes only that of its
-                // spike at n0 - 1, at step n0
-                if (prevbit && u < n0) wv = stdp_facilitate(w.s, wv, w.kp[static_cast<size_t>(pre)]);
-                wv = stdp_depress(w.s, wv, kminus);
-                w.s.w[e] = wv;
-                w.upto[e] = n;
-                pspec[k] += static_cast<Real>(wv);
-            }
-        }
-    }
-    int rs = -1;  // this neuron's column of the V_m record
-    if (a.rec_slot) rs = a.rec_slot[g];
-    uint32_t spmask = 0u;
-    RkState<Real, MODEL> q;
-    rk_begin<Real, MODEL>(q, st);
-    unsigned iters = 0u;
-    int k = 0;
-    while (k < Wk) {
-        if (!rk_done<Real, MODEL>(q, dt)) {
-            rk_substep<Real, MODEL>(c, q, r, dt);
-            continue;
-        }
-        const int64_t n = n0 + k;
-        Real in0 = pin[k][0], in1 = pin[k][1];
-        if (pp) {
-            const bool yb = k == 0 ? prevbit != 0 : ((spmask >> (k - 1)) & 1u) != 0;
-            const double y = yb ? 1.0 : 0.0;
-            const double t = post_tr * w.s.dec_post + y;
-            const double kminus = t - y;
-            post_tr = t;
-            Real pl = pspec[k];
-            if ((spmask & ((1u << k) - 1u)) != 0u) {
-                // the post fired at step s0 < k of the window: redo this
-                // step's updates with the facilitations of its spikes
-                const int s0 = __ffs(static_cast<int>(spmask)) - 1;
-                const uint64_t emask = (static_cast<uint64_t>(spmask) << 1) | prevbit;
-                pl = Real(0);
-                for (int qq = 0; qq < nak[k]; ++qq) {
-                    const WinArrival &en = w.arr[(static_cast<size_t>(k) * w.cap + qq) * np + j];
-                    const uint32_t pre = en.pre & kWinPreMask;
-                    // the edge's previous arrival in this window, if any
-                    const int kp_prev = static_cast<int>(en.pre >> kWinPreBits) - 1;
-                    // before it: the redone value of an arrival after s0,
-                    // else the value kept (exact up to s0)
-                    double wv = kp_prev > s0 ? w.s.w[en.e] : en.w_before;
-                    const int lo = kp_prev >= 0 ? kp_prev + 1 : 0;
-                    uint64_t due = emask & ((2ull << k) - 1ull) & ~((1ull << lo) - 1ull);
-                    for (; due; due &= due - 1ull) {
-                        const int b = __ffsll(static_cast<long long>(due)) - 1;
-                        wv = stdp_facilitate(w.s, wv, w.kp[static_cast<size_t>(b) * w.s.n_pre + pre]);
-                    }
-                    wv = stdp_depress(w.s, wv, kminus);
-                    w.s.w[en.e] = wv;
-                    pl += static_cast<Real>(wv);
-                }
-            }
-            if (rec == 0) in0 += pl;
-            else in1 += pl;
-        }
-        iters += static_cast<unsigned>(q.iters);
-        const bool sp = rk_end<Real, MODEL>(c, q, st, r, in0, in1, dt, a.err, nullptr);
-        spmask |= static_cast<uint32_t>(sp) << k;
-        const int bit = static_cast<int>(n & 63);
-        hw = (hw & ~(1ull << bit)) | (static_cast<uint64_t>(sp) << bit);
-        if (sp) {
-            const int pos = atomicAdd(&w.ctr[0], 1);
-            w.spk[pos] = (static_cast<uint32_t>(g) << 5) | static_cast<uint32_t>(k);
-            step_record_spike<Real>(a, g, n);
-        }
-        if (rs >= 0) a.v_out[static_cast<size_t>(n - a.run_step0) * a.n_rec + rs] = st[0];
-        ++k;
-        if (k < Wk) rk_begin<Real, MODEL>(q, st);
-    }
-    {
-        const unsigned m = __activemask();
-        const unsigned sum = __reduce_add_sync(m, iters);
-        if ((threadIdx.x & 31) == __ffs(m) - 1) atomicAdd(a.rk_iters, static_cast<unsigned long long>(sum));
     }
 #pragma unroll
     for (int i = 0; i < 8; ++i)
@@ -1349,9 +1184,9 @@ int run_windowed(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
         switch (a.model) {
             case 0: k_win_neuron<Real, 0><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
             case 1: k_win_neuron<Real, 1><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
-            case 2: k_win_neuron_rk<Real, 2><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
-            case 3: k_win_neuron_rk<Real, 3><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
-            case 4: k_win_neuron_rk<Real, 4><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
+            case 2: k_win_neuron<Real, 2><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
+            case 3: k_win_neuron<Real, 3><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
+            case 4: k_win_neuron<Real, 4><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
             default: k_win_neuron<Real, 5><<<nb, 128, 0, st>>>(a, w, n0, Wk, dt); break;
         }
         k_win_deliver<Real><<<eg, 256, 0, st>>>(a, w, n0);

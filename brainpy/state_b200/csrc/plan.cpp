@@ -1055,9 +1055,7 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
         for (auto &J : p->projs) {
             if (!J.plastic) continue;
             ++n_pl;
-            // (edge ids in 32 bits, pre indices in 26: WinArrival)
-            pl_ok = pl_ok && J.rule == 0 && J.post_local.size() < (size_t(1) << 32) &&
-                    p->pops[J.pre].n < (1 << 26);
+            pl_ok = pl_ok && J.rule == 0 && J.post_local.size() < (size_t(1) << 32);
             for (int32_t d : J.delay) pl_ok = pl_ok && d == J.delay[0];
             std::vector<int64_t> indeg(p->pops[J.post].n, 0);
             for (int32_t q : J.post_local) indeg[q]++;
