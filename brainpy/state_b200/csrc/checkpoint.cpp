@@ -104,6 +104,7 @@ int bspk_checkpoint_restore(bspk_plan *p, const void *host_buf, int64_t bytes) {
         st += s.bytes;
     }
     p->step = hdr[1];
+    p->restart_step = p->step;
     return BSPK_OK;
 }
 

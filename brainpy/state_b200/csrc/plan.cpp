@@ -1336,6 +1336,11 @@ int run_tiled(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
     // this run comes on another stream
     if (p->side) BSPK_CUDA(cudaStreamWaitEvent(st, p->ev_side, 0));
     const int64_t run0 = p->step;
+    // a run from a restored checkpoint is likely to be repeated from there
+    // (Runner.simulate): then the prefill after its last launch draws the
+    // drive of that step again instead of the continuation's
+    const bool restart = p->restart_step == run0;
+    if (!restart) p->restart_step = -1;
     int64_t launches = 0;
     for (int64_t done = 0; done < n_steps; done += chunk) {
         const int64_t n = std::min<int64_t>(chunk, n_steps - done);
@@ -1377,8 +1382,10 @@ int run_tiled(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
             // the drive of the steps after this launch (the next launch, or as
             // many steps after the run), into the other buffer, once every
             // launch enqueued so far (the last reader of that buffer) is done
-            const int64_t next0 = a.step0 + n;
-            const int64_t nn = done + n < n_steps ? std::min<int64_t>(chunk, n_steps - done - n) : n;
+            const bool last = done + n >= n_steps;
+            const int64_t next0 = last && restart ? run0 : a.step0 + n;
+            const int64_t nn = !last ? std::min<int64_t>(chunk, n_steps - done - n)
+                                     : (restart ? std::min<int64_t>(chunk, n_steps) : n);
             if (next0 + nn < (int64_t(1) << 32)) {
                 BSPK_CUDA(cudaStreamWaitEvent(p->side, p->ev_main, 0));
                 LifArgs<Real> b = lif_args<Real>(p, nn);

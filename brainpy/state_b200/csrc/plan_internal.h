@@ -178,6 +178,10 @@ struct bspk_plan {
     cudaEvent_t ev_side = nullptr, ev_main = nullptr;
     int64_t pref_step0 = -1, pref_n = 0;  // prefilled steps [pref_step0, +pref_n)
     int pref_buf = 0;                     // in buffer 0 (d_tdrive) or 1 (d_tdrive2)
+    // the step a checkpoint restore rewound the plan to (-1: none since the
+    // last run that started elsewhere): a run from there is taken for a
+    // rerun, and the prefill after it targets that step again
+    int64_t restart_step = -1;
     bool drive_overlap = true;
     int rec_rep = 1;                      // copies of every spike record (tiled kernel)
     int poll_pause = 400;                 // ns before a window's first record poll
