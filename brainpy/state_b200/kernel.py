@@ -608,7 +608,11 @@ class Runner:
                 rec["spike"] = counts
             if "V_m" in o.recordables:
                 at = np.searchsorted(prog.rec_v, cols)
-                rec["V_m"] = v[k - 1::k][:, at]
+                vk = v[k - 1::k]
+                # an observer of every recorded column in order takes the
+                # trace as it is (no gather copy)
+                full = at.size == v.shape[1] and np.array_equal(at, np.arange(at.size))
+                rec["V_m"] = vk if full else vk[:, at]
             rec.times = (self.n + (np.arange(ns) + 1) * k) * prog.dt
             recs[o.name] = rec
         self.n += n_steps
