@@ -104,6 +104,8 @@ def lib():
             "bspk_step_count": (i64, [vp]),
             "bspk_plan_engine": (C.c_char_p, [vp]),
             "bspk_plan_set_windowed": (C.c_int, [vp, C.c_int]),
+            "bspk_plan_tune_tiled": (C.c_int, [vp, i64, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                               C.POINTER(dbl)]),
             "bspk_record_weights": (C.c_int, [vp, C.c_int, C.c_int]),
             "bspk_weight_trace_get": (C.c_int, [vp, C.c_int, C.POINTER(i64), vp]),
             "bspk_plan_ring_fraction_bits": (C.c_int, [vp, C.POINTER(C.c_int)]),
@@ -482,6 +484,15 @@ class Plan:
         check(self._L.bspk_plan_set_tiled_options(self._h, int(record_copies), int(poll_pause_ns),
                                                   int(bool(drive_overlap)),
                                                   int(drive_chunk_steps), int(record_stride_bytes)))
+
+    def tune_tiled(self, pilot_steps=500):
+        """Time pilot runs over CTA counts and poll pauses and keep the best
+        (the state is restored after every pilot); returns (grid,
+        poll_pause_ns, pilot_ms)."""
+        g, pz, ms = C.c_int(), C.c_int(), C.c_double()
+        check(self._L.bspk_plan_tune_tiled(self._h, int(pilot_steps), C.byref(g), C.byref(pz),
+                                           C.byref(ms)))
+        return g.value, pz.value, ms.value
 
     def tiled_options(self):
         v = [C.c_int() for _ in range(5)]

@@ -45,7 +45,7 @@ namespace {
 constexpr int kMaxCtas = 160;                 // G <= 160 CTAs, one per SM
 constexpr int kListCap = 2048;                // spikes gathered per window and CTA
 constexpr int kEdgeUnroll = 8;                // edge loads in flight per thread
-constexpr int kUpd = 10;                      // window steps whose inputs sit in registers
+constexpr int kUpd = 2;                       // window steps whose inputs sit in registers
 constexpr int kEdgeCap = 4096;                // flattened edges mapped per pass
 constexpr int kTagShift = 14;                 // word = tag (18 bits) << 14 | payload
 constexpr uint32_t kPayMask = (1u << kTagShift) - 1u;

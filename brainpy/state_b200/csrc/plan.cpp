@@ -967,6 +967,52 @@ int build_tiled(bspk_plan *p) {
     return BSPK_OK;
 }
 
+// Frees one of the plan's device buffers.
+template <typename T>
+void dfree(bspk_plan *p, T *&ptr) {
+    if (!ptr) return;
+    cudaFree(ptr);
+    void *raw = static_cast<void *>(ptr);
+    p->allocs.erase(std::remove(p->allocs.begin(), p->allocs.end(), raw), p->allocs.end());
+    ptr = nullptr;
+}
+
+// dynamic shared memory budget of the tiled kernel: 227 KB minus its ~34 KB
+// of static arrays
+constexpr size_t kTiledBudget = 190 * 1024;
+
+// Whether G CTAs can run the tiled kernel on this plan (tile per CTA within
+// the kernel's limits and its shared memory budget).
+bool tiled_fits(const bspk_plan *p, int G) {
+    if (G < 1 || G > 160 || G > p->sm_count) return false;
+    const int tile = (p->N + G - 1) / G;
+    return tile <= 256 &&
+           lif_tiled_smem(tile, p->L, p->tW, p->N, static_cast<int>(p->pops.size()),
+                          static_cast<int>(p->projs.size()), p->elt == 8, false,
+                          p->ports_tiled != 0) <= kTiledBudget;
+}
+
+// The tiled path's per-CTA structures rebuilt for G CTAs.
+int retile(bspk_plan *p, int G) {
+    dfree(p, p->d_tptr);
+    dfree(p, p->d_tedges);
+    dfree(p, p->d_tw);
+    dfree(p, p->d_twproj);
+    dfree(p, p->d_tlist);
+    dfree(p, p->d_tovf);
+    dfree(p, p->d_trec);
+    p->grid = G;
+    p->tile = (p->N + G - 1) / G;
+    const int rc = build_tiled(p);
+    if (rc) return rc;
+    p->smem_ptr = lif_tiled_smem(p->tile, p->L, p->tW, p->N, static_cast<int>(p->pops.size()),
+                                 static_cast<int>(p->projs.size()), p->elt == 8, true,
+                                 p->ports_tiled != 0) <= kTiledBudget;
+    p->cspk_valid = false;
+    p->pref_step0 = -1;
+    return BSPK_OK;
+}
+
 }  // namespace
 
 // Buffers of the windowed engine (see WinDev).
@@ -1038,7 +1084,7 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
         const int L = p->W + max_lag + 1;
         if (!(tile <= 256 && grid <= 160 &&
               lif_tiled_smem(tile, L, p->W, p->N, static_cast<int>(p->pops.size()),
-                             static_cast<int>(p->projs.size()), dbl, false, true) <= 190 * 1024))
+                             static_cast<int>(p->projs.size()), dbl, false, true) <= kTiledBudget))
             p->ports_tiled = 0;
     }
     const bool aeif = plan_per_step(p);  // per-step engine (RKF45, multisynapse, ports)
@@ -1228,9 +1274,7 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
     p->tW = p->W;
     p->tpipe = min_lag >= 2 * p->W ? 1 : 0;
     const int nproj_t = static_cast<int>(p->projs.size());
-    // dynamic shared memory budget of the tiled kernel: 227 KB minus its ~34 KB
-    // of static arrays
-    const size_t tiled_budget = 190 * 1024;
+    const size_t tiled_budget = kTiledBudget;
     const bool two = p->ports_tiled != 0;
     if (!exact && !aeif && !plastic && p->tile <= 256 && p->grid <= 160 &&
         lif_tiled_smem(p->tile, p->L, p->tW, p->N, npop, nproj_t, dbl, false, two) <= tiled_budget) {
@@ -1706,6 +1750,57 @@ int bspk_plan_set_tiled_options(bspk_plan *p, int record_copies, int poll_pause_
     p->drive_chunk = drive_chunk_steps;
     p->rec_stride = record_stride_bytes / 4;
     p->pref_step0 = -1;
+    return BSPK_OK;
+}
+
+int bspk_plan_tune_tiled(bspk_plan *p, int64_t pilot_steps, int *grid, int *poll_pause_ns,
+                         double *pilot_ms) {
+    if (!p || !p->uploaded || !p->tiled) return fail(BSPK_ERR_STATE, "tuning needs an uploaded plan on the tiled path");
+    if (pilot_steps <= 0) return fail(BSPK_ERR_ARG, "pilot_steps must be > 0");
+    BSPK_CUDA(cudaSetDevice(p->cfg.device));
+    int64_t bytes = 0;
+    int rc = bspk_checkpoint_size(p, &bytes);
+    if (rc) return rc;
+    std::vector<char> snap(static_cast<size_t>(bytes));
+    rc = bspk_checkpoint_save(p, snap.data(), bytes);
+    if (rc) return rc;
+    const int g0 = p->grid, pause0 = p->poll_pause;
+    std::vector<int> cands;
+    for (int G : {g0, g0 * 3 / 4, g0 / 2})
+        if (tiled_fits(p, G) && std::find(cands.begin(), cands.end(), G) == cands.end()) cands.push_back(G);
+    if (cands.empty()) cands.push_back(g0);
+    double best = 1e300;
+    int best_g = g0, best_pause = pause0;
+    for (int G : cands) {
+        if (G != p->grid) {
+            rc = retile(p, G);
+            if (rc) break;
+        }
+        for (int pause : {200, 400, 700}) {
+            p->poll_pause = pause;
+            rc = bspk_run(p, pilot_steps, nullptr);
+            double ms = 0.0;
+            if (!rc) rc = sync_and_check(p);
+            if (!rc) rc = bspk_last_kernel_time(p, &ms, nullptr);
+            if (!rc) rc = bspk_checkpoint_restore(p, snap.data(), bytes);
+            if (rc) break;
+            if (ms < best) {
+                best = ms;
+                best_g = G;
+                best_pause = pause;
+            }
+        }
+        if (rc) break;
+    }
+    // the best shape, and the state as it was
+    int rc2 = best_g != p->grid ? retile(p, best_g) : BSPK_OK;
+    p->poll_pause = rc ? pause0 : best_pause;
+    if (!rc2) rc2 = bspk_checkpoint_restore(p, snap.data(), bytes);
+    if (rc) return rc;
+    if (rc2) return rc2;
+    if (grid) *grid = best_g;
+    if (poll_pause_ns) *poll_pause_ns = best_pause;
+    if (pilot_ms) *pilot_ms = best;
     return BSPK_OK;
 }
 

@@ -274,6 +274,18 @@ int bspk_plan_set_tiled_options(bspk_plan *plan, int record_copies, int poll_pau
 int bspk_plan_get_tiled_options(bspk_plan *plan, int *record_copies, int *poll_pause_ns,
                                 int *drive_overlap, int *drive_chunk_steps,
                                 int *record_stride_bytes);
+/* Autotuner of the tiled path (no counterpart in the reference; the batch
+ * path's is bspk_batch_tune).  Times pilot runs of pilot_steps on the plan's
+ * own network for each CTA count G in {G0, 3/4 G0, 1/2 G0} (G0: the upload's
+ * choice, one CTA per SM for large networks) whose tile fits
+ * (a tile per CTA, rebuilt for each G) and each poll pause in {200, 400, 700}
+ * ns, with the plan's state saved before and restored after every pilot (the
+ * plan is left where it was, at the best shape).  *grid, *poll_pause_ns and
+ * *pilot_ms (the best pilot's device time) are optional.  Results of later
+ * runs do not depend on the shape.  BSPK_ERR_STATE unless the plan is
+ * uploaded and on the tiled path. */
+int bspk_plan_tune_tiled(bspk_plan *plan, int64_t pilot_steps, int *grid, int *poll_pause_ns,
+                         double *pilot_ms);
 
 /* Synchronise and copy out what the last bspk_run recorded.
  * spikes: (step, gid) pairs in no particular order, *n_out = count. */
