@@ -161,6 +161,11 @@ def run_ours(args):
     prog, p = headline_program(32, seed=D.replica_seed(1234, rank))
     pl = prog.plan
     N = p["NE"] + p["NI"]
+    # the tiled path's shape from pilot runs (state restored), before warm-up
+    tuned = None
+    if pl.engine == "tiled":
+        g, pz, pms = pl.tune_tiled(pilot_steps=1000)
+        tuned = {"grid": g, "poll_pause_ns": pz, "pilot_ms": round(pms, 3)}
     time_runs(pl, args.warmup, stream, flush)
     if world > 1:
         dist.barrier()
@@ -211,6 +216,7 @@ def run_ours(args):
                     f"fixed-point ring of 2^-{kbits} pA resolution (weights rounded once)",
         "data": "synthetic (seeded Brunel network, the reference kernel path's streams)",
         "config": CONFIG_HEADLINE(N, p, int(pl._deg.sum()), sim_ms, world),
+        "tiled_shape": tuned,
         "syn_events_per_s": round(syn_ev_s, 1), "drive_events_per_s": round(drive_ev_s, 1),
         "rate_hz": round(rate_hz / (sim_ms / 1000.0), 3),
         "cv_isi": cv_isi,
