@@ -161,12 +161,14 @@ def run_ours(args):
     prog, p = headline_program(32, seed=D.replica_seed(1234, rank))
     pl = prog.plan
     N = p["NE"] + p["NI"]
-    # the tiled path's shape from pilot runs (state restored), before warm-up
+    time_runs(pl, args.warmup, stream, flush)
+    # the tiled path's shape from pilot runs on the warmed-up network (its
+    # state restored after each pilot), then one more warm-up run
     tuned = None
     if pl.engine == "tiled":
-        g, pz, pms = pl.tune_tiled(pilot_steps=1000)
+        g, pz, pms = pl.tune_tiled(pilot_steps=2000)
         tuned = {"grid": g, "poll_pause_ns": pz, "pilot_ms": round(pms, 3)}
-    time_runs(pl, args.warmup, stream, flush)
+        time_runs(pl, 1, stream, flush)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()

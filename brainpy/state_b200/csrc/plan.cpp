@@ -1778,11 +1778,17 @@ int bspk_plan_tune_tiled(bspk_plan *p, int64_t pilot_steps, int *grid, int *poll
         }
         for (int pause : {200, 400, 700}) {
             p->poll_pause = pause;
-            rc = bspk_run(p, pilot_steps, nullptr);
-            double ms = 0.0;
-            if (!rc) rc = sync_and_check(p);
-            if (!rc) rc = bspk_last_kernel_time(p, &ms, nullptr);
-            if (!rc) rc = bspk_checkpoint_restore(p, snap.data(), bytes);
+            // the faster of two pilots (one pilot's noise is of the order of
+            // the differences between pauses)
+            double ms = 1e300;
+            for (int rep = 0; rep < 2 && !rc; ++rep) {
+                double t = 0.0;
+                rc = bspk_run(p, pilot_steps, nullptr);
+                if (!rc) rc = sync_and_check(p);
+                if (!rc) rc = bspk_last_kernel_time(p, &t, nullptr);
+                if (!rc) rc = bspk_checkpoint_restore(p, snap.data(), bytes);
+                ms = std::min(ms, t);
+            }
             if (rc) break;
             if (ms < best) {
                 best = ms;

@@ -279,7 +279,8 @@ int bspk_plan_get_tiled_options(bspk_plan *plan, int *record_copies, int *poll_p
  * own network for each CTA count G in {G0, 3/4 G0, 1/2 G0} (G0: the upload's
  * choice, one CTA per SM for large networks) whose tile fits
  * (a tile per CTA, rebuilt for each G) and each poll pause in {200, 400, 700}
- * ns, with the plan's state saved before and restored after every pilot (the
+ * ns (the faster of two pilots each), with the plan's state saved before and
+ * restored after every pilot (the
  * plan is left where it was, at the best shape).  *grid, *poll_pause_ns and
  * *pilot_ms (the best pilot's device time) are optional.  Results of later
  * runs do not depend on the shape.  BSPK_ERR_STATE unless the plan is
