@@ -147,6 +147,7 @@ def lib():
             "bspk_adjoint_ctas_per_trial": (C.c_int, [vp]),
             "bspk_adjoint_set_contraction": (C.c_int, [vp, C.c_int]),
             "bspk_adjoint_contraction": (C.c_int, [vp]),
+            "bspk_adjoint_status": (C.c_int, [vp]),
             "bspk_adjoint_forward": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
             "bspk_adjoint_backward": (C.c_int, [vp, vp, vp, vp]),
             "bspk_xla_adjoint_forward": (None, [vp, vp, C.c_char_p, C.c_size_t]),

@@ -104,6 +104,11 @@ class LifAdjoint:
                                                  C.c_void_p(dw_in.data_ptr()), C.c_void_p(st)))
         return dw, dw_in
 
+    def status(self):
+        """Synchronise and raise if a bounded device wait of the gradient
+        contraction ran out since the last check."""
+        _lib.check(self._L.bspk_adjoint_status(self._h))
+
 
 def _function():
     import torch

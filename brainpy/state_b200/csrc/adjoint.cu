@@ -26,6 +26,7 @@
 // Per-trial gradient buffers are summed over trials in trial order by a
 // final kernel, so the result does not depend on scheduling.
 #include <cooperative_groups.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -36,6 +37,7 @@
 
 #include "../../../include/bspk.h"
 #include "plan_internal.h"
+#include "umma.h"
 
 namespace bspk {
 
@@ -485,85 +487,9 @@ __global__ void k_adj_reduce_in(const Real *part, int N, int NI, int B, Real *ou
     }
 }
 
-// Weight-gradient contraction (FP32 plans): C = A^T B over the rows r = (t, b)
-// shared by two row-major operands, A [K][M] (the input adjoints gD) and
-// B [K][Nc] (the shifted spikes gS, or the input counts as uint8), C [M][Nc].
-// A 256-thread CTA computes a 128 x 128 tile of C, each thread an 8 x 8
-// block (two 4-row by two 4-column quarters, so its shared-memory reads are
-// conflict-free 16-byte loads), over the rows [z kc, (z + 1) kc), double
-// buffering 8-row slices of both operands; it writes its partial sum to
-// part[z][M][Nc].  The partials are added in z order afterwards, so the
-// result does not depend on scheduling.
-constexpr int kGBM = 128, kGBN = 128, kGBK = 8;
-template <typename TB>
-__global__ void __launch_bounds__(256) k_gemm_tn(const float *A, const TB *Bm, int M, int Nc, int64_t K,
-                                                 int64_t kc, float *part) {
-    __shared__ __align__(16) float As[2][kGBK][kGBM];
-    __shared__ __align__(16) float Bs[2][kGBK][kGBN];
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    const int m0 = blockIdx.y * kGBM, n0 = blockIdx.x * kGBN;
-    const int64_t k0 = static_cast<int64_t>(blockIdx.z) * kc;
-    const int64_t k1 = k0 + kc < K ? k0 + kc : K;
-    // loader: k-row lr of the slice, columns lc .. lc + 3 of both tiles
-    const int lr = tid >> 5, lc = (tid & 31) * 4;
-    float ra[4], rb[4];
-    auto load = [&](int64_t kk) {
-        const int64_t r = kk + lr;
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int m = m0 + lc + u, n = n0 + lc + u;
-            ra[u] = (r < k1 && m < M) ? A[r * M + m] : 0.f;
-            rb[u] = (r < k1 && n < Nc) ? static_cast<float>(Bm[r * Nc + n]) : 0.f;
-        }
-    };
-    auto store = [&](int buf) {
-        *reinterpret_cast<float4 *>(&As[buf][lr][lc]) = make_float4(ra[0], ra[1], ra[2], ra[3]);
-        *reinterpret_cast<float4 *>(&Bs[buf][lr][lc]) = make_float4(rb[0], rb[1], rb[2], rb[3]);
-    };
-    float acc[8][8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
-    if (k0 < k1) {
-        load(k0);
-        store(0);
-    }
-    __syncthreads();
-    int buf = 0;
-    for (int64_t kk = k0; kk < k1; kk += kGBK) {
-        const bool more = kk + kGBK < k1;
-        if (more) load(kk + kGBK);  // in flight during this slice's products
-#pragma unroll
-        for (int k = 0; k < kGBK; ++k) {
-            const float4 a0 = *reinterpret_cast<const float4 *>(&As[buf][k][ty * 4]);
-            const float4 a1 = *reinterpret_cast<const float4 *>(&As[buf][k][64 + ty * 4]);
-            const float4 b0 = *reinterpret_cast<const float4 *>(&Bs[buf][k][tx * 4]);
-            const float4 b1 = *reinterpret_cast<const float4 *>(&Bs[buf][k][64 + tx * 4]);
-            const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-            const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-#pragma unroll
-                for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
-        }
-        if (more) store(buf ^ 1);
-        __syncthreads();
-        buf ^= 1;
-    }
-    float *P = part + static_cast<size_t>(blockIdx.z) * M * Nc;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const int m = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
-        if (m >= M) continue;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int n = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + j - 4);
-            if (n < Nc) P[static_cast<size_t>(m) * Nc + n] = acc[i][j];
-        }
-    }
-}
-
+// The FP32 weight-gradient contractions run on the tensor cores
+// (umma_gemm.cu); these two kernels add their split-K partial sums in a fixed
+// order.
 // out[e] = sum over z in order of part[z][post(e)][pre(e)], the caller's CSR edges
 __global__ void k_gemm_gather(const float *part, int S, int Nc, size_t MN, const int32_t *e_post,
                               const int32_t *e_pre, int64_t nnz, float *out) {
@@ -644,6 +570,8 @@ struct bspk_adjoint {
     void *gD = nullptr, *gS = nullptr;   // [n_steps][batch][n]
     float *gpart = nullptr;              // split-K partial sums
     int32_t *e_post = nullptr, *e_pre = nullptr;  // the CSR edges' (post, pre)
+    __nv_bfloat16 *ux = nullptr, *uy = nullptr;   // packed bf16 operand parts
+    int *d_err = nullptr;                         // device error flag (bounded waits)
 };
 
 extern "C" int bspk_adjoint_sizes(const bspk_adjoint *adj, int64_t *nnz, int64_t *n_w_in,
@@ -767,34 +695,27 @@ int run_forward(bspk_adjoint *h, const void *w, const void *w_in, double *loss, 
     return BSPK_OK;
 }
 
-// Row splits of a contraction with an M x Nc result: enough CTAs for two per
-// SM, at most 64 partials, and at least 64 rows per split.
-int gemm_splits(int sms, int M, int Nc, int64_t K) {
-    const int64_t tiles = static_cast<int64_t>((M + kGBM - 1) / kGBM) * ((Nc + kGBN - 1) / kGBN);
-    int64_t S = (2 * static_cast<int64_t>(std::max(sms, 1)) + tiles - 1) / tiles;
-    S = std::min<int64_t>(S, std::max<int64_t>(1, K / 64));
-    return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(S, 64)));
-}
-
-// dL/dw and dL/dw_in of an FP32 handle by contraction over (step, trial)
+// dL/dw and dL/dw_in of an FP32 handle by contraction over (step, trial) on
+// the tensor cores: the adjoints split into 3 bf16 parts, the spikes into 1
+// (0/1 values, exact) or 2 (the relaxed forward's surrogate values), the
+// input counts into 1 (exact)
 int run_contractions(bspk_adjoint *h, float *dw, float *dw_in, cudaStream_t st) {
     const bspk_adjoint_config &c = h->cfg;
     const int N = c.n, NI = c.n_in;
     const int64_t K = static_cast<int64_t>(c.n_steps) * c.batch;
-    const float *D = static_cast<const float *>(h->gD);
+    BSPK_CUDA(umma_pack_f32(static_cast<const float *>(h->gD), N, K, 3, h->ux, st));
     if (h->nnz > 0) {
-        const int S = gemm_splits(h->sms, N, N, K);
-        const int64_t kc = (K + S - 1) / S;
-        k_gemm_tn<float><<<dim3((N + kGBN - 1) / kGBN, (N + kGBM - 1) / kGBM, S), 256, 0, st>>>(
-            D, static_cast<const float *>(h->gS), N, N, K, kc, h->gpart);
+        const int ny = c.relaxed ? 2 : 1;
+        BSPK_CUDA(umma_pack_f32(static_cast<const float *>(h->gS), N, K, ny, h->uy, st));
+        const int S = umma_splits(h->sms, N, N, K);
+        BSPK_CUDA(umma_gemm(h->ux, N, h->uy, ny, N, K, S, h->gpart, h->d_err, st));
         k_gemm_gather<<<grid_of(h->nnz), 256, 0, st>>>(h->gpart, S, N, static_cast<size_t>(N) * N,
                                                        h->e_post, h->e_pre, h->nnz, dw);
     }
     if (NI > 0 && dw_in) {
-        const int S = gemm_splits(h->sms, N, NI, K);
-        const int64_t kc = (K + S - 1) / S;
-        k_gemm_tn<uint8_t><<<dim3((NI + kGBN - 1) / kGBN, (N + kGBM - 1) / kGBM, S), 256, 0, st>>>(
-            D, h->inputs, N, NI, K, kc, h->gpart);
+        BSPK_CUDA(umma_pack_u8(h->inputs, NI, K, h->uy, st));
+        const int S = umma_splits(h->sms, N, NI, K);
+        BSPK_CUDA(umma_gemm(h->ux, N, h->uy, 1, NI, K, S, h->gpart, h->d_err, st));
         const size_t n = static_cast<size_t>(N) * NI;
         k_gemm_sum<<<grid_of(static_cast<int64_t>(n)), 256, 0, st>>>(h->gpart, S, n, dw_in);
     }
@@ -846,6 +767,19 @@ int bspk_adjoint_set_contraction(bspk_adjoint *h, int on) {
 }
 
 int bspk_adjoint_contraction(const bspk_adjoint *h) { return h ? h->gemm : 0; }
+
+int bspk_adjoint_status(bspk_adjoint *h) {
+    if (!h) return fail(BSPK_ERR_ARG, "null handle");
+    BSPK_CUDA(cudaSetDevice(h->cfg.device));
+    BSPK_CUDA(cudaDeviceSynchronize());
+    int e = 0;
+    BSPK_CUDA(cudaMemcpy(&e, h->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        BSPK_CUDA(cudaMemset(h->d_err, 0, sizeof(int)));
+        return fail(BSPK_ERR_TIMEOUT, "a bounded wait of the gradient contraction ran out");
+    }
+    return BSPK_OK;
+}
 
 int bspk_adjoint_create(const bspk_adjoint_config *cfg, const int64_t *row_ptr, const int32_t *col,
                         int64_t nnz, bspk_adjoint **out) {
@@ -952,6 +886,7 @@ int bspk_adjoint_create(const bspk_adjoint_config *cfg, const int64_t *row_ptr, 
         {reinterpret_cast<void **>(&h->loss_b), 8 * B},
         {reinterpret_cast<void **>(&h->loss_dev), 8},
         {reinterpret_cast<void **>(&h->nspk), 8},
+        {reinterpret_cast<void **>(&h->d_err), 4},
     };
     for (const Buf &bf : bufs) {
         rc = aalloc(h, bf.p, bf.bytes);
@@ -969,15 +904,19 @@ int bspk_adjoint_create(const bspk_adjoint_config *cfg, const int64_t *row_ptr, 
     // 16 GB (otherwise the read-modify-write mode only)
     if (c.precision == 32) {
         const int64_t Kr = static_cast<int64_t>(c.n_steps) * c.batch;
-        const size_t S1 = gemm_splits(h->sms, N, N, Kr), S2 = gemm_splits(h->sms, N, c.n_in, Kr);
+        const size_t S1 = umma_splits(h->sms, N, N, Kr), S2 = umma_splits(h->sms, N, c.n_in, Kr);
         const size_t part = std::max(S1 * NN * NN, S2 * NN * static_cast<size_t>(c.n_in));
         const size_t op = 4 * static_cast<size_t>(Kr) * NN;
         const size_t ne = static_cast<size_t>(std::max<int64_t>(nnz, 1));
-        if (2 * op + 4 * part + 8 * ne <= (size_t(16) << 30)) {
-            void *p[5] = {};
-            const size_t by[5] = {op, op, 4 * std::max<size_t>(part, 1), 4 * ne, 4 * ne};
+        // bf16 parts of the operands: 3 of the adjoints, 2 of the spikes (or
+        // 1 of the input counts)
+        const size_t xb = 2 * 3 * umma_part_elems(N, Kr);
+        const size_t yb = 2 * std::max(2 * umma_part_elems(N, Kr), umma_part_elems(std::max(c.n_in, 1), Kr));
+        if (2 * op + 4 * part + 8 * ne + xb + yb <= (size_t(16) << 30)) {
+            void *p[7] = {};
+            const size_t by[7] = {op, op, 4 * std::max<size_t>(part, 1), 4 * ne, 4 * ne, xb, yb};
             bool ok = true;
-            for (int k = 0; k < 5 && ok; ++k) {
+            for (int k = 0; k < 7 && ok; ++k) {
                 ok = cudaMalloc(&p[k], by[k]) == cudaSuccess;
                 if (ok) h->allocs.push_back(p[k]);
             }
@@ -994,12 +933,15 @@ int bspk_adjoint_create(const bspk_adjoint_config *cfg, const int64_t *row_ptr, 
                 h->gpart = static_cast<float *>(p[2]);
                 h->e_post = static_cast<int32_t *>(p[3]);
                 h->e_pre = static_cast<int32_t *>(p[4]);
+                h->ux = static_cast<__nv_bfloat16 *>(p[5]);
+                h->uy = static_cast<__nv_bfloat16 *>(p[6]);
                 h->can_gemm = h->gemm = 1;
             } else {
                 cudaGetLastError();  // an allocation that failed leaves the mode off
             }
         }
     }
+    if (cudaMemset(h->d_err, 0, sizeof(int)) != cudaSuccess) return bail(fail(BSPK_ERR_CUDA, "memset failed"));
     rc = h->elt == 8 ? set_smem<double>(h) : set_smem<float>(h);
     if (rc) return bail(rc);
     if (cudaDeviceSynchronize() != cudaSuccess) return bail(fail(BSPK_ERR_CUDA, "upload failed"));

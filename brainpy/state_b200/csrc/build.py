@@ -35,10 +35,11 @@ SOURCES = {
     "checkpoint.cpp": [],
     "xla_ffi.cpp": [],
     "jax_rng.cpp": [],
+    "umma_gemm.cu": [],
 }
 HEADERS = ["common.cuh", "device_types.h", "lif_args.h", "aeif_args.h", "stdp_args.h",
            "host_rng.h", "batch_args.h", "plan_internal.h", "conn_gen.h", "conn_gen.cuh",
-           "coef_cast.h", "jax_rng.h"]
+           "coef_cast.h", "jax_rng.h", "umma.h"]
 
 
 def _mtime(p):

@@ -458,14 +458,20 @@ int bspk_adjoint_sizes(const bspk_adjoint *adj, int64_t *nnz, int64_t *n_w_in, i
 /* How an FP32 handle forms the weight gradients.  1 (the default when the
  * buffers fit): the backward stores the input adjoint of every (step, trial,
  * neuron) and the recompute the previous step's spikes, and dL/dw, dL/dw_in
- * are dense contractions over (step, trial) followed by a gather of the
- * edges (partial sums added in a fixed order: deterministic).  0: per-trial
+ * are dense contractions over (step, trial) on the tensor cores
+ * (tcgen05.mma on bf16 parts that restate the FP32 operands, FP32
+ * accumulation) followed by a gather of the edges (partial sums added in a
+ * fixed order: deterministic).  0: per-trial
  * read-modify-writes in time order, summed over trials in trial order (the
  * only mode of FP64 handles, bit-exact with the float64 restatement).
  * Setting 1 on an FP64 handle, or on one whose buffers could not be
  * allocated, is BSPK_ERR_UNSUPPORTED. */
 int bspk_adjoint_set_contraction(bspk_adjoint *adj, int on);
 int bspk_adjoint_contraction(const bspk_adjoint *adj);
+/* Synchronise the device and report (then clear) the handle's device error
+ * flag: BSPK_ERR_TIMEOUT if a bounded wait of the tensor-core contraction
+ * ran out since the last call. */
+int bspk_adjoint_status(bspk_adjoint *adj);
 
 /* No-allocation entry point (no counterpart in the reference).  For callers
  * that cannot call cudaMalloc -- code running inside another framework's

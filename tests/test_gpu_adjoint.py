@@ -49,6 +49,7 @@ def _gpu(T, precision=64, ckpt=50, split=None, contraction=None):
     nsp = torch.zeros((), dtype=torch.int64, device="cuda")
     loss = adj.forward(w, wi, inp, tg, n_spikes=nsp)
     dw, dwi = adj.backward()
+    adj.status()
     torch.cuda.synchronize()
     out = (float(loss), dw.double().cpu().numpy(), dwi.double().cpu().numpy(), int(nsp))
     adj.close()
