@@ -23,8 +23,9 @@
 // part) into shared memory with cp.async, one thread issues the chunk's
 // tcgen05.mma (M = 128, N = 128, K = 16, kind::f16 with bf16 inputs) into a
 // 128-column FP32 accumulator in tensor memory and commits them to the
-// buffer's mbarrier; two buffers let the next chunk's copies overlap the
-// MMAs.  Each warp then reads its 32 accumulator lanes with tcgen05.ld and
+// stage's mbarrier; with three stages (two when the relaxed spikes' second
+// part does not leave room) the copies of the next two chunks are in flight
+// while a chunk's MMAs run.  Each warp then reads its 32 accumulator lanes with tcgen05.ld and
 // writes the tile's partial sums.  Every mbarrier wait is bounded: past the
 // limit the kernel raises the error flag, stops issuing, waits (bounded) for
 // what it issued, frees its tensor memory and returns.
@@ -45,6 +46,7 @@ constexpr int kUT = 128;            // output tile rows / columns
 constexpr int kUK = 64;             // K chunk (elements)
 constexpr int kUTileBytes = kUT * kUK * 2;  // one part's tile: 16 KB
 constexpr int kUXParts = 3;
+constexpr int kUMaxStages = 3;       // shared-memory stages of the K loop
 constexpr uint32_t kUTmemCols = 128;
 constexpr long long kUSpinLimit = 1ll << 26;
 
@@ -154,13 +156,14 @@ struct UmmaArgs {
     int M, N;                    // valid output rows and columns
     int64_t nkc;                 // K chunks of the packing
     int64_t kc_split;            // K chunks per row split
+    int stages;                  // shared-memory stages (2 or 3)
     float *part;                 // [splits][M][N] partial sums
     int *err;
 };
 
 __global__ void __launch_bounds__(128, 1) k_umma_gemm(const UmmaArgs a) {
     extern __shared__ __align__(1024) unsigned char u_smem[];
-    __shared__ __align__(8) unsigned long long s_bar[2];
+    __shared__ __align__(8) unsigned long long s_bar[kUMaxStages];
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -178,8 +181,8 @@ __global__ void __launch_bounds__(128, 1) k_umma_gemm(const UmmaArgs a) {
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar[0])) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar[1])) : "memory");
+        for (int b = 0; b < kUMaxStages; ++b)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar[b])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_fail = 0;
     }
@@ -187,17 +190,13 @@ __global__ void __launch_bounds__(128, 1) k_umma_gemm(const UmmaArgs a) {
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
-    uint32_t parity[2] = {0u, 0u};
-    bool pending[2] = {false, false};
+    // NB stages: the copies of chunk c + NB - 1 are issued while the MMAs of
+    // chunk c run (a stage is refilled once the MMAs that read it are done)
+    const int NB = a.stages;
+    uint32_t parity[kUMaxStages] = {0u, 0u, 0u};
+    bool pending[kUMaxStages] = {false, false, false};
     const size_t tile_elems = static_cast<size_t>(kUT) * kUK;
-    for (int64_t c = c0; c < c1; ++c) {
-        const int b = static_cast<int>((c - c0) & 1);
-        // the MMAs that last read buffer b are complete before it is refilled
-        if (pending[b]) {
-            if (!mbar_wait(smem_u32(&s_bar[b]), parity[b])) s_fail = 1;
-            parity[b] ^= 1u;
-            pending[b] = false;
-        }
+    auto issue = [&](int64_t c, int b) {
         unsigned char *buf = base + static_cast<size_t>(b) * nparts * kUTileBytes;
         for (int p = 0; p < nparts; ++p) {
             const __nv_bfloat16 *src =
@@ -207,12 +206,32 @@ __global__ void __launch_bounds__(128, 1) k_umma_gemm(const UmmaArgs a) {
             for (int q = tid; q < kUTileBytes / 16; q += blockDim.x)
                 __pipeline_memcpy_async(dst + q * 16, reinterpret_cast<const unsigned char *>(src) + q * 16, 16);
         }
+    };
+    for (int st = 0; st < NB - 1; ++st) {
+        if (c0 + st < c1) issue(c0 + st, st);
         __pipeline_commit();
-        __pipeline_wait_prior(0);
+    }
+    for (int64_t c = c0; c < c1; ++c) {
+        const int i = static_cast<int>(c - c0);
+        const int b = i % NB;
+        const int64_t cn = c + NB - 1;
+        const int bn = (i + NB - 1) % NB;
+        if (cn < c1) {
+            // the MMAs that last read stage bn are complete before it is refilled
+            if (pending[bn]) {
+                if (!mbar_wait(smem_u32(&s_bar[bn]), parity[bn])) s_fail = 1;
+                parity[bn] ^= 1u;
+                pending[bn] = false;
+            }
+            issue(cn, bn);
+        }
+        __pipeline_commit();
+        __pipeline_wait_prior(NB - 1);
         // the copies (generic proxy) become visible to the tensor cores
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (s_fail) break;
+        unsigned char *buf = base + static_cast<size_t>(b) * nparts * kUTileBytes;
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t xb = smem_u32(buf), yb = xb + kUXParts * kUTileBytes;
@@ -233,9 +252,10 @@ __global__ void __launch_bounds__(128, 1) k_umma_gemm(const UmmaArgs a) {
         }
         pending[b] = true;
     }
+    __pipeline_wait_prior(0);  // no copy left in flight
     // the last MMAs (a second bounded wait after a failure, before the
     // accumulator's memory is released)
-    for (int b = 0; b < 2; ++b)
+    for (int b = 0; b < NB; ++b)
         if (pending[b] && !mbar_wait(smem_u32(&s_bar[b]), parity[b])) s_fail = 1;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     __syncthreads();
@@ -318,7 +338,9 @@ cudaError_t umma_gemm(const __nv_bfloat16 *x, int M, const __nv_bfloat16 *y, int
     a.kc_split = (a.nkc + splits - 1) / splits;
     a.part = part;
     a.err = err;
-    const int smem = 2 * (kUXParts + ny) * kUTileBytes + 1024;
+    // three stages when they fit in the 227 KB of a CTA, else two
+    a.stages = 3 * (kUXParts + ny) * kUTileBytes + 1024 <= 227 * 1024 ? 3 : 2;
+    const int smem = a.stages * (kUXParts + ny) * kUTileBytes + 1024;
     cudaError_t e = cudaFuncSetAttribute(k_umma_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     const dim3 grid(static_cast<unsigned>((N + kUT - 1) / kUT), static_cast<unsigned>((M + kUT - 1) / kUT),
