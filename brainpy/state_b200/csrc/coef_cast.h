@@ -20,6 +20,8 @@ PopCoef<Real> cast_coef(const PopCoef<double> &d) {
         c.msP21[k] = static_cast<Real>(d.msP21[k]);
     }
     c.inv_Delta_T = d.inv_Delta_T;
+    c.inv_Delta_T_hi = static_cast<float>(d.inv_Delta_T);
+    c.inv_Delta_T_lo = static_cast<float>(d.inv_Delta_T - static_cast<double>(c.inv_Delta_T_hi));
     c.inv_atol = d.inv_atol;
     c.nrec = d.nrec;
     c.ref_count = d.ref_count;

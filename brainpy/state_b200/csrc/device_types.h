@@ -63,6 +63,9 @@ struct PopCoef {
     // term and the error norm
     Real inv_C_m, inv_tau_syn_ex, inv_tau_syn_in, inv_tau_w;
     double inv_Delta_T, inv_atol;
+    // 1 / Delta_T as an unevaluated FP32 sum hi + lo (|lo| <= ulp(hi) / 2):
+    // an FP32 state forms the exponent d / Delta_T to FP64 accuracy in FP32
+    float inv_Delta_T_hi, inv_Delta_T_lo;
     // iaf_psc_exp_multisynapse: per-receptor decay and membrane coupling
     // (eP22 / eP20 hold the membrane propagators)
     Real msP11[4], msP21[4];

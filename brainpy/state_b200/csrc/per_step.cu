@@ -62,11 +62,20 @@ __device__ constexpr double kA[6][5] = {
 __device__ constexpr double kB[6] = {16.0 / 135, 0.0, 6656.0 / 12825, 28561.0 / 56430, -9.0 / 50, 2.0 / 55};
 __device__ constexpr double kBhat[6] = {25.0 / 216, 0.0, 1408.0 / 2565, 2197.0 / 4104, -1.0 / 5, 0.0};
 
-// Vector field (_nest_neuron/aeif_cond_alpha.py:554-592).  The exponential
-// spike current is evaluated in FP64 from 2 Delta_T below V_th upward whatever
-// the state precision (the spike-initiation zone, where the term grows without
-// bound); below that, an FP32 state takes it in FP32.
-constexpr double kExpFp64Above = -2.0;
+// Vector field (_nest_neuron/aeif_cond_alpha.py:554-592).
+//
+// The exponential spike current g_L Delta_T exp((V - V_th) / Delta_T) in an
+// FP64 state is FP64 throughout.  In an FP32 state it is FP32 arithmetic to
+// the accuracy of FP32 rounding: the exponent d / Delta_T is carried as the
+// unevaluated sum arg + lo (arg = d * hi rounded, lo = the product's rounding
+// error plus d * lo(1 / Delta_T), both exact to a few ulp of lo), and
+// exp(arg + lo) = expf(arg) (1 + lo) to O(lo^2) (|lo| < 1e-5, so lo^2 is far
+// below FP32's 6e-8).  expf's own error is at most 2 ulp, so the current is
+// within about 3 ulp of the correctly rounded value at every V, including the
+// spike-initiation zone where the term grows without bound and the adaptive
+// step control spends most of a spiking neuron's trial steps.  The exponent is
+// clamped to [-500, 88] (expf(88) is finite; a zero Delta_T then still gives a
+// zero term).
 template <typename Real>
 __device__ __forceinline__ void aeif_vf(const PopCoef<Real> &c, int r, Real i_stim, const Real *y,
                                         Real *dy) {
@@ -76,12 +85,13 @@ __device__ __forceinline__ void aeif_vf(const PopCoef<Real> &c, int r, Real i_st
     const Real i_ex = y[2] * (v_eff - c.E_ex);
     const Real i_in = y[4] * (v_eff - c.E_in);
     Real i_spike;
-    const Real argR = (v_eff - c.V_th) * static_cast<Real>(c.inv_Delta_T);
-    if (sizeof(Real) == 4 && argR < Real(kExpFp64Above)) {
-        // FP32 state, more than 2 Delta_T below V_th: the term is below
-        // g_L Delta_T e^-2 (8 pA at the NEST defaults) and expf's 2-ulp error
-        // is under the rounding of the FP32 current sum
-        i_spike = c.g_L * c.Delta_T * expf(argR < Real(-500) ? Real(-500) : argR);
+    if constexpr (sizeof(Real) == 4) {
+        const float d = v_eff - c.V_th;
+        const float arg = d * c.inv_Delta_T_hi;
+        const float lo = fmaf(d, c.inv_Delta_T_hi, -arg) + d * c.inv_Delta_T_lo;
+        const float ac = arg < -500.0f ? -500.0f : (arg > 88.0f ? 88.0f : arg);
+        const float e = expf(ac);
+        i_spike = (c.g_L * c.Delta_T) * fmaf(e, lo, e);
     } else {
         double arg = static_cast<double>(v_eff - c.V_th) * c.inv_Delta_T;
         arg = arg < -500.0 ? -500.0 : (arg > 500.0 ? 500.0 : arg);
