@@ -490,7 +490,7 @@ def adex_numbers(args):
     par = adex_parity()
     return {"workload": "16000E+4000I aeif_cond_alpha, in-degree 1600 E + 400 I, lognormal "
                         "weights (ln 1 nS, 0.5), E->E stdp_synapse (25.6 M edges), 5 kHz drive "
-                        "of 6 nS, RKF45 tol 1e-6, 2000 ms, FP32 stages / FP64 error control",
+                        "of 6 nS, RKF45 tol 1e-6, 2000 ms, FP32 state and stages / FP64 error control",
             "parity": par,
             "ms_per_simulated_s": round(kms / 2.0, 2),
             "rtf": round(2000.0 / kms, 4),

@@ -78,7 +78,10 @@ struct WinDev {
     StdpDev s;
     int W, cap;            // window; arrivals held per (step, post)
     double *kp;            // [W][n_pre] pre trace at step n0 + k without that step's arrival
-    long long *upto;       // [edges] last step whose facilitation reached the edge
+    uint32_t *amask;       // [n_pre] window steps at which each pre's spikes arrive
+                           // (bit k: step n0 + k); an edge's arrivals in the window
+                           // are exactly its pre's bits, so the last step that
+                           // brought it up to date follows from them
     WinArrival *arr;       // [W][cap][n_post] arrivals at n0 + k
     int *cnt;              // [W][n_post] arrivals per (step, post), cleared by their reader
     uint32_t *spk;         // spikes of the window: gid << 5 | step in window

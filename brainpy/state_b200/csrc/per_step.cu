@@ -42,6 +42,8 @@ __device__ __forceinline__ int find_pop_t(const PopCoef<Real> *c, int npop, int 
 // kChunkEdges = 32 kEdgeU per warp-sized item.
 constexpr int kEdgeU = 8;
 constexpr int kChunkEdges = 32 * kEdgeU;
+// plastic arrivals of one window step taken together by a neuron thread
+constexpr int kWinArrU = 8;
 
 __device__ __forceinline__ bool fired(const uint64_t *hist, int gid, int64_t m) {
     if (m < 0) return false;
@@ -98,8 +100,16 @@ __device__ __forceinline__ void aeif_vf(const PopCoef<Real> &c, int r, Real i_st
         i_spike = static_cast<Real>(static_cast<double>(c.g_L) * static_cast<double>(c.Delta_T) *
                                     exp(arg));
     }
-    const Real dV = (-c.g_L * (v_eff - c.E_L) + i_spike - i_ex - i_in - y[5] + c.I_e + i_stim) *
-                    c.inv_C_m;
+    Real dV;
+    if constexpr (sizeof(Real) == 4) {
+        // FP32: the terms that do not wait for the exponential are summed
+        // while it is evaluated, and the spike current joins last
+        const Real rest = -c.g_L * (v_eff - c.E_L) - i_ex - i_in - y[5] + c.I_e + i_stim;
+        dV = (rest + i_spike) * c.inv_C_m;
+    } else {
+        // FP64: the reference's order of the sum
+        dV = (-c.g_L * (v_eff - c.E_L) + i_spike - i_ex - i_in - y[5] + c.I_e + i_stim) * c.inv_C_m;
+    }
     dy[0] = refr ? Real(0) : dV;
     dy[1] = -y[1] * c.inv_tau_syn_ex;
     dy[2] = y[1] - y[2] * c.inv_tau_syn_ex;
@@ -226,7 +236,7 @@ __device__ __forceinline__ void rk_substep(const PopCoef<Real> &c, RkState<Real,
             else iaf_cond_vf<Real, MODEL>(c, r, q.i_stim, yi, k[st]);
         }
         Real yh[NS];
-        double err = 0.0;
+        double ev[NS];
 #pragma unroll
         for (int i = 0; i < NS; ++i) {
             Real acc = Real(0), eacc = Real(0);
@@ -252,9 +262,19 @@ __device__ __forceinline__ void rk_substep(const PopCoef<Real> &c, RkState<Real,
                                   : fabs(static_cast<double>(yh[i]));
             // |err| / atol (rtol = 0); the 0 * |y| term carries a NaN or an
             // infinite state into the norm as the reference's scale does
-            const double e = fabs(static_cast<double>(ye)) * inv_atol + 0.0 * ay;
-            err = i == 0 ? e : ((err != err || e != e) ? NAN : (err > e ? err : e));
+            ev[i] = fabs(static_cast<double>(ye)) * inv_atol + 0.0 * ay;
         }
+        // the largest component (NaN if any is NaN), folded as a tree: the
+        // same value as the sequential fold in fewer dependent steps
+#pragma unroll
+        for (int span = 1; span < NS; span <<= 1) {
+#pragma unroll
+            for (int i = 0; i + span < NS; i += 2 * span) {
+                const double x = ev[i], y = ev[i + span];
+                ev[i] = (x != x || y != y) ? NAN : (x > y ? x : y);
+            }
+        }
+        double err = ev[0];
         if (err != err) err = INFINITY;
         const bool accept = (err <= 1.0) || (q.h <= kRkMinH);
         if (accept) {
@@ -295,7 +315,7 @@ __device__ __forceinline__ bool rk_end(const PopCoef<Real> &c, RkState<Real, MOD
     constexpr int NS = RkState<Real, MODEL>::NS;
     if (q.iters >= rk_max_iters<MODEL>() && q.t_loc < dt) atomicExch(err, BSPK_DEV_ERR_RKCAP);
     if (q.unstable) atomicExch(err, BSPK_DEV_ERR_UNSTABLE);
-    {
+    if (rk_iters) {
         // one atomic per group of converged lanes, not one per neuron
         const unsigned m = __activemask();
         const unsigned sum = __reduce_add_sync(m, static_cast<unsigned>(q.iters));
@@ -717,6 +737,7 @@ __global__ void k_win_pretrace(WinDev w, const uint64_t *hist, int64_t n0, int W
         am |= static_cast<uint32_t>(x) << k;
     }
     w.s.pre_trace[i] = tr;
+    w.amask[i] = am;
     if (am) {
         const int q = atomicAdd(&w.ctr[1], 1);
         w.pre_list[q] = static_cast<uint32_t>(i);
@@ -761,11 +782,80 @@ __global__ void __launch_bounds__(256) k_win_arrivals(WinDev w) {
     }
 }
 
+// The plastic arrivals of window step k at post j (na of them), each edge
+// brought up to date and stored: first the facilitations the post's spikes
+// still owe it (bits of emask up to k: the spike at n0 - 1 + b is facilitated
+// at n0 + b with K+ kp[b]; owed after fdone, the step of the edge's previous
+// arrival in this window, or n0 - 1 when it has none, since the window before
+// brought every edge there), then the depression with K- kminus; each new
+// weight joins acc.  The arrivals of one step are distinct edges, so they go
+// kWinArrU at a time: every load of a group is issued before its first store
+// (the group's chains overlap).
+template <typename Real>
+__device__ __forceinline__ void win_arrivals_apply(const WinDev &w, int j, int k, int na,
+                                                   uint64_t emask, double kminus, Real &acc) {
+    const int np = w.s.n_post;
+    const uint64_t kmask = emask & ((2ull << k) - 1ull);
+    const WinArrival *ar = w.arr + static_cast<size_t>(k) * w.cap * np + j;
+    for (int q0 = 0; q0 < na; q0 += kWinArrU) {
+        uint32_t ee[kWinArrU], pr[kWinArrU];
+#pragma unroll
+        for (int u = 0; u < kWinArrU; ++u) {
+            ee[u] = 0u;
+            pr[u] = 0u;
+            if (q0 + u < na) {
+                const WinArrival en = ar[static_cast<size_t>(q0 + u) * np];
+                ee[u] = en.e;
+                pr[u] = en.pre;
+            }
+        }
+        double wv[kWinArrU];
+        uint64_t due[kWinArrU];
+#pragma unroll
+        for (int u = 0; u < kWinArrU; ++u) {
+            wv[u] = 0.0;
+            due[u] = 0ull;
+            if (q0 + u < na) {
+                wv[u] = w.s.w[ee[u]];
+                // the edge's previous arrival in the window (its pre's last
+                // bit below k) brought it up to date at that step
+                const uint32_t prev = w.amask[pr[u]] & ((1u << k) - 1u);
+                const int lo = prev ? 32 - __clz(static_cast<int>(prev)) : 0;
+                due[u] = kmask & ~((1ull << lo) - 1ull);
+            }
+        }
+        // K+ of each edge's first due facilitation, before any store
+        double kp0[kWinArrU];
+#pragma unroll
+        for (int u = 0; u < kWinArrU; ++u) {
+            kp0[u] = 0.0;
+            if (due[u]) {
+                const int b = __ffsll(static_cast<long long>(due[u])) - 1;
+                kp0[u] = w.kp[static_cast<size_t>(b) * w.s.n_pre + pr[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kWinArrU; ++u) {
+            if (q0 + u >= na) continue;
+            double x = wv[u];
+            uint64_t d = due[u];
+            if (d) {
+                x = stdp_facilitate(w.s, x, kp0[u]);
+                for (d &= d - 1ull; d; d &= d - 1ull) {
+                    const int b = __ffsll(static_cast<long long>(d)) - 1;
+                    x = stdp_facilitate(w.s, x, w.kp[static_cast<size_t>(b) * w.s.n_pre + pr[u]]);
+                }
+            }
+            x = stdp_depress(w.s, x, kminus);
+            w.s.w[ee[u]] = x;
+            acc += static_cast<Real>(x);
+        }
+    }
+}
+
 // Inputs of window step n = n0 + k of neuron g: the ring slot, then (a post
 // of the plastic projection) the post trace of step n and the arrivals of
-// step n -- each edge first receives the facilitations the post's spikes
-// still owe it, then the depression, and its new weight joins the input --
-// then the drives.
+// step n (win_arrivals_apply), then the drives.
 template <typename Real>
 __device__ __forceinline__ void win_inputs(const StepArgs<Real> &a, const WinDev &w, int g, int p,
                                            const PopCoef<Real> &c, int64_t n0, int k, bool pp,
@@ -786,29 +876,10 @@ __device__ __forceinline__ void win_inputs(const StepArgs<Real> &a, const WinDev
         int na = w.cnt[ci];
         w.cnt[ci] = 0;  // cleared for the next window
         if (na > w.cap) na = w.cap;
-        // the post's spikes at n0 - 1 + b (bit b), facilitated at n0 + b
-        // with K+ kp[b]
+        // the post's spikes at n0 - 1 + b (bit b)
         const uint64_t emask = (static_cast<uint64_t>(spmask) << 1) | prevbit;
         const int rec = w.s.receptor < a.R ? w.s.receptor : 0;
-        for (int q = 0; q < na; ++q) {
-            const WinArrival &en = w.arr[(static_cast<size_t>(k) * w.cap + q) * np + j];
-            const int64_t e = en.e;
-            const int pre = static_cast<int>(en.pre);
-            double wv = w.s.w[e];
-            // facilitations at steps f in (fdone, n]: fdone is the edge's last
-            // update, or n0 - 1 (the window before brought every edge there)
-            const long long u = w.upto[e];
-            const int lo = u >= n0 - 1 ? static_cast<int>(u - n0 + 1) : 0;
-            uint64_t due = emask & ((2ull << k) - 1ull) & ~((1ull << lo) - 1ull);
-            for (; due; due &= due - 1ull) {
-                const int b = __ffsll(static_cast<long long>(due)) - 1;
-                wv = stdp_facilitate(w.s, wv, w.kp[static_cast<size_t>(b) * w.s.n_pre + pre]);
-            }
-            wv = stdp_depress(w.s, wv, kminus);
-            w.s.w[e] = wv;
-            w.upto[e] = n;
-            in[rec] += static_cast<Real>(wv);
-        }
+        win_arrivals_apply<Real>(w, j, k, na, emask, kminus, in[rec]);
     }
     step_drives<Real>(a, g, p, c, n, in);
 }
@@ -850,8 +921,8 @@ __device__ __forceinline__ void win_close(const StepArgs<Real> &a, const WinDev 
     }
 }
 
-// Neuron pass of a window for the exact-propagator models (and any model):
-// one thread per neuron, the window's steps in order.
+// Neuron pass of a window: one thread per neuron, the window's steps in order
+// with all lanes of a warp at the same step (inputs, update, bookkeeping).
 template <typename Real, int MODEL>
 __global__ void __launch_bounds__(128) k_win_neuron(const StepArgs<Real> a, WinDev w, int64_t n0, int Wk,
                                                     double dt) {
@@ -930,10 +1001,10 @@ __global__ void __launch_bounds__(256) k_win_deliver(const StepArgs<Real> a, Win
 
 // The facilitations owed on all in-edges of the posts that fired at steps
 // n0 - 1 .. n0 + Wk - 2: for a spike at n0 - 1 + b, the facilitation at step
-// n0 + b (K+ kp[b]), unless the edge's last update (an arrival) already
-// covered it.  A spike of the window's last step is facilitated at the next
+// n0 + b (K+ kp[b]), unless an arrival of the edge at that step or later
+// already covered it.  A spike of the window's last step is facilitated at the next
 // window's first step, as in the per-step form.
-__global__ void __launch_bounds__(256) k_win_facilitate(WinDev w, int64_t n0) {
+__global__ void __launch_bounds__(256) k_win_facilitate(WinDev w) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
@@ -954,17 +1025,18 @@ __global__ void __launch_bounds__(256) k_win_facilitate(WinDev w, int64_t n0) {
             eid[u] = cpos < end ? w.s.cperm[cpos] : 0;
         }
         double wv[kEdgeU];
-        long long up[kEdgeU];
+        uint32_t am[kEdgeU];
 #pragma unroll
         for (int u = 0; u < kEdgeU; ++u) {
             if (pre[u] < 0) continue;
             wv[u] = w.s.w[eid[u]];
-            up[u] = w.upto[eid[u]];
+            am[u] = w.amask[pre[u]];
         }
 #pragma unroll
         for (int u = 0; u < kEdgeU; ++u) {
             if (pre[u] < 0) continue;
-            const int lo = up[u] >= n0 - 1 ? static_cast<int>(up[u] - n0 + 1) : 0;
+            // the edge's last arrival in the window brought it up to date
+            const int lo = am[u] ? 32 - __clz(static_cast<int>(am[u])) : 0;
             uint64_t due = mask & ~((1ull << lo) - 1ull);
             double x = wv[u];
             for (; due; due &= due - 1ull) {
@@ -1161,7 +1233,7 @@ WinDev win_desc(bspk_plan *p, const std::vector<StdpDev> &sd) {
     w.W = p->W;
     w.cap = p->win_cap;
     w.kp = p->d_win_kp;
-    w.upto = p->d_win_upto;
+    w.amask = p->d_win_amask;
     w.arr = p->d_win_arr;
     w.cnt = p->d_win_cnt;
     w.spk = p->d_win_spk;
@@ -1202,7 +1274,7 @@ int run_windowed(bspk_plan *p, int64_t n_steps, cudaStream_t st) {
         k_win_deliver<Real><<<eg, 256, 0, st>>>(a, w, n0);
         launches += 2;
         if (w.on) {
-            k_win_facilitate<<<eg, 256, 0, st>>>(w, n0);
+            k_win_facilitate<<<eg, 256, 0, st>>>(w);
             ++launches;
         }
         cudaError_t e = cudaGetLastError();

@@ -1025,7 +1025,7 @@ static int alloc_window(bspk_plan *p) {
     const size_t E = J ? std::max<size_t>(J->post_local.size(), 1) : 1;
     const size_t cap = J ? p->win_cap : 1;
     int rc = dalloc(p, &p->d_win_kp, W * npre);
-    if (!rc) rc = dalloc(p, &p->d_win_upto, E);
+    if (!rc) rc = dalloc(p, &p->d_win_amask, npre);
     if (!rc) rc = dalloc(p, &p->d_win_arr, W * cap * npost);
     if (!rc) rc = dalloc(p, &p->d_win_cnt, W * npost);
     if (!rc) rc = dalloc(p, &p->d_win_spk, W * static_cast<size_t>(p->N));
@@ -1033,8 +1033,7 @@ static int alloc_window(bspk_plan *p) {
     if (!rc) rc = dalloc(p, &p->d_win_post, 2 * npost);
     if (!rc) rc = dalloc(p, &p->d_win_ctr, 4);
     if (rc) return rc;
-    // no edge has been brought up to date by an arrival yet (step -1)
-    BSPK_CUDA(cudaMemset(p->d_win_upto, 0xFF, sizeof(long long) * E));
+    BSPK_CUDA(cudaMemset(p->d_win_amask, 0, sizeof(uint32_t) * npre));
     BSPK_CUDA(cudaMemset(p->d_win_cnt, 0, sizeof(int) * W * npost));
     return BSPK_OK;
 }

@@ -125,7 +125,7 @@ struct bspk_plan {
     // per-step form
     bool win = false, win_ok = false;  // selected, possible
     double *d_win_kp = nullptr;
-    long long *d_win_upto = nullptr;
+    uint32_t *d_win_amask = nullptr;
     bspk::WinArrival *d_win_arr = nullptr;
     int *d_win_cnt = nullptr;
     int win_cap = 0;

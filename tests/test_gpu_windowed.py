@@ -149,3 +149,55 @@ def test_windowed_aeif_matches_per_step():
     # input summation order
     n_w, n_r = win.rk_substeps(), ref.rk_substeps()
     assert abs(n_w - n_r) <= 1e-3 * n_r, (n_w, n_r)
+
+
+
+def _aeif_stdp_plan(windowed, seed=21):
+    """AdEx network with a plastic E->E projection (lag 21 steps; the others
+    21-26) and W = 21: posts fire inside windows that still bring them
+    arrivals, and the strong drive makes some pres fire twice within one
+    window (edges with two arrivals in a window)."""
+    rng = np.random.default_rng(seed)
+    NE, NI = 160, 40
+    pl = _lib.Plan(0.1, "aeif_cond_alpha", precision=64)
+    pl.add_pop(NE, AEIF)
+    pl.add_pop(NI, AEIF)
+    pl.add_poisson(0, 12000.0, 3.5, 5, 31, receptor=0)
+    pl.add_poisson(1, 12000.0, 3.5, 5, 32, receptor=0)
+    ids = []
+    for pre, K, w, rc in ((0, 16, 0.8, 0), (1, 4, 2.5, 1)):
+        for post in (0, 1):
+            n_pre, n_post = (NE if pre == 0 else NI), (NE if post == 0 else NI)
+            d = 20 if (pre, post) == (0, 0) else rng.integers(20, 26, n_post * K)
+            indptr, idx, ww, dd = random_csr(rng, n_pre, n_post, K, w, d)
+            ids.append(pl.add_csr(pre, post, indptr, idx, ww, dd, rc))
+    pl.attach_stdp(ids[0], 20.0, 20.0, 0.05, 1.0, 1.0, 1.0, 2.4)
+    v0 = rng.uniform(-65.0, -52.0, NE + NI)
+    pl.record_v(np.arange(0, 200, 3))
+    pl.upload()
+    pl.set_state(0, "V_m", v0[:NE])
+    pl.set_state(1, "V_m", v0[NE:])
+    if not windowed:
+        pl.set_windowed(False)
+    return pl, ids
+
+
+def test_windowed_aeif_stdp_matches_per_step():
+    """RKF45 neurons with a plastic projection: the windowed form against the
+    per-step form, identical rasters and FP64 weights, states within the
+    reordered input sums."""
+    win, ids = _aeif_stdp_plan(True)
+    ref, _ = _aeif_stdp_plan(False)
+    assert win.engine == "windowed"
+    for n in (140, 230):  # runs end inside windows
+        win.run(n)
+        ref.run(n)
+    r = _raster(ref)
+    assert len(r) > 300
+    assert _raster(win) == r
+    np.testing.assert_allclose(win.weights(ids[0]), ref.weights(ids[0]), rtol=1e-12, atol=0)
+    np.testing.assert_allclose(win.v_trace(), ref.v_trace(), rtol=0, atol=2e-6)
+    for name in ("w", "g_ex", "g_in"):
+        np.testing.assert_allclose(win.get_state(0, name), ref.get_state(0, name), rtol=0, atol=2e-6)
+    n_w, n_r = win.rk_substeps(), ref.rk_substeps()
+    assert abs(n_w - n_r) <= 1e-3 * n_r, (n_w, n_r)
