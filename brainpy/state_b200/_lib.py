@@ -103,6 +103,7 @@ def lib():
             "bspk_state_set": (C.c_int, [vp, C.c_int, C.c_char_p, vp]),
             "bspk_step_count": (i64, [vp]),
             "bspk_plan_engine": (C.c_char_p, [vp]),
+            "bspk_plan_set_trial": (C.c_int, [vp, C.c_uint32]),
             "bspk_plan_set_windowed": (C.c_int, [vp, C.c_int]),
             "bspk_plan_tune_tiled": (C.c_int, [vp, i64, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                                C.POINTER(dbl)]),
@@ -468,6 +469,11 @@ class Plan:
         """Kernel family of the uploaded plan: 'tiled', 'global_ring', 'exact',
         'per_step' or 'windowed'."""
         return self._L.bspk_plan_engine(self._h).decode()
+
+    def set_trial(self, trial):
+        """Trial index folded into every keyed drive's step keys (the kernel
+        path's batched trials); before upload."""
+        check(self._L.bspk_plan_set_trial(self._h, int(trial)))
 
     def set_windowed(self, on):
         """Run a plan that can run windowed in the windowed (True) or the

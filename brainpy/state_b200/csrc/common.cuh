@@ -65,15 +65,16 @@ __device__ __forceinline__ void fold_key(uint32_t &k0, uint32_t &k1, uint32_t d)
 //  kind 1: the reference kernel path's poisson_generator stream
 //    (_kernel/models/devices.py:103-145, _kernel/rng.py:338-420): unit
 //    u = unit_off + idx of the device population, block key
-//    fold(obj, u >> 10), step key fold(fold(block, step), trial 0), and the
-//    23 mantissa bits of jax.random.uniform's float32 draw at lane u & 1023.
+//    fold(obj, u >> 10), step key fold(fold(block, step), trial) (trial 0
+//    for an unbatched run), and the 23 mantissa bits of
+//    jax.random.uniform's float32 draw at lane u & 1023.
 __device__ __forceinline__ uint64_t drive_draw(const DriveDev &d, uint32_t step, uint32_t idx) {
     if (d.kind == 0) return bits53(d.seed, 0u, step, idx);
     const uint64_t unit = static_cast<uint64_t>(d.unit_off) + idx;
     uint32_t k0 = d.key0, k1 = d.key1;
     fold_key(k0, k1, static_cast<uint32_t>(unit >> 10));
     fold_key(k0, k1, step);
-    fold_key(k0, k1, 0u);
+    fold_key(k0, k1, d.trial);
     uint32_t y0, y1;
     threefry2x32(k0, k1, 0u, static_cast<uint32_t>(unit & 1023u), y0, y1);
     return (y0 ^ y1) >> 9;

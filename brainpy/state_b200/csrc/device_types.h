@@ -90,6 +90,7 @@ struct DriveDev {
     int kind;
     uint32_t key0, key1;
     int64_t unit_off;
+    uint32_t trial;    // kind 1: trial index folded into every step key
 };
 
 // One projection (CSR over the pre population's local indices).

@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64
     {
         // The reference kernel path's stream (kind 1) draws a step's numbers
         // for a block of 1024 units from one step key, fold(fold(block key,
-        // step), 0): two threefry rounds that every lane of a warp would
+        // step), trial): two threefry rounds that every lane of a warp would
         // repeat.  When all 32 lanes have one such drive with the same block
         // key, lag and window, lane l derives the step key of step kc + l and
         // the warp shares the 32 keys by shuffles: one threefry per draw.
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(256) k_drive_fill(const LifArgs<Real> a, int64
             for (int kc = k0; kc < k1; kc += 32) {
                 uint32_t s0 = kb0, s1 = kb1;
                 fold_key(s0, s1, static_cast<uint32_t>(m0 + kc + lane - lag0));
-                fold_key(s0, s1, 0u);
+                fold_key(s0, s1, d.trial);
                 const int kend = min(32, k1 - kc);
                 for (int j = 0; j < kend; ++j) {
                     const uint32_t t0 = __shfl_sync(kFull, s0, j), t1 = __shfl_sync(kFull, s1, j);

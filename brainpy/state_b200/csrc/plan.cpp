@@ -1180,6 +1180,7 @@ extern "C" int bspk_plan_upload(bspk_plan *p, void *stream) {
         d.key0 = D.key0;
         d.key1 = D.key1;
         d.unit_off = D.unit_off;
+        d.trial = p->trial;
         if (D.kind == 1) {
             d.cdf_n = static_cast<int>(D.thr.size());
             cdf.insert(cdf.end(), D.thr.begin(), D.thr.end());
@@ -1849,6 +1850,13 @@ int bspk_plan_ring_fraction_bits(bspk_plan *p, int *bits) {
     if (!p || !bits) return fail(BSPK_ERR_ARG, "null argument");
     if (!p->uploaded || !p->tiled) return fail(BSPK_ERR_STATE, "not an uploaded plan on the tiled path");
     *bits = static_cast<int>(std::lround(-std::log2(p->tinv_scale)));
+    return BSPK_OK;
+}
+
+int bspk_plan_set_trial(bspk_plan *p, uint32_t trial) {
+    if (!p) return fail(BSPK_ERR_ARG, "null plan");
+    if (p->uploaded) return fail(BSPK_ERR_STATE, "the trial is set before upload");
+    p->trial = trial;
     return BSPK_OK;
 }
 

@@ -129,6 +129,7 @@ struct bspk_plan {
     bspk::WinArrival *d_win_arr = nullptr;
     int *d_win_cnt = nullptr;
     int win_cap = 0;
+    uint32_t trial = 0;  // trial index of the keyed drives' step keys
     uint32_t *d_win_spk = nullptr;
     uint32_t *d_win_pre = nullptr;
     uint32_t *d_win_post = nullptr;

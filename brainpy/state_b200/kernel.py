@@ -34,8 +34,9 @@ Limits of this front end: the neuron models are ``iaf_psc_alpha`` and
 with fixed-substep RK4, which the library does not run); the one device is
 ``poisson_generator`` with rate * dt below 10 per step (the reference's CDF
 inversion range), connected ``one_to_one`` onto whole neuron populations;
-``fixed_indegree`` needs ``allow_multapses=True``; no batched trials,
-plasticity or learners.
+``fixed_indegree`` needs ``allow_multapses=True``; no plasticity or learners.
+Batched trials (``Runner(program, batch=B, rng=...)``) fold the trial index
+into the drives' step keys as the reference's ``vmap`` runs do.
 """
 from __future__ import annotations
 
@@ -48,6 +49,7 @@ from .streams import LogNormal, Normal, Uniform, name_id
 from .units import Hz, mV, ms, pA, mantissa
 
 __all__ = ["Network", "PopulationView", "Projection", "Observer", "Program", "Runner", "Results",
+           "trial_indices",
            "Recording", "poisson_generator", "all_to_all", "one_to_one", "fixed_indegree",
            "iaf_psc_alpha", "iaf_psc_exp", "name_id", "Uniform", "Normal", "LogNormal"]
 
@@ -394,13 +396,16 @@ def realise_positions(net, proj):
 class Program:
     """A compiled network: the library plan plus the gid maps (``runner()``)."""
 
-    def __init__(self, net, precision, upload=True, spike_capacity=None):
+    def __init__(self, net, precision, upload=True, spike_capacity=None, trial=0):
         self.net, self.precision, self.dt = net, precision, net.dt
+        self.spike_capacity, self.trial = spike_capacity, int(trial)
         neurons = [p for p in net.populations if not p.is_device]
         model = neurons[0].model if neurons else iaf_psc_alpha
         kw = {} if spike_capacity is None else {"spike_capacity": int(spike_capacity)}
         pl = _lib.Plan(net.dt, model.model_name, precision=precision, semantics=_lib.RING, **kw)
         pl.set_ports(True)
+        if self.trial:
+            pl.set_trial(self.trial)
         self.lib_gid0 = {}  # population index -> first library gid
         g0 = 0
         for p in neurons:
@@ -537,8 +542,8 @@ class Program:
                                  receptor=port)
             self.drives.append((p.lib_pop, prm["rate"], w, ds, okey, u0, t_min, t_max, port))
 
-    def runner(self):
-        return Runner(self)
+    def runner(self, batch=None, rng="independent"):
+        return Runner(self, batch=batch, rng=rng)
 
 
 class Recording(dict):
@@ -557,42 +562,98 @@ class Results:
         return (obs.name if isinstance(obs, Observer) else obs) in self._recs
 
 
+RNG_MODES = ("independent", "common")
+
+
+def trial_indices(batch, rng="independent"):
+    """Trial indices of a run (``_kernel/runner.py:84-113``): ``None`` -> trial
+    0 (a uint32 scalar); ``B`` -> ``0 .. B-1`` ('independent') or ``B`` zeros
+    ('common')."""
+    if rng not in RNG_MODES:
+        raise ValueError(f"rng must be one of {RNG_MODES}, got {rng!r}")
+    if batch is None:
+        return np.uint32(0)
+    if isinstance(batch, bool) or not isinstance(batch, (int, np.integer)) or batch < 1:
+        raise ValueError(f"batch must be a positive int or None, got {batch!r}")
+    b = int(batch)
+    return np.arange(b, dtype=np.uint32) if rng == "independent" else np.zeros(b, np.uint32)
+
+
 class Runner:
     """Runs a program (``_kernel/runner.py:782-960``): ``simulate`` (from the
-    initial state), ``cont`` (from the current state and time), ``reset``."""
+    initial state), ``cont`` (from the current state and time), ``reset``.
 
-    def __init__(self, program):
+    ``batch=B`` runs B trials of the program: the same connectivity, weights,
+    delays and initial state, with trial b's index folded into every
+    ``poisson_generator`` step key ('independent'; 'common' gives every trial
+    trial 0's numbers), so trial 0 equals the unbatched run.  Every recording
+    then has a leading trial axis.  Each distinct trial index is one library
+    plan run on the device after the other; 'common' runs one plan and repeats
+    its recordings."""
+
+    def __init__(self, program, batch=None, rng="independent"):
         if not isinstance(program, Program):
             raise TypeError(f"Runner needs a Program, got {type(program).__name__}")
+        self._trials = trial_indices(batch, rng)
+        if program.trial != 0:
+            raise ValueError("a Runner starts from the program of trial 0")
         self.program = program
+        self.batch = None if batch is None else int(batch)
+        self.rng = rng
+        self._progs = {0: program}
+        if self.batch is not None:
+            for t in sorted(set(int(x) for x in self._trials) - {0}):
+                self._progs[t] = Program(program.net, program.precision,
+                                         spike_capacity=program.spike_capacity, trial=t)
         self.n = 0
         self.h2d_bytes = self.d2h_bytes = 0
+
+    @property
+    def trials(self):
+        """Trial indices (uint32; a scalar unbatched, ``(batch,)`` batched)."""
+        return self._trials
 
     @property
     def t(self):
         return self.n * self.program.dt  # ms
 
     def reset(self):
-        self.program.plan.restore(self.program._ck0)
+        self.h2d_bytes = 0
+        for prog in self._progs.values():
+            prog.plan.restore(prog._ck0)
+            self.h2d_bytes += int(prog._ck0.nbytes)
         self.n = 0
-        self.h2d_bytes = int(self.program._ck0.nbytes)
 
     def simulate(self, duration):
         self.reset()
         return self.cont(duration)
 
     def cont(self, duration):
-        prog = self.program
-        n_steps = _steps(duration, prog.dt, "duration")
-        for o in prog.net.observers:
+        n_steps = _steps(duration, self.program.dt, "duration")
+        for o in self.program.net.observers:
             o.n_samples(n_steps)
+        self.d2h_bytes = 0
+        per = {t: self._run_one(prog, n_steps) for t, prog in self._progs.items()}
+        self.n += n_steps
+        if self.batch is None:
+            return Results(per[0])
+        recs = {}
+        for name, r0 in per[0].items():
+            rec = Recording()
+            for key in r0:
+                rec[key] = np.stack([per[int(t)][name][key] for t in self._trials])
+            rec.times = r0.times
+            recs[name] = rec
+        return Results(recs)
+
+    def _run_one(self, prog, n_steps):
         pl = prog.plan
         pl.run(n_steps)
         st, g = pl.spikes()
         v = pl.v_trace(np.float32 if prog.precision == 32 else np.float64) \
             if prog.rec_v.size else None
         # bytes read back from the device by this call (spike pairs, V_m)
-        self.d2h_bytes = int(st.nbytes + g.nbytes + (v.nbytes if v is not None else 0))
+        self.d2h_bytes += int(st.nbytes + g.nbytes + (v.nbytes if v is not None else 0))
         recs = {}
         for o in prog.net.observers:
             k, ns = o.interval, o.n_samples(n_steps)
@@ -615,5 +676,4 @@ class Runner:
                 rec["V_m"] = vk if full else vk[:, at]
             rec.times = (self.n + (np.arange(ns) + 1) * k) * prog.dt
             recs[o.name] = rec
-        self.n += n_steps
-        return Results(recs)
+        return recs

@@ -149,8 +149,9 @@ int bspk_drive_add_poisson(bspk_plan *plan, int post_pop, double rate_hz, double
  * device population with object key obj_key = fold(fold(PRNGKey(seed),
  * hi), lo) of its name id (_kernel/rng.py:153-176), whose unit
  * unit_off + i drives neuron i of post_pop one_to_one.  Per emission step n
- * the units of block b draw jax.random.uniform(fold(fold(fold(obj, b), n), 0),
- * (1024,), float32) (block keys, _kernel/rng.py:338-420) and the count is
+ * the units of block b draw jax.random.uniform(fold(fold(fold(obj, b), n), t),
+ * (1024,), float32) with t the plan's trial (0 unless bspk_plan_set_trial)
+ * (block keys, _kernel/rng.py:338-420) and the count is
  * the CDF inversion of _kernel/models/devices.py:46-67 in float32, active iff
  * t_min < n <= t_max; the counts arrive delay_steps later with weight.
  * Replaces poisson_counts (_kernel/models/devices.py:70-145); rate*dt/1000
@@ -160,6 +161,12 @@ int bspk_drive_add_poisson_keyed(bspk_plan *plan, int post_pop, double rate_hz, 
                                  int delay_steps, const uint32_t *obj_key, int64_t unit_off,
                                  int64_t t_min_step, int64_t t_max_step, int receptor,
                                  int *drive_id);
+/* The trial index every keyed drive of the plan folds into its step keys in
+ * place of 0: fold(fold(fold(obj, b), n), trial) -- trial b of the kernel
+ * path's batched runs (Runner(batch=B), 'independent': trial b; 'common' and
+ * unbatched runs: 0), _kernel/rng.py:335-356 and _kernel/runner.py:84-113.
+ * Set before upload (BSPK_ERR_STATE after). */
+int bspk_plan_set_trial(bspk_plan *plan, uint32_t trial);
 
 /* The reference's random draws on the host (JAX's threefry PRNG,
  * partitionable layout): fold_in (jax.random.fold_in), uniform

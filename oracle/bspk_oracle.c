@@ -308,13 +308,18 @@ int64_t bo_kernel_poisson_count(const uint32_t step_key[2], uint32_t lane, float
     return k;
 }
 
-/* The step key of block b of a device population at step n, trial 0:
- * fold(fold(fold(obj, b), n), 0) (_kernel/rng.py:338-420). */
-void bo_kernel_step_key(const uint32_t obj[2], uint32_t block, uint32_t step, uint32_t out[2]) {
+/* The step key of block b of a device population at step n of trial t:
+ * fold(fold(fold(obj, b), n), t) (_kernel/rng.py:335-356, 338-420); an
+ * unbatched run is trial 0. */
+void bo_kernel_step_key_trial(const uint32_t obj[2], uint32_t block, uint32_t step, uint32_t trial,
+                              uint32_t out[2]) {
     uint32_t a[2], c[2];
     bo_jax_fold_in(obj, block, a);
     bo_jax_fold_in(a, step, c);
-    bo_jax_fold_in(c, 0u, out);
+    bo_jax_fold_in(c, trial, out);
+}
+void bo_kernel_step_key(const uint32_t obj[2], uint32_t block, uint32_t step, uint32_t out[2]) {
+    bo_kernel_step_key_trial(obj, block, step, 0u, out);
 }
 
 /* ----------------------------------------------------------- propagators */
@@ -387,6 +392,7 @@ typedef struct {
     int ddelay;
     uint32_t seed;
     int64_t tmin, tmax;
+    uint32_t trial; /* keyed drive: trial index of its step keys */
     /* keyed drive (the kernel path's stream): object key, first unit, lam */
     int keyed;
     uint32_t okey[2];
@@ -422,6 +428,7 @@ struct bo_sim {
     int64_t step;
     int64_t rk_substeps;
     int threads;  /* OpenMP threads of the independent per-neuron phases */
+    uint32_t trial; /* trial index of the keyed drives' step keys */
     double *acc; /* [RCH][ntot] input accumulator */
     double *y;   /* [2][ntot] per-projection vector */
 };
@@ -639,6 +646,11 @@ int bo_add_drive(bo_sim *s, int post_pop, double rate_hz, double weight, int del
     return s->nin++;
 }
 
+void bo_set_trial(bo_sim *s, uint32_t trial) {
+    s->trial = trial;
+    for (int i = 0; i < s->nin; ++i) s->ins[i].trial = trial;
+}
+
 int bo_add_drive_keyed(bo_sim *s, int post_pop, double rate_hz, double weight, int delay_steps,
                        const uint32_t okey[2], int64_t unit_off, int64_t t_min_step,
                        int64_t t_max_step, int receptor) {
@@ -647,6 +659,7 @@ int bo_add_drive_keyed(bo_sim *s, int post_pop, double rate_hz, double weight, i
     if (id < 0) return id;
     input_t *in = &s->ins[id];
     in->keyed = 1;
+    in->trial = s->trial;
     in->okey[0] = okey[0];
     in->okey[1] = okey[1];
     in->unit_off = unit_off;
@@ -778,7 +791,7 @@ static int64_t drive_count(const input_t *in, int64_t emit_step, int t) {
          * unit & 1023 (_kernel/rng.py draw_blocked, GID_BLOCK = 1024) */
         uint64_t unit = (uint64_t)in->unit_off + (uint64_t)t;
         uint32_t sk[2];
-        bo_kernel_step_key(in->okey, (uint32_t)(unit >> 10), (uint32_t)emit_step, sk);
+        bo_kernel_step_key_trial(in->okey, (uint32_t)(unit >> 10), (uint32_t)emit_step, in->trial, sk);
         return bo_kernel_poisson_count(sk, (uint32_t)(unit & 1023u), in->lam32);
     }
     double u = bo_uniform01(in->seed, 0u, (uint32_t)emit_step, (uint32_t)t);

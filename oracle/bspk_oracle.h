@@ -65,6 +65,10 @@ void bo_jax_uniform(const uint32_t key[2], int nbits, int64_t n, double lo, doub
 void bo_jax_normal(const uint32_t key[2], int nbits, int64_t n, double *out);
 /* kernel-path poisson_generator: step key of a block, count of one unit */
 void bo_kernel_step_key(const uint32_t obj[2], uint32_t block, uint32_t step, uint32_t out[2]);
+void bo_kernel_step_key_trial(const uint32_t obj[2], uint32_t block, uint32_t step, uint32_t trial,
+                              uint32_t out[2]);
+/* trial index folded into every keyed drive's step keys (default 0) */
+void bo_set_trial(bo_sim *s, uint32_t trial);
 int64_t bo_kernel_poisson_count(const uint32_t step_key[2], uint32_t lane, float lam);
 /* legacy fixed-indegree sampler (connectivity.py:101-135): post-major edges */
 int bo_fixed_indegree(int64_t seed, int n_pre, int n_post, int K, int pre_is_post,

@@ -97,6 +97,8 @@ def lib():
         L.bo_kernel_poisson_count.argtypes = [vp, u32, C.c_float]
         L.bo_add_drive_keyed.argtypes = [vp, C.c_int, dbl, dbl, C.c_int, vp, i64, i64, i64,
                                          C.c_int]
+        L.bo_set_trial.argtypes = [vp, u32]
+        L.bo_set_trial.restype = None
         L.bo_uniform01.restype = dbl
         L.bo_uniform01.argtypes = [u32, u32, u32, u32]
         L.bo_poisson.argtypes = [dbl, dbl, dbl]
@@ -312,6 +314,10 @@ class OracleSim:
         if r < 0:
             raise ValueError("add_drive failed")
         return r
+
+    def set_trial(self, trial):
+        """Trial index folded into the keyed drives' step keys (default 0)."""
+        self._L.bo_set_trial(self._h, int(trial))
 
     def add_drive_keyed(self, post_pop, rate_hz, weight, delay_steps, obj_key, unit_off=0,
                         t_min=0, t_max=2 ** 62, receptor=0):

@@ -121,3 +121,32 @@ def test_headline_kernel_network_rates_within_1pct_of_oracle(oracle):
         rate = ref / (p["NE"] + p["NI"]) / (steps * 1e-4)
         assert 20.0 < rate < 60.0   # Hz
         assert abs(count - ref) / ref < 0.01, (bits, count, ref)
+
+
+def test_batched_trials_fold_the_trial_into_the_drive_keys(oracle):
+    """Runner(batch=3): trial 0 is the unbatched run; trial 2's noise comes
+    from the step keys with 2 folded in (the oracle run with that trial);
+    trials differ; rng='common' repeats trial 0 (_kernel/runner.py:84-113,
+    _kernel/rng.py:335-356)."""
+    from brainpy.state_b200.kernel import Runner
+    from oracle import kernel_net as KN
+    order, n = 100, 300
+    rec = np.arange(0, 500, 7)
+    net, p, _ = brunel.build_kernel_network(order=order)
+    obs = net.observe(_view(net, rec), "V_m", name="taps")
+    prog = net.compile("float64")
+    base = prog.runner().simulate(n * 0.1)[obs]["V_m"]
+    run = Runner(prog, batch=3)
+    assert run.trials.tolist() == [0, 1, 2]
+    v = run.simulate(n * 0.1)[obs]["V_m"]
+    assert v.shape == (3,) + base.shape
+    np.testing.assert_array_equal(v[0], base)
+    assert np.abs(v[1] - v[0]).max() > 1e-3
+    sim, _ = KN.build(p, seed=1234, order=order, bits=64)
+    sim.set_trial(2)
+    sim.record_v(rec)
+    _, _, ov = sim.run(n)
+    np.testing.assert_allclose(v[2], ov, rtol=0, atol=1e-9)
+    common = Runner(prog, batch=2, rng="common").simulate(n * 0.1)[obs]["V_m"]
+    np.testing.assert_array_equal(common[0], base)
+    np.testing.assert_array_equal(common[1], base)

@@ -96,3 +96,35 @@ def test_realised_edges_do_not_depend_on_unrelated_populations():
             return out
         return named(proj.pre, src), named(proj.post, dst)
     assert build(False) == build(True)
+
+
+def test_trial_indices():
+    """The reference's doctest (_kernel/runner.py:100-106) and its checks."""
+    assert K.trial_indices(3).tolist() == [0, 1, 2]
+    assert K.trial_indices(2, "common").tolist() == [0, 0]
+    assert int(K.trial_indices(None)) == 0
+    assert K.trial_indices(4).dtype == np.uint32
+    with pytest.raises(ValueError):
+        K.trial_indices(2, "shared")
+    for bad in (0, -1, 2.0, True):
+        with pytest.raises(ValueError):
+            K.trial_indices(bad)
+
+
+def test_oracle_trial_folds_into_keyed_step_keys(oracle):
+    """The oracle's keyed drive draws trial t's counts from
+    fold(fold(fold(obj, b), n), t): its counts for trial 0 are the unbatched
+    ones, another trial's differ."""
+    from oracle import kernel_net as KN
+    counts = []
+    for trial in (0, 0, 3):
+        sim = oracle.OracleSim(0.1, "iaf_psc_alpha", semantics=oracle.RING)
+        sim.set_ports(True)
+        a = sim.add_pop(200, [0.0, 250.0, 20.0, 2.0, 20.0, 10.0, 0.5, 0.5, 0.0, -np.inf])
+        sim.set_trial(trial)
+        sim.add_drive_keyed(a, 30000.0, 25.0, 10, KN.object_key(7, "noise"), 0, 0, 2 ** 62, 0)
+        sim.record_v(np.arange(0, 200, 9))
+        _, _, v = sim.run(60, cap=1 << 16)
+        counts.append(v)
+    np.testing.assert_array_equal(counts[0], counts[1])
+    assert np.abs(counts[2] - counts[0]).max() > 1e-6
