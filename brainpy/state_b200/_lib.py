@@ -411,8 +411,9 @@ class Plan:
         check(self._L.bspk_run(self._h, int(n_steps), stream))
         self._last_steps = int(n_steps)
 
-    def spikes(self, cap=None):
-        """(steps, gids) of the last run's recorded spikes, sorted by step then gid."""
+    def spikes(self, cap=None, sort=True):
+        """(steps, gids) of the last run's recorded spikes, sorted by step then
+        gid (``sort=False``: in the device's record order)."""
         n = C.c_int64()
         if cap is None:  # ask for the count first, then copy exactly that many
             check(self._L.bspk_spikes_get(self._h, 0, None, None, C.byref(n)))
@@ -422,6 +423,8 @@ class Plan:
         g = np.empty(cap, np.int32)
         check(self._L.bspk_spikes_get(self._h, cap, ptr(st), ptr(g), C.byref(n)))
         m = min(n.value, cap)
+        if not sort:
+            return st[:m], g[:m]
         order = np.lexsort((g[:m], st[:m]))
         return st[:m][order], g[:m][order]
 

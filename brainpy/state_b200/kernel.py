@@ -442,6 +442,12 @@ class Program:
         # library columns of every observer, in view order
         self.obs_cols = {o.name: np.array([self._lib_gid(x) for x in o.view.gids], np.int64)
                          for o in net.observers}
+        # library gid -> observer column (-1: not observed), per spike observer
+        self.obs_pos = {}
+        for o in net.observers:
+            pos = np.full(self.n_lib, -1, np.int64)
+            pos[self.obs_cols[o.name]] = np.arange(self.obs_cols[o.name].size)
+            self.obs_pos[o.name] = pos
 
     @property
     def bits(self):
@@ -649,7 +655,7 @@ class Runner:
     def _run_one(self, prog, n_steps):
         pl = prog.plan
         pl.run(n_steps)
-        st, g = pl.spikes()
+        st, g = pl.spikes(sort=False)  # binned into counts below: order is irrelevant
         v = pl.v_trace(np.float32 if prog.precision == 32 else np.float64) \
             if prog.rec_v.size else None
         # bytes read back from the device by this call (spike pairs, V_m)
@@ -661,8 +667,7 @@ class Runner:
             rec = Recording()
             if "spike" in o.recordables:
                 counts = np.zeros((ns, cols.size), np.float64)
-                pos = np.full(prog.n_lib, -1, np.int64)
-                pos[cols] = np.arange(cols.size)
+                pos = prog.obs_pos[o.name]
                 col = pos[g] if g.size else np.zeros(0, np.int64)
                 ok = col >= 0
                 np.add.at(counts, ((st[ok] - self.n) // k, col[ok]), 1.0)

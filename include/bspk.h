@@ -515,7 +515,9 @@ int bspk_adjoint_status(bspk_adjoint *adj);
  * drive_seed each.  All calls on a device share the scratch array, so calls
  * that overlap on the GPU race; serialise them.  The first call on a device
  * looks up the scratch array's device address (once per device, with that
- * device current); make that first call before capturing any stream. */
+ * device current).  Every call copies its small tables (coefficients, drive,
+ * CDF, projection descriptor) from host memory with cudaMemcpyAsync, so no
+ * call may be made on a stream that is being captured into a CUDA graph. */
 int bspk_iaf_exact_run_noalloc(double dt, const double *params, int n_params, int n,
                                const int64_t *in_indptr, const uint32_t *in_edges,
                                const double *in_w, double w_const, int min_delay_steps,
