@@ -201,8 +201,9 @@ def run_ours(args):
         with open(prof) as f:
             for line in f:
                 if line.startswith("traffic_bytes_per_launch ="):
-                    # an ncu capture of a 1000-step launch of this kernel, scaled to
-                    # this launch's time steps (not measured in this run)
+                    # an ncu capture of one launch of this kernel, given per
+                    # 10 000 time steps and scaled to this launch's steps (not
+                    # measured in this run)
                     traffic = int(line.split("=")[1]) * STEPS_PER_BENCH_STEP // 10000
                     traffic_source = ("ncu capture summarised in profiles/"
                                       "k_lif_tiled_brunel12500_ncu_full.md, scaled")
